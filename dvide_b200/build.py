@@ -1,0 +1,74 @@
+"""Build recipe for the native parts of dvide_b200.
+
+* libdvide_b200.so -- every CUDA kernel and the C ABI of include/dvide.h,
+  compiled for sm_100a only, with -fmad=false so that the FP64 path rounds
+  exactly like the CPU oracle (no fused multiply-add).
+* libdvide_cxx.so -- the C++ System/Body/APGD/CollisionDetector classes
+  (include/dvide/*.h) layered on the C ABI.
+
+Outputs are written in-tree, next to this file, so they travel with the
+repository snapshot.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+
+CUDA_SOURCES = ["dv_sort.cu", "dv_collide.cu", "dv_apgd.cu", "dv_scene.cu"]
+CUDA_HEADERS = ["dv_common.cuh", "dv_internal.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-fvisibility=hidden"]
+
+LIB = os.path.join(HERE, "libdvide_b200.so")
+
+
+def _nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if c and (os.path.isabs(c) and os.path.exists(c) or not os.path.isabs(c)):
+            return c
+    return "nvcc"
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_cuda(force=False, verbose=False):
+    srcs = [os.path.join(CSRC, s) for s in CUDA_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [os.path.join(INCLUDE, "dvide.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objs = []
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    for s in srcs:
+        o = os.path.join(HERE, "_build", os.path.basename(s) + ".o")
+        cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-c", s, "-o", o]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+        objs.append(o)
+    tmp = LIB + ".tmp"
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart_static"]
+    subprocess.check_call(cmd)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build(force=False, verbose=False):
+    out = [build_cuda(force=force, verbose=verbose)]
+    return out
+
+
+if __name__ == "__main__":
+    for p in build(force="--force" in sys.argv, verbose=True):
+        print(p)

@@ -1,0 +1,235 @@
+"""Seeded synthetic scenes for the rigid-body contact step.
+
+Every scene is a set of bodies in the layout DVIDE's ``System::initializeSystem``
+flattens (src/System.cu:342-424): position, velocity, mass, contact geometry
+``(r, 0, 0)`` for a sphere or box half-extents ``(hx, hy, hz)`` (src/Body.cuh:18-60),
+a fixed flag and a collision family (src/PhysicsItem.cuh:13-33).
+
+Workloads (no dataset exists for this path; all inputs are generated here):
+
+* :func:`settling_box` -- 1,000 spheres r = 0.05 m, rho = 2600, on a 10x10x10
+  lattice of spacing 0.11 m with +-0.005 m jitter, in an open box of 5 fixed
+  boxes (floor 1.2 x 1.2 m interior, walls 1.5 m high), mu = 0.25, h = 1e-3.
+  The reference analogue is models/test_compaction.cu:272-333 (boxes first,
+  then spheres), with the sphere mass set to rho * 4/3 pi r^3 as in
+  models/test_shear.cu:329.
+* :func:`poured_column` -- 200,000 spheres, r ~ U[0.004, 0.006] m, rho = 2500,
+  mu = 0.3, random sequential addition (rejection sampling) in a column of
+  0.4 x 0.4 m cross-section, h = 5e-4.  The column is taller than 1.0 m because
+  200,000 such spheres occupy 0.109 m^3, which no non-overlapping random
+  packing fits into 0.16 m^3; the settled pile is about 1.1 m high.
+* :func:`batch_scenes` -- independent settling scenes with log-uniform sphere
+  counts, r ~ U[0.004, 0.006], mu ~ U[0.1, 0.5], each in its own container.
+* :func:`ball_on_ground` -- models/test_oneBall.cu:240-283 (unit ball resting
+  on a fixed box; at rest the normal impulse is m g h).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+G = 9.81
+
+
+@dataclasses.dataclass
+class Scene:
+    pos: np.ndarray
+    vel: np.ndarray
+    mass: np.ndarray
+    geom: np.ndarray
+    fixed: np.ndarray
+    family: np.ndarray
+    params: dict
+    name: str = "scene"
+
+    @property
+    def nb(self) -> int:
+        return int(self.pos.shape[0])
+
+    def copy(self) -> "Scene":
+        return Scene(self.pos.copy(), self.vel.copy(), self.mass.copy(), self.geom.copy(),
+                     self.fixed.copy(), self.family.copy(), dict(self.params), self.name)
+
+
+def default_params(**kw) -> dict:
+    """Defaults of the reference: h = 1e-3, mu = 0.25 (System.cu:62-72),
+    envelope 0.001 (CollisionDetector.cu:512), APGD tolerance 1e-4 and
+    maxIterations 100000 (APGD.cu:10-11), warm start off (APGD.cu:14)."""
+    p = dict(h=1e-3, mu=0.25, gravity=(0.0, -9.81, 0.0), envelope=1e-3, tolerance=1e-4,
+             max_iterations=100000, warm_start=0, max_backtracks=4096)
+    p.update(kw)
+    return p
+
+
+def _assemble(boxes, spheres_pos, spheres_r, rho, params, name, spheres_vel=None):
+    nbx = len(boxes)
+    ns = spheres_pos.shape[0]
+    nb = nbx + ns
+    pos = np.zeros((nb, 3))
+    geom = np.zeros((nb, 3))
+    mass = np.ones(nb)
+    fixed = np.zeros(nb, dtype=np.int32)
+    for i, (c, he, fx) in enumerate(boxes):
+        pos[i] = c
+        geom[i] = he
+        fixed[i] = 1 if fx else 0
+    pos[nbx:] = spheres_pos
+    geom[nbx:, 0] = spheres_r
+    mass[nbx:] = rho * 4.0 / 3.0 * math.pi * spheres_r ** 3
+    vel = np.zeros((nb, 3))
+    if spheres_vel is not None:
+        vel[nbx:] = spheres_vel
+    family = np.full(nb, -1, dtype=np.int32)
+    return Scene(pos, vel, mass, geom, fixed, family, params, name)
+
+
+def open_box(inner_x, inner_y, height, thick=0.1, cx=0.0, cy=0.0):
+    """Floor + 4 walls, all fixed; floor top at z = 0 and interior
+    [cx - inner_x/2, cx + inner_x/2] x [cy - inner_y/2, cy + inner_y/2]."""
+    t = 0.5 * thick
+    hx, hy = 0.5 * inner_x, 0.5 * inner_y
+    return [
+        ((cx, cy, -t), (hx + thick, hy + thick, t), True),
+        ((cx - hx - t, cy, 0.5 * height), (t, hy + thick, 0.5 * height), True),
+        ((cx + hx + t, cy, 0.5 * height), (t, hy + thick, 0.5 * height), True),
+        ((cx, cy - hy - t, 0.5 * height), (hx, t, 0.5 * height), True),
+        ((cx, cy + hy + t, 0.5 * height), (hx, t, 0.5 * height), True),
+    ]
+
+
+def settling_box(seed=0, n_side=10, radius=0.05, spacing=0.11, jitter=0.005, rho=2600.0,
+                 mu=0.25, h=1e-3, tolerance=1e-4, max_iterations=1000, warm_start=1) -> Scene:
+    rng = np.random.default_rng(seed)
+    idx = np.arange(n_side)
+    off = -0.5 * spacing * (n_side - 1)
+    gx, gy, gz = np.meshgrid(idx, idx, idx, indexing="ij")
+    pos = np.stack([off + spacing * gx.ravel(), off + spacing * gy.ravel(),
+                    radius + 0.01 + spacing * gz.ravel()], axis=1)
+    pos += rng.uniform(-jitter, jitter, size=pos.shape)
+    r = np.full(pos.shape[0], radius)
+    inner = 1.2 * (n_side / 10.0)
+    boxes = open_box(inner, inner, 1.5 * (n_side / 10.0))
+    params = default_params(h=h, mu=mu, gravity=(0.0, 0.0, -G), tolerance=tolerance,
+                            max_iterations=max_iterations, warm_start=warm_start)
+    return _assemble(boxes, pos, r, rho, params, f"settling_box_{pos.shape[0]}")
+
+
+def _rsa_column(rng, n, rmin, rmax, lx, ly, z0, fill=0.30, batch=16384):
+    """Random sequential addition: spheres are drawn uniformly in the column;
+    a draw is rejected when it overlaps an accepted sphere or an earlier draw of
+    its batch.  Radii are drawn with the positions, so the accepted radii keep
+    the U[rmin, rmax] law only approximately (small spheres fit more often)."""
+    from scipy.spatial import cKDTree
+
+    mean_v = 4.0 / 3.0 * math.pi * (rmax ** 4 - rmin ** 4) / (4.0 * (rmax - rmin))
+    height = n * mean_v / (fill * lx * ly) + 2 * rmax
+    P = np.zeros((0, 3))
+    R = np.zeros(0)
+    while P.shape[0] < n:
+        k = batch
+        r = rng.uniform(rmin, rmax, size=k)
+        p = np.stack([rng.uniform(r, lx - r), rng.uniform(r, ly - r),
+                      rng.uniform(r, height - r)], axis=1)
+        ok = np.ones(k, dtype=bool)
+        if P.shape[0]:
+            tree = cKDTree(P)
+            d, idx = tree.query(p, k=24, distance_upper_bound=2 * rmax)
+            valid = np.isfinite(d)
+            idc = np.where(valid, idx, 0)
+            ok &= ~np.any(valid & (d <= R[idc] + r[:, None]), axis=1)
+        cand = np.nonzero(ok)[0]
+        if cand.size > 1:
+            pairs = cKDTree(p[cand]).query_pairs(2 * rmax, output_type="ndarray")
+            if pairs.size:
+                i, j = pairs[:, 0], pairs[:, 1]
+                dd = np.linalg.norm(p[cand[i]] - p[cand[j]], axis=1)
+                hit = dd <= r[cand[i]] + r[cand[j]]
+                later = np.maximum(i[hit], j[hit])
+                keep = np.ones(cand.size, dtype=bool)
+                keep[later] = False
+                cand = cand[keep]
+        take = cand[: n - P.shape[0]]
+        P = np.concatenate([P, p[take]])
+        R = np.concatenate([R, r[take]])
+    P = P.copy()
+    P[:, 0] -= 0.5 * lx
+    P[:, 1] -= 0.5 * ly
+    P[:, 2] += z0
+    return P, R, height
+
+
+def poured_column(seed=1, n=200_000, rmin=0.004, rmax=0.006, rho=2500.0, mu=0.3, h=5e-4,
+                  lx=0.4, ly=0.4, tolerance=1e-4, max_iterations=500, warm_start=1,
+                  fill=0.30) -> Scene:
+    rng = np.random.default_rng(seed)
+    P, R, height = _rsa_column(rng, n, rmin, rmax, lx, ly, 0.0, fill=fill)
+    boxes = open_box(lx, ly, height + 0.1, thick=0.05)
+    params = default_params(h=h, mu=mu, gravity=(0.0, 0.0, -G), tolerance=tolerance,
+                            max_iterations=max_iterations, warm_start=warm_start)
+    return _assemble(boxes, P, R, rho, params, f"poured_column_{n}")
+
+
+def lattice_container(rng, n, rmin=0.004, rmax=0.006, rho=2500.0, mu=None, h=1e-3,
+                      tolerance=1e-4, max_iterations=500, warm_start=1, name="batch"):
+    """One settling scene of n spheres: square floor of side ~ cbrt(n) * 2.2 r_max,
+    walls twice the fill height, spheres on a jittered lattice of spacing 2.2 r_max."""
+    if mu is None:
+        mu = float(rng.uniform(0.1, 0.5))
+    s = 2.2 * rmax
+    side_n = max(1, int(round(n ** (1.0 / 3.0))))
+    layers = int(math.ceil(n / float(side_n * side_n)))
+    inner = side_n * s
+    fill_h = layers * s
+    gi = np.arange(n)
+    ix, iy, iz = gi % side_n, (gi // side_n) % side_n, gi // (side_n * side_n)
+    jit = 0.5 * (s - 2 * rmax) * 0.9
+    pos = np.stack([(ix + 0.5) * s - 0.5 * inner, (iy + 0.5) * s - 0.5 * inner,
+                    (iz + 0.5) * s], axis=1) + rng.uniform(-jit, jit, size=(n, 3))
+    r = rng.uniform(rmin, rmax, size=n)
+    boxes = open_box(inner, inner, 2.0 * fill_h + s, thick=0.02)
+    params = default_params(h=h, mu=mu, gravity=(0.0, 0.0, -G), tolerance=tolerance,
+                            max_iterations=max_iterations, warm_start=warm_start)
+    return _assemble(boxes, pos, r, rho, params, name)
+
+
+def batch_scenes(seed=3, count=512, nmin=100, nmax=20000, **kw):
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(math.log(nmin), math.log(nmax), size=count)).astype(np.int64)
+    return [lattice_container(rng, int(n), name=f"batch_{i}_{int(n)}", **kw)
+            for i, n in enumerate(ns)]
+
+
+def ball_on_ground(h=1e-2, tolerance=1e-5, warm_start=0, latforce=0.0) -> Scene:
+    """models/test_oneBall.cu:240-283: fixed unit box at y = -1, unit ball
+    (mass 1) at y = 1, gravity (latForce, -9.81, 0), h = 1e-2."""
+    pos = np.array([[0.0, -1.0, 0.0], [0.0, 1.0, 0.0]])
+    geom = np.array([[1.0, 1.0, 1.0], [1.0, 0.0, 0.0]])
+    params = default_params(h=h, tolerance=tolerance, warm_start=warm_start,
+                            gravity=(latforce, -9.81, 0.0), max_iterations=100000)
+    return Scene(pos, np.zeros((2, 3)), np.ones(2), geom, np.array([1, 0], dtype=np.int32),
+                 np.full(2, -1, dtype=np.int32), params, "ball_on_ground")
+
+
+def random_cluster(seed, n=40, box=True, radius=0.05, mu=0.25, h=1e-3, warm_start=1,
+                   max_iterations=400, tolerance=1e-6) -> Scene:
+    """Small parity-test scene: spheres on a jittered cubic lattice whose
+    spacing equals the largest diameter, so neighbours range from slightly
+    overlapping through inside the envelope to just separated; the lowest
+    layer rests on a fixed floor inside fixed walls; random initial velocities."""
+    rng = np.random.default_rng(seed)
+    side = max(2, int(math.ceil(n ** (1.0 / 3.0))))
+    s = 2.0 * radius
+    gi = np.arange(n)
+    ix, iy, iz = gi % side, (gi // side) % side, gi // (side * side)
+    pos = np.stack([(ix - 0.5 * (side - 1)) * s, (iy - 0.5 * (side - 1)) * s, radius + iz * s],
+                   axis=1)
+    pos += rng.uniform(-0.0015, 0.0015, size=pos.shape)
+    r = rng.uniform(0.97 * radius, radius, size=n)
+    inner = side * s + 0.004
+    boxes = open_box(inner, inner, (side + 2) * s, thick=0.1) if box else []
+    params = default_params(h=h, mu=mu, gravity=(0.0, 0.0, -G), tolerance=tolerance,
+                            max_iterations=max_iterations, warm_start=warm_start)
+    vel = rng.normal(0.0, 0.05, size=(n, 3))
+    return _assemble(boxes, pos, r, 2600.0, params, f"cluster_{seed}_{n}", spheres_vel=vel)

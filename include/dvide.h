@@ -1,0 +1,152 @@
+/*
+ * dvide.h -- C ABI of the B200-native DVIDE rigid-body contact step.
+ *
+ * One scene = one DVIDE System holding rigid spheres and boxes (3 DOF each,
+ * src/Body.cuh:14-100).  A time step is the reference's System::DoTimeStep
+ * (src/System.cu:544-602): collision detection, APGD cone-complementarity
+ * solve, half-implicit velocity/position update.  All state lives on the GPU;
+ * every call returns a status (0 = DV_OK).  Plain pointers and sizes only.
+ *
+ * The reference has no C ABI; each entry point names the C++ member of the
+ * reference it stands in for.
+ */
+#ifndef DVIDE_H_
+#define DVIDE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define DV_API __declspec(dllexport)
+#else
+#define DV_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference returns 0 from every method and checks no CUDA
+ * errors; src/System.cu, src/APGD.cu). */
+enum {
+  DV_OK = 0,
+  DV_ERR_ARG = 1,        /* invalid argument */
+  DV_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+  DV_ERR_NAN = 3,        /* non-finite value in the solve (e.g. sphere centre inside a box) */
+  DV_ERR_NOCONV = 4,     /* Lipschitz backtracking exceeded max_backtracks */
+  DV_ERR_OOM = 5,        /* device allocation failed or over the memory budget */
+  DV_ERR_TIMEOUT = 6,    /* a persistent kernel's bounded wait expired */
+  DV_ERR_UNSUPPORTED = 7,
+  DV_ERR_ABORTED = 8     /* cancelled through dv_*_abort */
+};
+
+enum { DV_PREC_FP64 = 0, DV_PREC_MIXED = 1 };
+enum { DV_SOLVER_APGD = 1 };
+
+/* One rigid body, as System::initializeSystem flattens it (System.cu:344-424). */
+typedef struct dv_body_desc {
+  double pos[3];
+  double vel[3];
+  double mass;       /* Body::mass, default 1.0 (Body.cuh:39) */
+  double geom[3];    /* (r, 0, 0) sphere, (hx, hy, hz) box half-extents (Body.cuh:18-60) */
+  int32_t fixed;     /* Body::fixed */
+  int32_t family;    /* PhysicsItem::collisionFamily, -1 collides with all */
+} dv_body_desc;
+
+typedef struct dv_params {
+  double h;              /* System::h (System.cu:66), default 1e-3 */
+  double mu;             /* System::frictionCoefficient (System.cu:65), default 0.25 */
+  double gravity[3];     /* System::gravity (System.cu:64), default (0, -9.81, 0) */
+  double envelope;       /* CollisionDetector::envelope (CollisionDetector.cu:512), default 1e-3 */
+  double tolerance;      /* Solver::tolerance (APGD.cu:10), default 1e-4 */
+  int32_t max_iterations;/* Solver::maxIterations (APGD.cu:11), default 100000 */
+  int32_t warm_start;    /* APGD::setWarmStarting (APGD.cuh:62), default 0 */
+  int32_t solver;        /* System(int solverType) (System.cu:84-107); 1 = APGD */
+  int32_t precision;     /* DV_PREC_FP64 (drop-in) or DV_PREC_MIXED */
+  int32_t max_backtracks;/* cap on Lipschitz doublings per solve (reference: unbounded) */
+  int32_t verbose;       /* print the per-step line of System.cu:592 */
+} dv_params;
+
+/* Per-step report (System.cu:586-599 and APGD.cu:351-357). */
+typedef struct dv_step_stats {
+  int32_t num_contacts;      /* CollisionDetector::numCollisions */
+  int32_t num_possible;      /* CollisionDetector::numPossibleCollisions */
+  int32_t iterations;        /* Solver::iterations */
+  int32_t backtracks;        /* Lipschitz doublings in the solve */
+  double residual;           /* best APGD residual */
+  double objective;          /* System::objectiveCCP */
+  double elapsed_ms;         /* System::elapsedTime (device time of the step) */
+  double time;               /* System::time */
+  int32_t time_index;        /* System::timeIndex */
+  int32_t status;
+} dv_step_stats;
+
+typedef struct dv_scene dv_scene;
+
+/* Fills *p with the reference defaults listed above. */
+DV_API int dv_params_default(dv_params* p);
+
+/* System(int solverType) + add(Body*) for each body + initializeSystem()
+ * (System.cu:62-133, 148-152, 342-508).  Copies the bodies to the device. */
+DV_API int dv_scene_create(const dv_body_desc* bodies, int32_t nb, const dv_params* params,
+                           dv_scene** out);
+DV_API int dv_scene_destroy(dv_scene* s);
+
+/* Runs the scene's kernels on a caller-provided cudaStream_t (NULL = the
+ * scene's own stream). */
+DV_API int dv_scene_set_stream(dv_scene* s, void* cuda_stream);
+DV_API int dv_set_params(dv_scene* s, const dv_params* params);
+
+/* System::DoTimeStep (System.cu:544-602), nsteps times. */
+DV_API int dv_step(dv_scene* s, int32_t nsteps);
+
+/* CollisionDetector::generateAxisAlignedBoundingBoxes +
+ * detectPossibleCollisions_spatialSubdivision + detectCollisions
+ * (CollisionDetector.cu:547-665): detection only, no solve or update. */
+DV_API int dv_collide(dv_scene* s);
+
+/* Body state, 3 doubles per body as System::p_d / v_d (System.cu:355-366). */
+DV_API int dv_get_state(dv_scene* s, double* p, double* v);
+DV_API int dv_set_state(dv_scene* s, const double* p, const double* v);
+/* System::f_contact_d after a step (System.cu:570-573), 3 per body. */
+DV_API int dv_get_contact_force(dv_scene* s, double* f);
+
+DV_API int dv_get_num_contacts(dv_scene* s, int32_t* nc, int32_t* npossible);
+/* collisionIdentifierA_d / B_d, normalsAndPenetrations_d (double4: stored
+ * normal B->A and gap) and collisionLocations_d (CollisionDetector.cuh:88-92,
+ * CollisionDetector.cu:493-498); any pointer may be NULL. */
+DV_API int dv_get_contacts(dv_scene* s, uint32_t* a, uint32_t* b, double* nP, double* loc);
+/* System::gamma_d, 3 per contact (warm-start buffer after the solve).
+ * Returns its length in contacts through *n. */
+DV_API int dv_get_gamma(dv_scene* s, double* gamma, int32_t cap, int32_t* n);
+/* Overwrites the warm-start buffer (length n contacts). */
+DV_API int dv_set_gamma(dv_scene* s, const double* gamma, int32_t n);
+/* Contact frames n, u, v (9 per contact) and Schur vector r (3 per contact)
+ * of the last step: System.cu:753-762, 1561-1580. */
+DV_API int dv_get_frames(dv_scene* s, double* F);
+DV_API int dv_get_schur_vector(dv_scene* s, double* r);
+
+/* System::getCCPViolation (System.cu:1605-1643): out4 = (min gamma_n,
+ * min v_n, gamma_n . v_n, ||cone violation||). */
+DV_API int dv_ccp_violation(dv_scene* s, double* out4);
+/* System::getKineticEnergy / getPotentialEnergy (System.cu:1645-1658). */
+DV_API int dv_energies(dv_scene* s, double* kinetic, double* potential);
+/* System::calculateContactForcePerCollision (System.cu:1259-1295): normal and
+ * friction force per contact, 3 doubles each. */
+DV_API int dv_contact_forces_per_collision(dv_scene* s, double* normal, double* friction);
+
+DV_API int dv_get_step_stats(dv_scene* s, dv_step_stats* out);
+DV_API const char* dv_status_string(int status);
+/* Last CUDA error text recorded by the library (thread-local). */
+DV_API const char* dv_last_error(void);
+/* Number of kernel launches issued by this scene so far. */
+DV_API int64_t dv_scene_launch_count(dv_scene* s);
+/* Per-step reports since the last clear, oldest first (the per-step line the
+ * reference prints at System.cu:592 and APGD.cu:351). */
+DV_API int dv_get_step_history(dv_scene* s, dv_step_stats* out, int32_t cap, int32_t* n);
+DV_API int dv_clear_step_history(dv_scene* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DVIDE_H_ */

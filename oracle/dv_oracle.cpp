@@ -1,0 +1,948 @@
+/*
+ * dv_oracle.cpp -- CPU restatement of DVIDE's rigid-body frictional-contact
+ * time step (sphere + fixed/dynamic box bodies, APGD solver).
+ *
+ * TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg, never by the product library.
+ *
+ * PARITY UNPINNED against the reference binary: melanz/DVIDE cannot be built
+ * here (CUSP headers absent) and ships no golden vectors.  This file follows
+ * the reference source, cited by file:line (paths relative to the DVIDE tree):
+ *   state layout ........ src/System.cu:342-424 (p, v, f = m g, Minv = 1/m, 0 if fixed)
+ *   time step ........... src/System.cu:544-583 (DoTimeStep)
+ *   applied impulse ..... src/System.cu:1411-1417, 1502-1514 (k = M v + h f)
+ *   Jacobian frame ...... src/System.cu:753-762, body branches :905-1203
+ *   Schur vector ........ src/System.cu:1516-1524, 1561-1580 (r = D Minv k + b)
+ *   CCP violation ....... src/System.cu:1590-1643
+ *   AABBs / bins ........ src/CollisionDetector.cu:10-110, 547-631
+ *   narrowphase ......... src/CollisionDetector.cu:187-501
+ *   APGD ................ src/APGD.cu:6-361
+ *   vector helpers ...... src/helper_math_double.h:58-61, 555-605, 689-697
+ *                         (length = float sqrtf, normalize = float 1/sqrtf)
+ * Third-party arithmetic: CUSP (version unpinned, CMakeLists.txt:28) supplies
+ * COO SpMV and BLAS-1 in the reference; each call is restated from its
+ * definition (multiply: y = A x; axpby: z = a x + b y; axpy: y = a x + y;
+ * axpbypcz: w = a x + b y + c z; nrm2 = sqrt(sum x^2); nrmmax = max |x|).
+ *
+ * Floating-point conventions shared bit-for-bit with the CUDA kernels:
+ *  - built with -ffp-contract=off: no fused multiply-add anywhere;
+ *  - pow(x, 2.0) is evaluated as x*x;
+ *  - reductions (dot, nrm2) use one fixed tiled order, ordered_sum() below,
+ *    which the GPU reproduces exactly (reduce_mode 0).  reduce_mode 1 sums
+ *    sequentially like CUSP's host backend; spmv_mode 1 applies D and D^T in
+ *    literal COO entry order.  Tests use modes 1/1 to show that the choice of
+ *    summation order moves results far less than the 1e-10 parity bar.
+ *  - the matrix-free product groups D^T x per contact, q_c = F_c x_c with
+ *    q_k = (n_k x0 + u_k x1) + v_k x2, then sums +-q_c over a body's contacts
+ *    in ascending contact order; D w is n.(w_A - w_B) = (n_x d_x + n_y d_y) + n_z d_z.
+ */
+#include "dv_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct V3 {
+  double x, y, z;
+};
+
+inline V3 mk(double x, double y, double z) { return V3{x, y, z}; }
+inline V3 add(V3 a, V3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 sub(V3 a, V3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 scale(V3 a, double s) { return mk(a.x * s, a.y * s, a.z * s); }
+inline V3 neg(V3 a) { return mk(-a.x, -a.y, -a.z); }
+
+/* helper_math_double.h:559-562 */
+inline double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+/* helper_math_double.h:576-579 with the host sqrtf (float) */
+inline double length3(V3 a) { return (double)sqrtf((float)dot3(a, a)); }
+/* helper_math_double.h:594-597 with the host rsqrtf = 1.0f / sqrtf(x) (:58-61) */
+inline V3 normalize3(V3 a) {
+  double inv = (double)(1.0f / sqrtf((float)dot3(a, a)));
+  return scale(a, inv);
+}
+/* helper_math_double.h:692-695 */
+inline V3 cross3(V3 a, V3 b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+/* ---------------------------------------------------------------------
+ * Ordered reduction shared with the GPU.
+ * Items are grouped in tiles of 1024.  In tile t, slot j (0..255) sums
+ * items 1024t + j + 256m for m = 0..3, starting from 0.0; the 256 slots are
+ * folded as 8 warps of 32 by halving strides 16,8,4,2,1 (slot l += slot
+ * l+off), then the 8 warp results by strides 4,2,1.  The tile partials are
+ * folded the same way: slot j sums tiles j, j+256, ... then the 256-tree.
+ * ------------------------------------------------------------------- */
+double tree256(double* s) {
+  double W[8];
+  for (int w = 0; w < 8; ++w) {
+    double* a = s + 32 * w;
+    for (int off = 16; off >= 1; off >>= 1)
+      for (int l = 0; l < off; ++l) a[l] = a[l] + a[l + off];
+    W[w] = a[0];
+  }
+  for (int off = 4; off >= 1; off >>= 1)
+    for (int l = 0; l < off; ++l) W[l] = W[l] + W[l + off];
+  return W[0];
+}
+
+double ordered_sum(const double* v, int64_t n) {
+  if (n <= 0) return 0.0;
+  int64_t T = (n + 1023) / 1024;
+  std::vector<double> P(T);
+#pragma omp parallel for schedule(static)
+  for (int64_t t = 0; t < T; ++t) {
+    double s[256];
+    for (int j = 0; j < 256; ++j) {
+      double acc = 0.0;
+      for (int m = 0; m < 4; ++m) {
+        int64_t i = 1024 * t + j + 256 * m;
+        if (i < n) acc = acc + v[i];
+      }
+      s[j] = acc;
+    }
+    P[t] = tree256(s);
+  }
+  double a[256];
+  for (int j = 0; j < 256; ++j) {
+    double acc = 0.0;
+    for (int64_t t = j; t < T; t += 256) acc = acc + P[t];
+    a[j] = acc;
+  }
+  return tree256(a);
+}
+
+/* APGD.cu:47-78, friction-cone projection of one contact impulse. */
+inline void project3(double* g, double mu) {
+  double gn = g[0];
+  double gt = sqrt(g[1] * g[1] + g[2] * g[2]);
+  double o0, o1, o2;
+  if (mu == 0) {
+    o0 = gn; o1 = 0; o2 = 0;
+    if (gn < 0) { o0 = 0; o1 = 0; o2 = 0; }
+  } else if (gt < mu * gn) {
+    return;
+  } else if ((gt < -(1.0 / mu) * gn) || (fabs(gn) < 10e-15)) {
+    o0 = 0; o1 = 0; o2 = 0;
+  } else {
+    double gnp = (gt * mu + gn) / (mu * mu + 1.0);
+    double gtp = gnp * mu;
+    double ratio = gtp / gt;
+    o0 = gnp; o1 = ratio * g[1]; o2 = ratio * g[2];
+  }
+  g[0] = o0; g[1] = o1; g[2] = o2;
+}
+
+/* System.cu:753-762, tangent frame from the stored normal. */
+inline void frame_from_normal(V3 n, V3* u, V3* v) {
+  V3 uu;
+  if (n.z != 0) {
+    uu = normalize3(mk(1, 0, -n.x / n.z));
+  } else if (n.x != 0) {
+    uu = normalize3(mk(-n.z / n.x, 0, 1));
+  } else {
+    uu = normalize3(mk(1, -n.x / n.y, 0));
+  }
+  *u = uu;
+  *v = normalize3(cross3(n, uu));
+}
+
+struct Scene {
+  or_params P;
+  int nb = 0;
+  std::vector<double> p, v, minv, f, k, fcont, geom;
+  std::vector<int> fixed, family;
+  /* contacts (sorted by (A, B)) */
+  int nc = 0, npossible = 0;
+  std::vector<uint32_t> A, B;
+  std::vector<double> nP, loc, F, r, bst;
+  std::vector<double> gamma;  // warm-start buffer, 3 * capacity
+  int gsize = 0;              // contacts currently held (System.cu:185 starts at nb)
+  /* body incidence, ascending contact order, sign +1 = body A */
+  std::vector<int> incStart, incC;
+  std::vector<signed char> incS;
+  or_stats st;
+  double time = 0;
+  int timeIndex = 0;
+};
+
+/* ------------------------------ reductions ------------------------------ */
+double dotv(const Scene& S, const double* x, const double* y, int nc) {
+  if (S.P.reduce_mode == 1) {
+    double s = 0.0;
+    for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) s = s + x[i] * y[i];
+    return s;
+  }
+  std::vector<double> it(nc);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < nc; ++c) {
+    const double* a = x + 3 * c;
+    const double* b = y + 3 * c;
+    it[c] = (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+  }
+  return ordered_sum(it.data(), nc);
+}
+
+double nrm2v(const Scene& S, const double* x, int nc) { return sqrt(dotv(S, x, x, nc)); }
+
+double nrmmaxv(const double* x, int nc, int* nan_flag) {
+  double m = 0.0;
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) {
+    double a = fabs(x[i]);
+    if (a != a) *nan_flag = 1;
+    if (a > m) m = a;
+  }
+  return m;
+}
+
+/* ------------------------------ collision ------------------------------- */
+struct AabbSet {
+  std::vector<V3> mn, mx;  // shifted by the global origin (CollisionDetector.cu:574)
+};
+
+inline bool is_sphere(const Scene& S, int i) { return S.geom[3 * i + 1] == 0; }
+
+/* CollisionDetector.cu:24-79 (rigid-body branch) and :555-576. */
+void build_aabbs(const Scene& S, AabbSet& a) {
+  int nb = S.nb;
+  a.mn.resize(nb);
+  a.mx.resize(nb);
+  double env = S.P.envelope;
+  for (int i = 0; i < nb; ++i) {
+    V3 g = mk(S.geom[3 * i], S.geom[3 * i + 1], S.geom[3 * i + 2]);
+    if (g.y == 0) g = mk(g.x, g.x, g.x);
+    g = add(g, mk(env, env, env));
+    V3 pos = mk(S.p[3 * i], S.p[3 * i + 1], S.p[3 * i + 2]);
+    a.mn[i] = sub(pos, g);
+    a.mx[i] = add(pos, g);
+  }
+  if (nb == 0) return;
+  V3 lo = a.mn[0], hi = a.mn[0];
+  for (int pass = 0; pass < 2; ++pass) {
+    const std::vector<V3>& pts = pass ? a.mx : a.mn;
+    for (int i = 0; i < nb; ++i) {
+      lo = mk(fmin(lo.x, pts[i].x), fmin(lo.y, pts[i].y), fmin(lo.z, pts[i].z));
+      hi = mk(fmax(hi.x, pts[i].x), fmax(hi.y, pts[i].y), fmax(hi.z, pts[i].z));
+    }
+  }
+  V3 origin = sub(lo, mk(0.01, 0.01, 0.01));
+  for (int i = 0; i < nb; ++i) {
+    a.mn[i] = sub(a.mn[i], origin);
+    a.mx[i] = sub(a.mx[i], origin);
+  }
+}
+
+/* CollisionDetector.cu:112-178: overlap on shifted boxes, identity and family filters. */
+inline bool candidate(const Scene& S, const AabbSet& a, int i, int j) {
+  const V3 &Amn = a.mn[i], &Amx = a.mx[i], &Bmn = a.mn[j], &Bmx = a.mx[j];
+  bool in = (Amn.x <= Bmx.x && Bmn.x <= Amx.x) && (Amn.y <= Bmx.y && Bmn.y <= Amx.y) &&
+            (Amn.z <= Bmx.z && Bmn.z <= Amx.z);
+  if (i == j) in = false;
+  int fa = S.family[i], fb = S.family[j];
+  if (fa == fb && fa != -1) in = false;
+  return in;
+}
+
+struct ContactOut {
+  uint32_t b;
+  V3 nstored;  // -normal (B -> A)
+  double gap;  // -penetration
+  V3 loc;
+};
+
+/* CollisionDetector.cu:187-331 (count) and :333-501 (store), rigid bodies. */
+bool narrowphase(const Scene& S, int ia, int ib, double env, ContactOut* out) {
+  V3 posA = mk(S.p[3 * ia], S.p[3 * ia + 1], S.p[3 * ia + 2]);
+  V3 posB = mk(S.p[3 * ib], S.p[3 * ib + 1], S.p[3 * ib + 2]);
+  V3 gA = mk(S.geom[3 * ia], S.geom[3 * ia + 1], S.geom[3 * ia + 2]);
+  V3 gB = mk(S.geom[3 * ib], S.geom[3 * ib + 1], S.geom[3 * ib + 2]);
+  double pen;
+  V3 normal, location;
+  if (gA.y == 0 && gB.y == 0) {
+    V3 d = sub(posB, posA);
+    pen = (gA.x + gB.x) - length3(d);
+    if (!(pen >= -env)) return false;
+    normal = normalize3(d);
+    location = add(posA, scale(normal, gA.x));
+  } else if ((gA.y != 0 && gB.y == 0) || (gA.y == 0 && gB.y != 0)) {
+    double dmin = 0;
+    double r = gB.x;
+    V3 center = posB;
+    V3 bmin = sub(posA, gA);
+    V3 bmax = add(posA, gA);
+    bool sphereA = (gA.y == 0 && gB.y != 0);
+    if (sphereA) {
+      r = gA.x;
+      center = posA;
+      bmin = sub(posB, gB);
+      bmax = add(posB, gB);
+    }
+    V3 nrm = mk(0, 0, 0);
+    double t;
+    if (center.x < bmin.x) { t = center.x - bmin.x; dmin += t * t; nrm.x = nrm.x + t; }
+    else if (center.x > bmax.x) { t = center.x - bmax.x; dmin += t * t; nrm.x = nrm.x + t; }
+    if (center.y < bmin.y) { t = center.y - bmin.y; dmin += t * t; nrm.y = nrm.y + t; }
+    else if (center.y > bmax.y) { t = center.y - bmax.y; dmin += t * t; nrm.y = nrm.y + t; }
+    if (center.z < bmin.z) { t = center.z - bmin.z; dmin += t * t; nrm.z = nrm.z + t; }
+    else if (center.z > bmax.z) { t = center.z - bmax.z; dmin += t * t; nrm.z = nrm.z + t; }
+    pen = r - sqrt(dmin);
+    if (!(pen >= -env)) return false;
+    normal = normalize3(nrm);
+    location = sub(center, scale(normal, r));
+    if (sphereA) normal = neg(normal);
+  } else {
+    return false;  // box-box is never a contact
+  }
+  out->b = (uint32_t)ib;
+  out->nstored = neg(normal);
+  out->gap = -pen;
+  out->loc = location;
+  return true;
+}
+
+void collide(Scene& S) {
+  int nb = S.nb;
+  AabbSet a;
+  build_aabbs(S, a);
+  double env = S.P.envelope;
+
+  /* Spheres go in a uniform grid keyed on their shifted AABB min corner with
+   * cell size above the largest sphere box; boxes are tested against all
+   * bodies.  The candidate set is exactly the AABB-overlap set of
+   * CollisionDetector.cu:112-178, which does not depend on the binning. */
+  std::vector<int> small, large;
+  double W = 0;
+  for (int i = 0; i < nb; ++i) {
+    if (is_sphere(S, i)) {
+      small.push_back(i);
+      W = std::max(W, a.mx[i].x - a.mn[i].x);
+      W = std::max(W, a.mx[i].y - a.mn[i].y);
+      W = std::max(W, a.mx[i].z - a.mn[i].z);
+    } else {
+      large.push_back(i);
+    }
+  }
+  double w = W * (1.0 + 1e-7) + 1e-300;
+  std::vector<int64_t> ckey(nb, -1);
+  std::vector<int> cx(nb), cy(nb), cz(nb);
+  int mxc[3] = {0, 0, 0};
+  for (int i : small) {
+    cx[i] = (int)floor(a.mn[i].x / w);
+    cy[i] = (int)floor(a.mn[i].y / w);
+    cz[i] = (int)floor(a.mn[i].z / w);
+    mxc[0] = std::max(mxc[0], cx[i]);
+    mxc[1] = std::max(mxc[1], cy[i]);
+    mxc[2] = std::max(mxc[2], cz[i]);
+  }
+  int64_t D0 = mxc[0] + 1, D1 = mxc[1] + 1;
+  std::vector<std::pair<int64_t, int>> cells;
+  cells.reserve(small.size());
+  for (int i : small) {
+    ckey[i] = cx[i] + D0 * (cy[i] + D1 * (int64_t)cz[i]);
+    cells.push_back(std::make_pair(ckey[i], i));
+  }
+  std::sort(cells.begin(), cells.end());
+
+  std::vector<std::vector<ContactOut>> per(nb);
+  std::vector<int> ncand(nb, 0);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int ia = 0; ia < nb; ++ia) {
+    std::vector<int> cand;
+    if (is_sphere(S, ia)) {
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            int x = cx[ia] + dx, y = cy[ia] + dy, z = cz[ia] + dz;
+            if (x < 0 || y < 0 || z < 0 || x >= D0 || y >= D1) continue;
+            int64_t key = x + D0 * (y + D1 * (int64_t)z);
+            auto it = std::lower_bound(cells.begin(), cells.end(), std::make_pair(key, -1));
+            for (; it != cells.end() && it->first == key; ++it) {
+              int jb = it->second;
+              if (jb > ia && candidate(S, a, ia, jb)) cand.push_back(jb);
+            }
+          }
+      for (int jb : large)
+        if (jb > ia && candidate(S, a, ia, jb)) cand.push_back(jb);
+    } else {
+      for (int jb = ia + 1; jb < nb; ++jb)
+        if (candidate(S, a, ia, jb)) cand.push_back(jb);
+    }
+    std::sort(cand.begin(), cand.end());
+    ncand[ia] = (int)cand.size();
+    for (int jb : cand) {
+      ContactOut o;
+      if (narrowphase(S, ia, jb, env, &o)) per[ia].push_back(o);
+    }
+  }
+  int64_t np = 0, nc = 0;
+  for (int i = 0; i < nb; ++i) {
+    np += ncand[i];
+    nc += (int64_t)per[i].size();
+  }
+  S.npossible = (int)np;
+  S.nc = (int)nc;
+  S.A.resize(nc);
+  S.B.resize(nc);
+  S.nP.resize(4 * nc);
+  S.loc.resize(3 * nc);
+  int64_t c = 0;
+  for (int ia = 0; ia < nb; ++ia)
+    for (const ContactOut& o : per[ia]) {
+      S.A[c] = (uint32_t)ia;
+      S.B[c] = o.b;
+      S.nP[4 * c + 0] = o.nstored.x;
+      S.nP[4 * c + 1] = o.nstored.y;
+      S.nP[4 * c + 2] = o.nstored.z;
+      S.nP[4 * c + 3] = o.gap;
+      S.loc[3 * c + 0] = o.loc.x;
+      S.loc[3 * c + 1] = o.loc.y;
+      S.loc[3 * c + 2] = o.loc.z;
+      ++c;
+    }
+  S.st.num_contacts = S.nc;
+  S.st.num_possible = S.npossible;
+}
+
+/* System.cu:676-1257 (rigid-body branches): frames, b = gap / h (:1516-1524). */
+void build_frames(Scene& S) {
+  int nc = S.nc;
+  S.F.resize(9 * (size_t)nc);
+  S.bst.resize(3 * (size_t)nc);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < nc; ++c) {
+    V3 n = mk(S.nP[4 * c], S.nP[4 * c + 1], S.nP[4 * c + 2]);
+    V3 u, v;
+    frame_from_normal(n, &u, &v);
+    double* F = &S.F[9 * (size_t)c];
+    F[0] = n.x; F[1] = n.y; F[2] = n.z;
+    F[3] = u.x; F[4] = u.y; F[5] = u.z;
+    F[6] = v.x; F[7] = v.y; F[8] = v.z;
+    S.bst[3 * c + 0] = S.nP[4 * c + 3] / S.P.h;
+    S.bst[3 * c + 1] = 0;
+    S.bst[3 * c + 2] = 0;
+  }
+  /* incidence in ascending contact order (the row order of sort_by_row(D^T),
+   * System.cu:1388-1409) */
+  int nb = S.nb;
+  std::vector<int> cnt(nb + 1, 0);
+  for (int c = 0; c < nc; ++c) {
+    cnt[S.A[c] + 1]++;
+    cnt[S.B[c] + 1]++;
+  }
+  for (int i = 0; i < nb; ++i) cnt[i + 1] += cnt[i];
+  S.incStart = cnt;
+  S.incC.assign(2 * (size_t)nc, 0);
+  S.incS.assign(2 * (size_t)nc, 0);
+  std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+  for (int c = 0; c < nc; ++c) {
+    int b = S.B[c], a = S.A[c];
+    S.incC[pos[b]] = c; S.incS[pos[b]] = -1; pos[b]++;
+    S.incC[pos[a]] = c; S.incS[pos[a]] = +1; pos[a]++;
+  }
+}
+
+/* D^T x (one value per body DOF). */
+void apply_DT(const Scene& S, const double* x, double* out) {
+  int nb = S.nb;
+  if (S.P.spmv_mode == 1) {
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < nb; ++b) {
+      for (int k = 0; k < 3; ++k) {
+        double y = 0.0;
+        for (int e = S.incStart[b]; e < S.incStart[b + 1]; ++e) {
+          int c = S.incC[e];
+          double s = S.incS[e];
+          const double* F = &S.F[9 * (size_t)c];
+          y = y + (s * F[k]) * x[3 * c];
+          y = y + (s * F[3 + k]) * x[3 * c + 1];
+          y = y + (s * F[6 + k]) * x[3 * c + 2];
+        }
+        out[3 * b + k] = y;
+      }
+    }
+    return;
+  }
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; ++b) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int e = S.incStart[b]; e < S.incStart[b + 1]; ++e) {
+      int c = S.incC[e];
+      const double* F = &S.F[9 * (size_t)c];
+      const double* xc = x + 3 * c;
+      for (int k = 0; k < 3; ++k) {
+        double q = (F[k] * xc[0] + F[3 + k] * xc[1]) + F[6 + k] * xc[2];
+        if (S.incS[e] > 0) acc[k] = acc[k] + q;
+        else acc[k] = acc[k] - q;
+      }
+    }
+    out[3 * b] = acc[0];
+    out[3 * b + 1] = acc[1];
+    out[3 * b + 2] = acc[2];
+  }
+}
+
+/* D w (one value per contact row). */
+void apply_D(const Scene& S, const double* w, double* out) {
+  int nc = S.nc;
+  if (S.P.spmv_mode == 1) {
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nc; ++c) {
+      const double* F = &S.F[9 * (size_t)c];
+      const double* wa = w + 3 * (size_t)S.A[c];
+      const double* wb = w + 3 * (size_t)S.B[c];
+      for (int row = 0; row < 3; ++row) {
+        const double* f = F + 3 * row;
+        double y = 0.0;
+        y = y + f[0] * wa[0];
+        y = y + f[1] * wa[1];
+        y = y + f[2] * wa[2];
+        y = y + (-f[0]) * wb[0];
+        y = y + (-f[1]) * wb[1];
+        y = y + (-f[2]) * wb[2];
+        out[3 * c + row] = y;
+      }
+    }
+    return;
+  }
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < nc; ++c) {
+    const double* F = &S.F[9 * (size_t)c];
+    const double* wa = w + 3 * (size_t)S.A[c];
+    const double* wb = w + 3 * (size_t)S.B[c];
+    double d0 = wa[0] - wb[0], d1 = wa[1] - wb[1], d2 = wa[2] - wb[2];
+    for (int row = 0; row < 3; ++row) {
+      const double* f = F + 3 * row;
+      out[3 * c + row] = (f[0] * d0 + f[1] * d1) + f[2] * d2;
+    }
+  }
+}
+
+/* APGD.cu:81-87: gammaTmp = D (Minv (D^T x)). */
+void schur(const Scene& S, const double* x, double* out, std::vector<double>& bodytmp) {
+  bodytmp.resize(3 * (size_t)S.nb);
+  apply_DT(S, x, bodytmp.data());
+  for (size_t i = 0; i < bodytmp.size(); ++i) bodytmp[i] = S.minv[i] * bodytmp[i];
+  apply_D(S, bodytmp.data(), out);
+}
+
+/* APGD.cu:90-102 */
+double get_residual(const Scene& S, const double* src, std::vector<double>& T,
+                    std::vector<double>& bt, int* nan_flag) {
+  int nc = S.nc;
+  double gdiff = 1.0 / ((double)nc * (double)nc);
+  schur(S, src, T.data(), bt);
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = S.r[i] + T[i];
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = src[i] + (-gdiff) * T[i];
+  for (int c = 0; c < nc; ++c) project3(&T[3 * c], S.P.mu);
+  double a = 1.0 / gdiff, b = -1.0 / gdiff;
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = a * src[i] + b * T[i];
+  return nrmmaxv(T.data(), nc, nan_flag);
+}
+
+/* APGD.cu:164-361 */
+void apgd_solve(Scene& S) {
+  int nc = S.nc;
+  int64_t n3 = 3 * (int64_t)nc;
+  /* thrust resize keeps the prefix and zero-fills growth (APGD.cu:166). */
+  if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
+  if (S.gsize < nc)
+    for (int64_t i = 3 * (int64_t)S.gsize; i < n3; ++i) S.gamma[i] = 0.0;
+  S.gsize = nc;
+  double* gamma = S.gamma.data();
+  std::vector<double> gHat(n3, 1.0), gNew(n3), g(n3), y(n3), yNew(n3), T(n3), bt;
+  if (!S.P.warm_start)
+    for (int c = 0; c < nc; ++c) { gamma[3 * c] = 1.0; gamma[3 * c + 1] = 0.0; gamma[3 * c + 2] = 0.0; }
+  for (int64_t i = 0; i < n3; ++i) y[i] = gamma[i];
+
+  double theta = 1.0, thetaNew = theta, Beta = 0.0, obj1 = 0.0, obj2 = 0.0;
+  double residual = 10e30;
+  int nan_flag = 0, status = 0, backtracks = 0;
+  double t;
+  double L;
+  for (int64_t i = 0; i < n3; ++i) T[i] = gamma[i] + (-1.0) * gHat[i];
+  L = nrm2v(S, T.data(), nc);
+  schur(S, T.data(), T.data(), bt);
+  L = nrm2v(S, T.data(), nc) / L;
+  t = 1.0 / L;
+  int k;
+  const double mu = S.P.mu;
+  for (k = 0; k < S.P.max_iterations; ++k) {
+    schur(S, y.data(), T.data(), bt);
+    for (int64_t i = 0; i < n3; ++i) g[i] = T[i] + S.r[i];
+    for (int64_t i = 0; i < n3; ++i) gNew[i] = y[i] + (-t) * g[i];
+    for (int c = 0; c < nc; ++c) project3(&gNew[3 * c], mu);
+    schur(S, gNew.data(), T.data(), bt);
+    obj1 = 0.5 * dotv(S, gNew.data(), T.data(), nc) + dotv(S, gNew.data(), S.r.data(), nc);
+    schur(S, y.data(), T.data(), bt);
+    obj2 = 0.5 * dotv(S, y.data(), T.data(), nc) + dotv(S, y.data(), S.r.data(), nc);
+    for (int64_t i = 0; i < n3; ++i) T[i] = gNew[i] + (-1.0) * y[i];
+    {
+      double nr = nrm2v(S, T.data(), nc);
+      obj2 += dotv(S, g.data(), T.data(), nc) + 0.5 * L * (nr * nr);
+    }
+    while (obj1 >= obj2) {
+      if (backtracks >= S.P.max_backtracks) { status = 3; break; }
+      ++backtracks;
+      L = 2.0 * L;
+      t = 1.0 / L;
+      for (int64_t i = 0; i < n3; ++i) gNew[i] = y[i] + (-t) * g[i];
+      for (int c = 0; c < nc; ++c) project3(&gNew[3 * c], mu);
+      schur(S, gNew.data(), T.data(), bt);
+      obj1 = 0.5 * dotv(S, gNew.data(), T.data(), nc) + dotv(S, gNew.data(), S.r.data(), nc);
+      schur(S, y.data(), T.data(), bt);
+      obj2 = 0.5 * dotv(S, y.data(), T.data(), nc) + dotv(S, y.data(), S.r.data(), nc);
+      for (int64_t i = 0; i < n3; ++i) T[i] = gNew[i] + (-1.0) * y[i];
+      double nr = nrm2v(S, T.data(), nc);
+      obj2 += dotv(S, g.data(), T.data(), nc) + 0.5 * L * (nr * nr);
+    }
+    if (status) break;
+    thetaNew = (-(theta * theta) + theta * sqrt(theta * theta + 4.0)) / 2.0;
+    Beta = theta * (1.0 - theta) / (theta * theta + thetaNew);
+    for (int64_t i = 0; i < n3; ++i) yNew[i] = (1.0 + Beta) * gNew[i] + (-Beta) * gamma[i];
+    double res = get_residual(S, gNew.data(), T, bt, &nan_flag);
+    if (res < residual) {
+      residual = res;
+      for (int64_t i = 0; i < n3; ++i) gHat[i] = gNew[i];
+    }
+    if (residual < S.P.tolerance) break;
+    for (int64_t i = 0; i < n3; ++i) T[i] = gNew[i] + (-1.0) * gamma[i];
+    if (dotv(S, g.data(), T.data(), nc) > 0) {
+      for (int64_t i = 0; i < n3; ++i) yNew[i] = gNew[i];
+      thetaNew = 1.0;
+    }
+    L = 0.9 * L;
+    t = 1.0 / L;
+    theta = thetaNew;
+    for (int64_t i = 0; i < n3; ++i) gamma[i] = gNew[i];
+    for (int64_t i = 0; i < n3; ++i) y[i] = yNew[i];
+  }
+  /* APGD.cu:353-354 */
+  schur(S, gHat.data(), T.data(), bt);
+  double objective = 0.5 * dotv(S, gHat.data(), T.data(), nc) + dotv(S, gHat.data(), S.r.data(), nc);
+  for (int64_t i = 0; i < n3; ++i) gamma[i] = gHat[i];
+  S.st.iterations = k;
+  S.st.backtracks = backtracks;
+  S.st.residual = residual;
+  S.st.objective = objective;
+  if (nan_flag || obj1 != obj1) status = status ? status : 2;
+  S.st.status = status;
+}
+
+void build_k(Scene& S) {
+  int n = 3 * S.nb;
+  double h = S.P.h;
+  for (int i = 0; i < n; ++i) {
+    double m = S.minv[i];
+    if (m) m = 1.0 / m;
+    double kk = m * S.v[i];
+    S.k[i] = h * S.f[i] + kk;
+  }
+}
+
+void build_r(Scene& S) {
+  int nb = S.nb, nc = S.nc;
+  std::vector<double> tmp(3 * (size_t)nb);
+  for (int i = 0; i < 3 * nb; ++i) tmp[i] = S.minv[i] * S.k[i];
+  S.r.assign(3 * (size_t)nc, 0.0);
+  apply_D(S, tmp.data(), S.r.data());
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) S.r[i] = S.bst[i] + S.r[i];
+}
+
+int do_step(Scene& S) {
+  S.st.status = 0;
+  S.st.iterations = 0;
+  S.st.backtracks = 0;
+  S.st.residual = 0;
+  S.st.objective = 0;
+  collide(S);
+  build_k(S);
+  int n = 3 * S.nb;
+  double h = S.P.h;
+  if (S.nc) {
+    build_frames(S);
+    build_r(S);
+    apgd_solve(S);
+    std::vector<double> fc(n);
+    apply_DT(S, S.gamma.data(), fc.data());
+    for (int i = 0; i < n; ++i) {
+      double tmp = S.k[i] + fc[i];
+      S.v[i] = S.minv[i] * tmp;
+      S.fcont[i] = (1.0 / h) * fc[i];
+    }
+  } else {
+    S.F.clear();
+    S.r.clear();
+    S.bst.clear();
+    S.incStart.assign(S.nb + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      S.v[i] = S.minv[i] * S.k[i];
+      S.fcont[i] = 0.0;
+    }
+  }
+  for (int i = 0; i < n; ++i) S.p[i] = h * S.v[i] + S.p[i];
+  S.time += h;
+  S.timeIndex++;
+  S.st.gamma_size = S.gsize;
+  return S.st.status;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* or_create(int nb, const double* pos, const double* vel, const double* mass,
+                const double* geom, const int* fixed, const int* family,
+                const or_params* prm) {
+  Scene* S = new Scene();
+  S->P = *prm;
+  S->nb = nb;
+  S->p.assign(pos, pos + 3 * (size_t)nb);
+  S->v.assign(vel, vel + 3 * (size_t)nb);
+  S->geom.assign(geom, geom + 3 * (size_t)nb);
+  S->fixed.assign(fixed, fixed + nb);
+  S->family.assign(family, family + nb);
+  S->minv.resize(3 * (size_t)nb);
+  S->f.resize(3 * (size_t)nb);
+  S->k.assign(3 * (size_t)nb, 0.0);
+  S->fcont.assign(3 * (size_t)nb, 0.0);
+  for (int i = 0; i < nb; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      /* System.cu:368-376, 409-417 */
+      S->f[3 * i + d] = fixed[i] ? 0.0 : mass[i] * prm->gravity[d];
+      S->minv[3 * i + d] = fixed[i] ? 0.0 : 1.0 / mass[i];
+    }
+  }
+  /* gamma_d = a_h: 3 nb zeros (System.cu:185) */
+  S->gamma.assign(3 * (size_t)nb, 0.0);
+  S->gsize = nb;
+  memset(&S->st, 0, sizeof(S->st));
+#ifdef _OPENMP
+  if (prm->threads > 0) omp_set_num_threads(prm->threads);
+#endif
+  return S;
+}
+
+void or_destroy(void* s) { delete (Scene*)s; }
+
+int or_set_params(void* s, const or_params* prm) {
+  Scene* S = (Scene*)s;
+  S->P = *prm;
+#ifdef _OPENMP
+  if (prm->threads > 0) omp_set_num_threads(prm->threads);
+#endif
+  return 0;
+}
+
+int or_step(void* s, int nsteps) {
+  Scene* S = (Scene*)s;
+  int st = 0;
+  for (int i = 0; i < nsteps; ++i) {
+    st = do_step(*S);
+    if (st) break;
+  }
+  return st;
+}
+
+int or_collide(void* s) {
+  Scene* S = (Scene*)s;
+  collide(*S);
+  if (S->nc) build_frames(*S);
+  return 0;
+}
+
+int or_get_stats(void* s, or_stats* out) {
+  Scene* S = (Scene*)s;
+  *out = S->st;
+  out->num_contacts = S->nc;
+  out->num_possible = S->npossible;
+  out->gamma_size = S->gsize;
+  return 0;
+}
+
+int or_get_state(void* s, double* p, double* v) {
+  Scene* S = (Scene*)s;
+  if (p) memcpy(p, S->p.data(), sizeof(double) * 3 * S->nb);
+  if (v) memcpy(v, S->v.data(), sizeof(double) * 3 * S->nb);
+  return 0;
+}
+
+int or_set_state(void* s, const double* p, const double* v) {
+  Scene* S = (Scene*)s;
+  if (p) memcpy(S->p.data(), p, sizeof(double) * 3 * S->nb);
+  if (v) memcpy(S->v.data(), v, sizeof(double) * 3 * S->nb);
+  return 0;
+}
+
+int or_get_fcontact(void* s, double* f) {
+  Scene* S = (Scene*)s;
+  memcpy(f, S->fcont.data(), sizeof(double) * 3 * S->nb);
+  return 0;
+}
+
+int or_get_gamma(void* s, double* gamma, int cap) {
+  Scene* S = (Scene*)s;
+  int n = std::min(cap, S->gsize);
+  if (gamma && n > 0) memcpy(gamma, S->gamma.data(), sizeof(double) * 3 * (size_t)n);
+  return S->gsize;
+}
+
+int or_set_gamma(void* s, const double* gamma, int ncont) {
+  Scene* S = (Scene*)s;
+  if ((int64_t)S->gamma.size() < 3 * (int64_t)ncont) S->gamma.resize(3 * (size_t)ncont, 0.0);
+  if (ncont > 0) memcpy(S->gamma.data(), gamma, sizeof(double) * 3 * (size_t)ncont);
+  S->gsize = ncont;
+  return 0;
+}
+
+int or_get_contacts(void* s, uint32_t* a, uint32_t* b, double* nP, double* loc) {
+  Scene* S = (Scene*)s;
+  int nc = S->nc;
+  if (a) memcpy(a, S->A.data(), sizeof(uint32_t) * nc);
+  if (b) memcpy(b, S->B.data(), sizeof(uint32_t) * nc);
+  if (nP) memcpy(nP, S->nP.data(), sizeof(double) * 4 * (size_t)nc);
+  if (loc) memcpy(loc, S->loc.data(), sizeof(double) * 3 * (size_t)nc);
+  return nc;
+}
+
+int or_get_frames(void* s, double* F) {
+  Scene* S = (Scene*)s;
+  if ((int64_t)S->F.size() != 9 * (int64_t)S->nc) return -1;
+  memcpy(F, S->F.data(), sizeof(double) * S->F.size());
+  return S->nc;
+}
+
+int or_get_r(void* s, double* r) {
+  Scene* S = (Scene*)s;
+  if ((int64_t)S->r.size() != 3 * (int64_t)S->nc) return -1;
+  memcpy(r, S->r.data(), sizeof(double) * S->r.size());
+  return S->nc;
+}
+
+/* System.cu:1590-1643 */
+int or_ccp_violation(void* s, double* out4) {
+  Scene* S = (Scene*)s;
+  out4[0] = out4[1] = out4[2] = out4[3] = 0.0;
+  int nc = S->nc;
+  if (!nc) return 0;
+  const double* gm = S->gamma.data();
+  double x = gm[0];
+  for (int c = 1; c < nc; ++c) x = std::min(x, gm[3 * c]);
+  if (x > 0) x = 0;
+  std::vector<double> tg(3 * (size_t)nc);
+  apply_D(*S, S->v.data(), tg.data());
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) tg[i] = S->bst[i] + tg[i];
+  double y = tg[0];
+  for (int c = 1; c < nc; ++c) y = std::min(y, tg[3 * c]);
+  if (y > 0) y = 0;
+  std::vector<double> it(nc);
+  for (int c = 0; c < nc; ++c) it[c] = gm[3 * c] * tg[3 * c];
+  double z;
+  if (S->P.reduce_mode == 1) {
+    z = 0.0;
+    for (int c = 0; c < nc; ++c) z = z + it[c];
+  } else {
+    z = ordered_sum(it.data(), nc);
+  }
+  for (int c = 0; c < nc; ++c) {
+    double gt = sqrt(gm[3 * c + 1] * gm[3 * c + 1] + gm[3 * c + 2] * gm[3 * c + 2]);
+    double cv = S->P.mu * gm[3 * c] - gt;
+    if (cv > 0) cv = 0;
+    it[c] = cv * cv;
+  }
+  double w2;
+  if (S->P.reduce_mode == 1) {
+    w2 = 0.0;
+    for (int c = 0; c < nc; ++c) w2 = w2 + it[c];
+  } else {
+    w2 = ordered_sum(it.data(), nc);
+  }
+  out4[0] = x;
+  out4[1] = y;
+  out4[2] = z;
+  out4[3] = sqrt(w2);
+  return 0;
+}
+
+/* System.cu:1645-1658 */
+double or_kinetic_energy(void* s) {
+  Scene* S = (Scene*)s;
+  std::vector<double> it(S->nb);
+  for (int b = 0; b < S->nb; ++b) {
+    double a[3];
+    for (int d = 0; d < 3; ++d) {
+      double m = S->minv[3 * b + d];
+      if (m) m = 1.0 / m;
+      a[d] = S->v[3 * b + d] * (m * S->v[3 * b + d]);
+    }
+    it[b] = (a[0] + a[1]) + a[2];
+  }
+  return 0.5 * ordered_sum(it.data(), S->nb);
+}
+
+double or_potential_energy(void* s) {
+  Scene* S = (Scene*)s;
+  std::vector<double> it(S->nb);
+  for (int b = 0; b < S->nb; ++b)
+    it[b] = (S->f[3 * b] * S->p[3 * b] + S->f[3 * b + 1] * S->p[3 * b + 1]) + S->f[3 * b + 2] * S->p[3 * b + 2];
+  return -ordered_sum(it.data(), S->nb);
+}
+
+void or_project(double* x3, double mu) { project3(x3, mu); }
+
+void or_frame(const double* n3, double* u3, double* v3) {
+  V3 u, v;
+  frame_from_normal(mk(n3[0], n3[1], n3[2]), &u, &v);
+  u3[0] = u.x; u3[1] = u.y; u3[2] = u.z;
+  v3[0] = v.x; v3[1] = v.y; v3[2] = v.z;
+}
+
+double or_length3(const double* v3) { return length3(mk(v3[0], v3[1], v3[2])); }
+
+void or_normalize3(const double* v3, double* out3) {
+  V3 r = normalize3(mk(v3[0], v3[1], v3[2]));
+  out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
+}
+
+double or_ordered_sum(const double* v, int64_t n) { return ordered_sum(v, n); }
+
+void or_schur(int nb, int nc, const uint32_t* a, const uint32_t* b, const double* F,
+              const double* minv, const double* x, double* out, int spmv_mode) {
+  Scene S;
+  S.nb = nb;
+  S.nc = nc;
+  S.P.spmv_mode = spmv_mode;
+  S.A.assign(a, a + nc);
+  S.B.assign(b, b + nc);
+  S.F.assign(F, F + 9 * (size_t)nc);
+  S.minv.assign(minv, minv + 3 * (size_t)nb);
+  S.nP.assign(4 * (size_t)nc, 0.0);
+  for (int c = 0; c < nc; ++c)
+    for (int d = 0; d < 3; ++d) S.nP[4 * c + d] = F[9 * (size_t)c + d];
+  S.P.h = 1.0;
+  /* incidence only */
+  std::vector<int> cnt(nb + 1, 0);
+  for (int c = 0; c < nc; ++c) { cnt[a[c] + 1]++; cnt[b[c] + 1]++; }
+  for (int i = 0; i < nb; ++i) cnt[i + 1] += cnt[i];
+  S.incStart = cnt;
+  S.incC.assign(2 * (size_t)nc, 0);
+  S.incS.assign(2 * (size_t)nc, 0);
+  std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+  for (int c = 0; c < nc; ++c) {
+    S.incC[pos[b[c]]] = c; S.incS[pos[b[c]]] = -1; pos[b[c]]++;
+    S.incC[pos[a[c]]] = c; S.incS[pos[a[c]]] = +1; pos[a[c]]++;
+  }
+  std::vector<double> bt;
+  schur(S, x, out, bt);
+}
+
+}  // extern "C"

@@ -1,0 +1,227 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bar: bit-exact for the contact list (ids, normal, gap, location, frame) and,
+because both sides share one floating-point order, bit-exact for the FP64
+solve too (gamma, v, p, contact forces, iteration count, residual); the
+north-star tolerance (1e-10 relative on gamma and v) is asserted as well so a
+failure reports its size."""
+import numpy as np
+import pytest
+
+from dvide_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-10  # plain FP64 parity bar on gamma and body velocities
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    d = np.linalg.norm(a - b)
+    n = np.linalg.norm(b)
+    return d / n if n > 0 else d
+
+
+def _pair(native, oracle_mod, sc, **kw):
+    g = native.NativeScene.from_scene(sc, **kw)
+    o = oracle_mod.OracleScene(sc)
+    if kw:
+        o.params = oracle_mod.make_params({**sc.params, **kw})
+        oracle_mod.lib().or_set_params(o.h, o.params)
+    return g, o
+
+
+def _compare_contacts(g, o):
+    ga, gb, gnP, gloc = g.contacts()
+    oa, ob, onP, oloc = o.contacts()
+    assert np.array_equal(ga, oa) and np.array_equal(gb, ob)
+    assert np.array_equal(gnP, onP)
+    assert np.array_equal(gloc, oloc)
+    return ga.size
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 4])
+def test_collide_bitexact(native, oracle_mod, seed):
+    sc = scenes.random_cluster(seed, n=60)
+    g, o = _pair(native, oracle_mod, sc)
+    g.collide()
+    o.collide()
+    nc = _compare_contacts(g, o)
+    assert nc > 20
+    assert np.array_equal(g.frames(), o.frames())
+    assert g.num_contacts()[1] == o.stats()["num_possible"]
+
+
+def test_collide_settling_box_bitexact(native, oracle_mod):
+    sc = scenes.settling_box()
+    g, o = _pair(native, oracle_mod, sc)
+    # squeeze the lattice so that many neighbours are in contact
+    p = sc.pos.copy()
+    p[5:, :2] *= 0.905
+    p[5:, 2] = 0.05 + (p[5:, 2] - 0.06) * 0.905
+    g.set_state(p, sc.vel)
+    o.set_state(p, sc.vel)
+    g.collide()
+    o.collide()
+    nc = _compare_contacts(g, o)
+    assert nc > 1000
+
+
+def _teacher_forced(native, oracle_mod, sc, steps, check_every=1, **kw):
+    g, o = _pair(native, oracle_mod, sc, **kw)
+    worst = 0.0
+    solved = 0
+    for k in range(steps):
+        p, v = o.state()
+        g.set_state(p, v)
+        g.set_gamma(o.gamma())
+        o.step(1)
+        g.step(1)
+        so, sg = o.stats(), g.stats()
+        assert sg["num_contacts"] == so["num_contacts"], k
+        if k % check_every:
+            continue
+        pg, vg = g.state()
+        po, vo = o.state()
+        gg, go = g.gamma(), o.gamma()
+        assert _rel(gg, go) <= REL_TOL and _rel(vg, vo) <= REL_TOL, k
+        assert np.array_equal(gg, go), (k, _rel(gg, go))
+        assert np.array_equal(vg, vo), k
+        assert np.array_equal(pg, po), k
+        assert np.array_equal(g.fcontact(), o.fcontact()), k
+        if so["num_contacts"]:
+            solved += 1
+            assert sg["iterations"] == so["iterations"], k
+            assert sg["residual"] == so["residual"], k
+            assert sg["objective"] == so["objective"], k
+            assert sg["backtracks"] == so["backtracks"], k
+        worst = max(worst, _rel(gg, go))
+    return solved
+
+
+def test_ball_on_ground_bitexact(native, oracle_mod):
+    sc = scenes.ball_on_ground()
+    assert _teacher_forced(native, oracle_mod, sc, 5) == 5
+
+
+@pytest.mark.parametrize("seed", [0, 3])
+def test_cluster_teacher_forced(native, oracle_mod, seed):
+    sc = scenes.random_cluster(seed, n=40)
+    assert _teacher_forced(native, oracle_mod, sc, 12) >= 10
+
+
+def test_cluster_no_warm_start_and_frictionless(native, oracle_mod):
+    sc = scenes.random_cluster(11, n=30, warm_start=0)
+    assert _teacher_forced(native, oracle_mod, sc, 4) >= 3
+    sc = scenes.random_cluster(12, n=30, mu=0.0)
+    assert _teacher_forced(native, oracle_mod, sc, 4) >= 3
+
+
+def test_settling_box_free_running_identical(native, oracle_mod):
+    """A 216-sphere settling box run free for 150 steps stays bit-identical."""
+    sc = scenes.settling_box(n_side=6, max_iterations=300)
+    g, o = _pair(native, oracle_mod, sc)
+    for k in range(150):
+        o.step(1)
+        g.step(1)
+        assert g.stats()["num_contacts"] == o.stats()["num_contacts"], k
+    pg, vg = g.state()
+    po, vo = o.state()
+    assert np.array_equal(pg, po) and np.array_equal(vg, vo)
+    assert np.array_equal(g.gamma(), o.gamma())
+    assert np.array_equal(g.ccp_violation(), o.ccp_violation())
+    ke, pe = g.energies()
+    assert ke == o.kinetic_energy() and pe == o.potential_energy()
+    hist = g.history()
+    assert len(hist) == 150
+
+
+def test_c0_settling_teacher_forced(native, oracle_mod):
+    """The 1,000-sphere settling box: bit-exact per step once the pile is in
+    contact (states taken from the oracle's own trajectory)."""
+    sc = scenes.settling_box()
+    o = oracle_mod.OracleScene(sc)
+    o.step(60)   # spheres reach the floor / each other
+    p, v = o.state()
+    sc2 = sc.copy()
+    sc2.pos, sc2.vel = p, v
+    g, o2 = _pair(native, oracle_mod, sc2)
+    o2.set_gamma(o.gamma())
+    assert _teacher_forced_from(native, g, o2, 8) >= 6
+
+
+def _teacher_forced_from(native, g, o, steps):
+    solved = 0
+    for k in range(steps):
+        p, v = o.state()
+        g.set_state(p, v)
+        g.set_gamma(o.gamma())
+        o.step(1)
+        g.step(1)
+        so, sg = o.stats(), g.stats()
+        assert sg["num_contacts"] == so["num_contacts"]
+        assert np.array_equal(g.gamma(), o.gamma()), k
+        pg, vg = g.state()
+        po, vo = o.state()
+        assert np.array_equal(vg, vo) and np.array_equal(pg, po), k
+        if so["num_contacts"]:
+            solved += 1
+            assert sg["iterations"] == so["iterations"]
+    return solved
+
+
+def test_positional_warm_start(native, oracle_mod):
+    """gamma_d is resized positionally: the prefix survives, growth is zero
+    (APGD.cu:166); a step without contacts leaves it untouched."""
+    sc = scenes.random_cluster(21, n=30)
+    g, o = _pair(native, oracle_mod, sc)
+    g.step(2)
+    o.step(2)
+    n0 = g.gamma().shape[0]
+    # shrink the buffer, then grow back through the next solve
+    short = o.gamma()[: max(1, n0 // 3)] * 0.5
+    g.set_gamma(short)
+    o.set_gamma(short)
+    g.step(1)
+    o.step(1)
+    assert np.array_equal(g.gamma(), o.gamma())
+    # lift every sphere out of contact: no solve, gamma unchanged
+    p, v = o.state()
+    p2 = p.copy()
+    p2[sc.fixed == 0, 2] += 5.0
+    before = o.gamma()
+    g.set_state(p2, v)
+    o.set_state(p2, v)
+    g.step(1)
+    o.step(1)
+    assert g.stats()["num_contacts"] == 0
+    assert np.array_equal(g.gamma(), before) and np.array_equal(o.gamma(), before)
+
+
+def test_contact_force_outputs(native, oracle_mod):
+    sc = scenes.random_cluster(8, n=30)
+    g, o = _pair(native, oracle_mod, sc)
+    g.step(3)
+    o.step(3)
+    n, f = g.contact_forces()
+    F = o.frames()
+    gam = o.gamma()
+    h = sc.params["h"]
+    assert np.array_equal(n, (gam[:, :1] * F[:, 0:3]) / h)
+    assert np.allclose(f, (gam[:, 1:2] * F[:, 3:6] + gam[:, 2:3] * F[:, 6:9]) / h, rtol=0,
+                       atol=1e-12)
+    assert np.array_equal(g.r(), o.r())
+
+
+def test_repeatable_bits(native):
+    """Two runs of the same scene give identical bits (no atomics in any
+    floating-point reduction)."""
+    sc = scenes.settling_box(n_side=5, max_iterations=200)
+    out = []
+    for _ in range(2):
+        g = native.NativeScene.from_scene(sc)
+        g.step(80)
+        out.append(g.state() + (g.gamma(),))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
