@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Contact-steps/s of the DVIDE rigid-body contact step on B200.
+
+Workload (default): the 200,000-sphere column at rest (about 7.3e5 contacts
+per step; r ~ U[0.004, 0.006] m, rho 2500, mu 0.3, h 5e-4, APGD tolerance 1e-4,
+at most 500 iterations, warm start, plain FP64), loaded from
+dvide_b200/data/column_settled.npz.  A step is one System::DoTimeStep:
+collision detection, APGD solve, velocity/position update.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: W untimed steps, then K steps timed with CUDA events on the stream
+the library launches on (barrier + synchronize on both sides, max over ranks);
+value = contacts summed over the K steps and all ranks / time.  e2e repeats
+K steps through the host-buffer API (state copied in from pinned memory and
+back out every step).  Under torchrun every rank runs its own replica of the
+scene (no collective on the data path).
+Reference arm (--impl reference): the CPU restatement of the reference's
+algorithm (oracle/, OpenMP over all host cores) on the same state and
+configuration; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+# Compulsory FP64 bytes (structure of arrays, each array touched once):
+#   one Schur product N x ........ 136 nc + 60 nb
+#   one APGD iteration ........... 440 nc + 120 nb  (two products + vector streams)
+#   per extra backtrack .......... one product
+#   per step outside the loop .... setup (k, r, the Lipschitz estimate: 2 products),
+#                                  final D^T gamma and update: 136 nc + 96 nb
+def solve_bytes(nc, nb, sweeps, backtracks):
+    bN = 136 * nc + 60 * nb
+    return sweeps * (440 * nc + 120 * nb) + backtracks * bN + 2 * bN + (136 * nc + 96 * nb)
+
+
+# DRAM bytes per algorithmic byte of the solve kernel, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on a 50-iteration launch of the
+# current kernel version on this workload; the full launch is scaled by it.
+TRAFFIC_PER_ALGORITHMIC_BYTE = 21.56 / 18.68
+
+
+def collide_bytes(nc, nb, npossible):
+    return 24 * nb + 4 * 16 * nb + 8 * npossible + 8 * npossible + 48 * npossible + nc * (8 + 32 + 72)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def load_workload(name):
+    from dvide_b200 import scenes, workloads
+    if name == "column":
+        sc = workloads.column_settled()
+        desc = ("column_settled: 200000 spheres r~U[0.004,0.006] rho 2500 mu 0.3 h 5e-4 "
+                "tol 1e-4 maxIter 500 warm start, FP64")
+    elif name == "settling":
+        sc = scenes.settling_box()
+        desc = "settling_box: 1000 spheres r 0.05 rho 2600 mu 0.25 h 1e-3 tol 1e-4 maxIter 1000"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return sc, desc
+
+
+def run_reference(args, sc, desc):
+    """The reference's algorithm on the host cores (oracle/), same state and config."""
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    o = O.OracleScene(sc, threads=threads)
+    budget = args.ref_budget_s
+    warm = 1 if args.warmup > 0 else 0
+    t0 = time.perf_counter()
+    o.step(warm)
+    t_warm = time.perf_counter() - t0
+    contacts = 0
+    done = 0
+    t0 = time.perf_counter()
+    while done < args.steps:
+        o.step(1)
+        contacts += o.stats()["num_contacts"]
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    value = contacts / dt
+    sample = (f"{done} of {args.steps} full time steps after {warm} warm-up step "
+              f"({t_warm:.1f} s), {threads} OpenMP threads, oracle port of APGD/System")
+    return {"metric": "contact-steps/s", "value": value, "unit": "contact-steps/s",
+            "impl": "reference", "n_gpus": 0, "steps": done, "warmup": warm,
+            "ms_per_step": 1e3 * dt / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc},
+            "cpu_baseline": {"value": value, "unit": "contact-steps/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "contact-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline_sample(sc, budget_s):
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    o = O.OracleScene(sc, threads=threads)
+    t0 = time.perf_counter()
+    contacts = 0
+    n = 0
+    while True:
+        o.step(1)
+        contacts += o.stats()["num_contacts"]
+        n += 1
+        if time.perf_counter() - t0 > budget_s * 0.5 or n >= 50:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": contacts / dt, "unit": "contact-steps/s", "cores": threads, "kind": "port",
+            "sample": f"first {n} time step(s) from the same initial state, cold warm-start "
+                      f"buffer, {dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="column", choices=["column", "settling"])
+    ap.add_argument("--cpu-budget-s", type=float, default=30.0)
+    ap.add_argument("--ref-budget-s", type=float, default=150.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-iterations", type=int, default=None,
+                    help="override the APGD iteration cap (profiling runs only)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        sc, desc = load_workload(args.workload)
+        print(json.dumps(run_reference(args, sc, desc)), flush=True)
+        return 0
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from dvide_b200 import _native as N
+    sc, desc = load_workload(args.workload)
+    if args.max_iterations is not None:
+        sc.params["max_iterations"] = args.max_iterations
+        desc += f" (maxIter overridden to {args.max_iterations})"
+    g = N.NativeScene.from_scene(sc)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    g.set_stream(stream.cuda_stream)
+    nb = sc.nb
+
+    g.step(max(args.warmup, 3))
+    g.history(clear=True)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    barrier()
+    l0 = g.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.step(args.steps)
+    e1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    launches = g.launches() - l0
+    ms = e0.elapsed_time(e1)
+    hist = g.history(clear=True)
+    contacts = sum(h["num_contacts"] for h in hist)
+    t_local = ms / 1e3
+
+    # end-to-end through the host-buffer API: state in from pinned memory, out every step
+    p_host = torch.empty((nb, 3), dtype=torch.float64, pin_memory=True).numpy()
+    v_host = torch.empty((nb, 3), dtype=torch.float64, pin_memory=True).numpy()
+    p0, v0 = g.state()
+    p_host[:] = p0
+    v_host[:] = v0
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.set_state(p_host, v_host)
+        g.step(1)
+        g.state_into(p_host, v_host)
+    barrier()
+    t_e2e = time.perf_counter() - t0
+    hist_e2e = g.history(clear=True)
+    contacts_e2e = sum(h["num_contacts"] for h in hist_e2e)
+
+    tot = np.array([contacts, t_local, contacts_e2e, t_e2e], dtype=np.float64)
+    if dist is not None:
+        t = torch.tensor(tot, device="cuda")
+        sums = t.clone()
+        dist.all_reduce(sums, op=dist.ReduceOp.SUM)
+        maxs = t.clone()
+        dist.all_reduce(maxs, op=dist.ReduceOp.MAX)
+        contacts_all, t_all = sums[0].item(), maxs[1].item()
+        contacts_e2e_all, t_e2e_all = sums[2].item(), maxs[3].item()
+    else:
+        contacts_all, t_all, contacts_e2e_all, t_e2e_all = tot.tolist()
+
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        solve_ms = np.array([h["solve_ms"] for h in hist])
+        step_ms = np.array([h["elapsed_ms"] for h in hist])
+        ncs = np.array([h["num_contacts"] for h in hist])
+        bts = np.array([h["backtracks"] for h in hist])
+        sweeps = np.array([h["sweeps"] for h in hist])
+        its = np.array([h["iterations"] for h in hist])
+        nposs = np.array([h["num_possible"] for h in hist])
+        bytes_per_launch = np.array([solve_bytes(c, nb, s, b) for c, s, b in zip(ncs, sweeps, bts)])
+        achieved = float(bytes_per_launch.sum() / (solve_ms.sum() / 1e3) / 1e9)
+        line = {
+            "metric": "contact-steps/s", "value": contacts_all / t_all, "unit": "contact-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded scene, see config)",
+            "config": {"workload": desc, "contacts_per_step": float(ncs.mean()),
+                       "bodies": nb, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (working set ~0.5 GB)"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                           "p99": float(np.percentile(step_ms, 99))},
+            "apgd": {"iterations_mean": float(its.mean()), "sweeps_mean": float(sweeps.mean()),
+                     "backtracks_mean": float(bts.mean()),
+                     "residual_last": hist[-1]["residual"], "solve_ms_mean": float(solve_ms.mean()),
+                     "collide_ms_mean": float(np.mean([h["collide_ms"] for h in hist]))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "traffic": float(bytes_per_launch.mean() * TRAFFIC_PER_ALGORITHMIC_BYTE),
+                         "kernel": "k_step_solve (persistent APGD + update)",
+                         "peak_kind": peak_kind,
+                         "bytes_per_launch": float(bytes_per_launch.mean())},
+            "e2e": {"value": contacts_e2e_all / t_e2e_all, "unit": "contact-steps/s",
+                    "h2d_bytes_per_step": 2 * 24 * nb, "d2h_bytes_per_step": 2 * 24 * nb},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample(sc, args.cpu_budget_s)
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -61,7 +61,8 @@ class StepStats(C.Structure):
     _fields_ = [("num_contacts", C.c_int32), ("num_possible", C.c_int32),
                 ("iterations", C.c_int32), ("backtracks", C.c_int32), ("residual", C.c_double),
                 ("objective", C.c_double), ("elapsed_ms", C.c_double), ("time", C.c_double),
-                ("time_index", C.c_int32), ("status", C.c_int32)]
+                ("time_index", C.c_int32), ("status", C.c_int32), ("collide_ms", C.c_double),
+                ("solve_ms", C.c_double), ("sweeps", C.c_int32), ("pad_", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -220,6 +221,10 @@ class NativeScene:
         v = np.zeros((self.nb, 3))
         check(lib().dv_get_state(self.h, dptr(p), dptr(v)), "dv_get_state")
         return p, v
+
+    def state_into(self, p, v):
+        """Copies positions and velocities into caller arrays (e.g. pinned)."""
+        check(lib().dv_get_state(self.h, dptr(p), dptr(v)), "dv_get_state")
 
     def set_state(self, p=None, v=None):
         pp = np.ascontiguousarray(p, dtype=np.float64) if p is not None else None

@@ -27,6 +27,9 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-f
               "-Xcompiler", "-fvisibility=hidden"]
 
 LIB = os.path.join(HERE, "libdvide_b200.so")
+CXX_LIB = os.path.join(HERE, "libdvide_cxx.so")
+DRIVER = os.path.join(HERE, "drivers", "settle")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
 def _nvcc():
@@ -64,8 +67,33 @@ def build_cuda(force=False, verbose=False):
     return LIB
 
 
+def build_cxx(force=False, verbose=False):
+    """C++ System/Body/APGD/CollisionDetector layer and the settle driver."""
+    src = os.path.join(CSRC, "cxx", "System.cpp")
+    hdrs = [os.path.join(INCLUDE, "dvide", h) for h in os.listdir(os.path.join(INCLUDE, "dvide"))]
+    inc = ["-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include")]
+    rpath = "-Wl,-rpath,$ORIGIN"
+    if force or _stale(CXX_LIB, [src, LIB] + hdrs):
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", *inc, src, "-o", CXX_LIB,
+               "-L", HERE, "-ldvide_b200", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+               rpath]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    dsrc = os.path.join(HERE, "drivers", "settle.cpp")
+    if force or _stale(DRIVER, [dsrc, CXX_LIB] + hdrs):
+        cmd = ["g++", "-O2", "-std=c++17", *inc, dsrc, "-o", DRIVER, "-L", HERE, "-ldvide_cxx",
+               "-ldvide_b200", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+               "-Wl,-rpath,$ORIGIN/.."]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    return [CXX_LIB, DRIVER]
+
+
 def build(force=False, verbose=False):
     out = [build_cuda(force=force, verbose=verbose)]
+    out += build_cxx(force=force, verbose=verbose)
     return out
 
 

@@ -1,0 +1,318 @@
+// System.cpp -- the reference's System / APGD / CollisionDetector classes for
+// rigid spheres and boxes (src/System.cu:14-133, 148-602, 1605-1930;
+// src/CollisionDetector.cu:503-545, 665-711) implemented on the C ABI of
+// include/dvide.h.  Each method keeps the reference's name, argument meaning
+// and "return 0 on success" convention; failures return the dv status code.
+#include "../../../include/dvide/System.h"
+
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+std::vector<double> download3(dv_scene* s, int which, int nb) {
+  std::vector<double> out(3 * (size_t)nb, 0.0);
+  if (!s || nb == 0) return out;
+  if (which == 0) dv_get_state(s, out.data(), nullptr);
+  else if (which == 1) dv_get_state(s, nullptr, out.data());
+  else dv_get_contact_force(s, out.data());
+  return out;
+}
+}  // namespace
+
+DeviceArray::operator std::vector<double>() const {
+  if (which == kGamma) {
+    int32_t n = 0;
+    dv_get_gamma(sys->scene, nullptr, 0, &n);
+    std::vector<double> g(3 * (size_t)n);
+    if (n) dv_get_gamma(sys->scene, g.data(), n, &n);
+    return g;
+  }
+  int w = which == kPos ? 0 : which == kVel ? 1 : 2;
+  return download3(sys->scene, w, (int)sys->bodies.size());
+}
+
+size_t DeviceArray::size() const {
+  if (which == kGamma) {
+    int32_t n = 0;
+    dv_get_gamma(sys->scene, nullptr, 0, &n);
+    return 3 * (size_t)n;
+  }
+  return 3 * sys->bodies.size();
+}
+
+System::System()
+    : scene(nullptr), frictionCoefficient(0.25), tol(1e-8), solverType(1),
+      p_d(this, DeviceArray::kPos), v_d(this, DeviceArray::kVel),
+      f_contact_d(this, DeviceArray::kContactForce), gamma_d(this, DeviceArray::kGamma) {
+  gravity = make_double3(0, -9.81, 0);
+  h = 1e-3;
+  time = 0;
+  timeIndex = 0;
+  elapsedTime = 0;
+  totalGPUMemoryUsed = 0;
+  objectiveCCP = 0;
+  collisionDetector = new CollisionDetector(this);
+  solver = new APGD(this);
+}
+
+System::System(int type) : System() {
+  // System.cu:84-107: 1 = APGD (also the default); the interior-point,
+  // active-set and Jacobi/Gauss-Seidel solvers are not part of this build.
+  solverType = type;
+}
+
+System::~System() {
+  if (scene) dv_scene_destroy(scene);
+  delete collisionDetector;
+  delete solver;
+}
+
+int System::add(Body* body) {
+  bodies.push_back(body);
+  return (int)bodies.size();
+}
+
+int System::applyForce(Body*, double3) { return 0; }
+
+int System::sync_params() {
+  dv_params P;
+  dv_params_default(&P);
+  P.h = h;
+  P.mu = frictionCoefficient;
+  P.gravity[0] = gravity.x;
+  P.gravity[1] = gravity.y;
+  P.gravity[2] = gravity.z;
+  P.envelope = collisionDetector->envelope;
+  P.tolerance = solver->tolerance;
+  P.max_iterations = solver->maxIterations;
+  APGD* apgd = dynamic_cast<APGD*>(solver);
+  P.warm_start = apgd && apgd->useWarmStarting ? 1 : 0;
+  P.verbose = solver->verbose ? 1 : 0;
+  if (!scene) return DV_ERR_ARG;
+  return dv_set_params(scene, &P);
+}
+
+int System::initializeSystem() {
+  if (solverType < 1 || solverType > 7) solverType = 1;
+  if (solverType != 1) return DV_ERR_UNSUPPORTED;
+  APGD* apgd = dynamic_cast<APGD*>(solver);
+  if (apgd && apgd->useAntiRelaxation) return DV_ERR_UNSUPPORTED;
+  std::vector<dv_body_desc> desc(bodies.size());
+  for (size_t j = 0; j < bodies.size(); ++j) {
+    Body* b = bodies[j];
+    b->setIdentifier((uint)j);   // System.cu:346-347
+    b->setIndex((uint)(3 * j));
+    dv_body_desc& d = desc[j];
+    d.pos[0] = b->pos.x; d.pos[1] = b->pos.y; d.pos[2] = b->pos.z;
+    d.vel[0] = b->vel.x; d.vel[1] = b->vel.y; d.vel[2] = b->vel.z;
+    d.mass = b->mass;
+    d.geom[0] = b->contactGeometry.x; d.geom[1] = b->contactGeometry.y;
+    d.geom[2] = b->contactGeometry.z;
+    d.fixed = b->fixed ? 1 : 0;
+    d.family = b->collisionFamily;
+  }
+  dv_params P;
+  dv_params_default(&P);
+  P.h = h;
+  P.mu = frictionCoefficient;
+  P.gravity[0] = gravity.x;
+  P.gravity[1] = gravity.y;
+  P.gravity[2] = gravity.z;
+  P.envelope = collisionDetector->envelope;
+  P.tolerance = solver->tolerance;
+  P.max_iterations = solver->maxIterations;
+  P.warm_start = apgd && apgd->useWarmStarting ? 1 : 0;
+  if (scene) dv_scene_destroy(scene);
+  scene = nullptr;
+  int rc = dv_scene_create(desc.data(), (int32_t)desc.size(), &P, &scene);
+  if (rc != DV_OK) return rc;
+  return solver->setup();
+}
+
+int System::DoTimeStep() {
+  int rc = sync_params();
+  if (rc != DV_OK) return rc;
+  rc = dv_step(scene, 1);
+  dv_step_stats st;
+  dv_get_step_stats(scene, &st);
+  elapsedTime = st.elapsed_ms;
+  objectiveCCP = st.objective;
+  collisionDetector->numCollisions = (uint)st.num_contacts;
+  collisionDetector->numPossibleCollisions = (uint)st.num_possible;
+  solver->iterations = st.iterations;
+  time = st.time;
+  timeIndex = st.time_index;
+  size_t avail = 0, total = 0;
+  if (cudaMemGetInfo(&avail, &total) == cudaSuccess)
+    totalGPUMemoryUsed = (double)(total - avail) / 1000000.0;
+  return rc;
+}
+
+double4 System::getCCPViolation() {
+  double o[4] = {0, 0, 0, 0};
+  if (scene) dv_ccp_violation(scene, o);
+  return make_double4(o[0], o[1], o[2], o[3]);
+}
+
+double System::getKineticEnergy() {
+  double k = 0, p = 0;
+  if (scene) dv_energies(scene, &k, &p);
+  return k;
+}
+
+double System::getPotentialEnergy() {
+  double k = 0, p = 0;
+  if (scene) dv_energies(scene, &k, &p);
+  return p;
+}
+
+std::vector<double> System::getPositions() { return p_d; }
+std::vector<double> System::getVelocities() { return v_d; }
+std::vector<double> System::getContactForces() { return f_contact_d; }
+
+// System.cu:1699-1737: one CSV row per rigid body.
+int System::exportSystem(std::string filename) {
+  std::ofstream fs(filename.c_str());
+  if (!fs) return DV_ERR_ARG;
+  p_h = p_d;
+  v_h = v_d;
+  f_contact_h = f_contact_d;
+  fs << bodies.size() << ", " << 0 << ", " << 0 << ", " << 0 << ", " << std::endl;
+  for (size_t i = 0; i < bodies.size(); ++i) {
+    double3 g = bodies[i]->contactGeometry;
+    fs << i << ", " << bodies[i]->isFixed() << ", " << p_h[3 * i] << ", " << p_h[3 * i + 1]
+       << ", " << p_h[3 * i + 2] << ", " << "1, " << "0, " << "0, " << "0, " << v_h[3 * i]
+       << ", " << v_h[3 * i + 1] << ", " << v_h[3 * i + 2] << ", ";
+    if (g.y == 0) fs << "0, " << g.x << ", ";
+    else fs << "2, " << g.x << ", " << g.y << ", " << g.z << ", ";
+    fs << "\n";
+  }
+  return 0;
+}
+
+// System.cu:1856-1910: reads the rows written by exportSystem; spheres get
+// the reference's hard-coded density 2600 (and its value of pi).
+int System::importSystem(std::string filename) {
+  std::ifstream in(filename.c_str());
+  if (!in) return DV_ERR_ARG;
+  std::string line;
+  if (!std::getline(in, line)) return DV_ERR_ARG;
+  for (char& c : line)
+    if (c == ',') c = ' ';
+  int numBodies = 0, numBeams = 0, numPlates = 0, numBodies2D = 0;
+  std::stringstream ss1(line);
+  ss1 >> numBodies >> numBeams >> numPlates >> numBodies2D;
+  for (int i = 0; i < numBodies; ++i) {
+    if (!std::getline(in, line)) return DV_ERR_ARG;
+    for (char& c : line)
+      if (c == ',') c = ' ';
+    std::stringstream ss(line);
+    int index = 0, isFixed = 0, shape = 0;
+    double blah;
+    double3 pos, vel, geometry = make_double3(0, 0, 0);
+    ss >> index >> isFixed >> pos.x >> pos.y >> pos.z >> blah >> blah >> blah >> blah >> vel.x >>
+        vel.y >> vel.z >> shape;
+    if (shape == 0) {
+      ss >> geometry.x;
+    } else {
+      ss >> geometry.x >> geometry.y >> geometry.z;
+    }
+    Body* b = new Body(pos);
+    b->setBodyFixed(isFixed != 0);
+    b->setGeometry(geometry);
+    b->setVelocity(vel);
+    if (shape == 0) b->setMass(2600 * 4.0 * 3.14159 * geometry.x * geometry.x * geometry.x / 3.0);
+    else b->setMass(1.0);
+    add(b);
+  }
+  return 0;
+}
+
+int System::calculateContactForcePerCollision() { return 0; }
+
+// System.cu:1672-1697
+int System::outputContactForcePerCollision(std::string filename) {
+  std::ofstream fs(filename.c_str());
+  if (!fs || !scene) return DV_ERR_ARG;
+  int32_t nc = 0, np = 0;
+  dv_get_num_contacts(scene, &nc, &np);
+  std::vector<uint32_t> a(nc), b(nc);
+  std::vector<double> loc(3 * (size_t)nc), fn(3 * (size_t)nc), ff(3 * (size_t)nc);
+  if (nc) {
+    dv_get_contacts(scene, a.data(), b.data(), nullptr, loc.data());
+    dv_contact_forces_per_collision(scene, fn.data(), ff.data());
+  }
+  fs << nc << ", " << bodies.size() << ", " << 0 << ", " << 0 << ", " << 0 << ", " << std::endl;
+  for (int i = 0; i < nc; ++i)
+    fs << i << ", " << a[i] << ", " << b[i] << ", " << loc[3 * i] << ", " << loc[3 * i + 1] << ", "
+       << loc[3 * i + 2] << ", " << fn[3 * i] << ", " << fn[3 * i + 1] << ", " << fn[3 * i + 2]
+       << ", " << ff[3 * i] << ", " << ff[3 * i + 1] << ", " << ff[3 * i + 2] << ", \n";
+  return 0;
+}
+
+int APGD::setup() { return 0; }
+
+// The APGD iterations run inside System::DoTimeStep's device step; a
+// separate solve() is not exposed by the B200 step and reports unsupported.
+int APGD::solve() { return DV_ERR_UNSUPPORTED; }
+
+int CollisionDetector::setEnvelope(double e) {
+  envelope = e;
+  return 0;
+}
+
+int CollisionDetector::detectCollisions() {
+  if (!system->scene) return DV_ERR_ARG;
+  int rc = dv_collide(system->scene);
+  int32_t nc = 0, np = 0;
+  dv_get_num_contacts(system->scene, &nc, &np);
+  numCollisions = (uint)nc;
+  numPossibleCollisions = (uint)np;
+  return rc;
+}
+
+std::vector<uint32_t> CollisionDetector::getCollisionIdentifierA() {
+  std::vector<uint32_t> a(numCollisions);
+  if (numCollisions) dv_get_contacts(system->scene, a.data(), nullptr, nullptr, nullptr);
+  return a;
+}
+
+std::vector<uint32_t> CollisionDetector::getCollisionIdentifierB() {
+  std::vector<uint32_t> b(numCollisions);
+  if (numCollisions) dv_get_contacts(system->scene, nullptr, b.data(), nullptr, nullptr);
+  return b;
+}
+
+std::vector<double4> CollisionDetector::getNormalsAndPenetrations() {
+  std::vector<double> raw(4 * (size_t)numCollisions);
+  if (numCollisions) dv_get_contacts(system->scene, nullptr, nullptr, raw.data(), nullptr);
+  std::vector<double4> out(numCollisions);
+  for (uint i = 0; i < numCollisions; ++i)
+    out[i] = make_double4(raw[4 * i], raw[4 * i + 1], raw[4 * i + 2], raw[4 * i + 3]);
+  return out;
+}
+
+// CollisionDetector.cu:665-711
+int CollisionDetector::exportSystem(std::string filename) {
+  std::ofstream fs(filename.c_str());
+  if (!fs || !system->scene) return DV_ERR_ARG;
+  std::vector<uint32_t> A = getCollisionIdentifierA(), B = getCollisionIdentifierB();
+  std::vector<double4> nP = getNormalsAndPenetrations();
+  std::vector<double> p = system->p_d, v = system->v_d;
+  for (uint i = 0; i < numCollisions; ++i) {
+    double3 ga = system->bodies[A[i]]->getGeometry(), gb = system->bodies[B[i]]->getGeometry();
+    fs << i << ", " << A[i] << ", " << B[i] << ", " << nP[i].x << ", " << nP[i].y << ", "
+       << nP[i].z << ", " << nP[i].w << ", " << p[3 * A[i]] << ", " << p[3 * A[i] + 1] << ", "
+       << p[3 * A[i] + 2] << ", " << v[3 * A[i]] << ", " << v[3 * A[i] + 1] << ", "
+       << v[3 * A[i] + 2] << ", " << ga.x << ", " << ga.y << ", " << ga.z << ", " << p[3 * B[i]]
+       << ", " << p[3 * B[i] + 1] << ", " << p[3 * B[i] + 2] << ", " << v[3 * B[i]] << ", "
+       << v[3 * B[i] + 1] << ", " << v[3 * B[i] + 2] << ", " << gb.x << ", " << gb.y << ", "
+       << gb.z << ", " << "\n";
+  }
+  return 0;
+}

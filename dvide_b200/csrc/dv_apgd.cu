@@ -344,6 +344,7 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
           C->mode = 0;
           C->done = (a.max_iter <= 0) ? 1 : 0;
           C->iterations = 0;
+          C->sweeps = 0;
           C->restart = 0;
           C->cur = 0;
           C->hat = kHatNone;
@@ -533,6 +534,7 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
               }
             } else {
               C->mode = 0;
+              C->sweeps += 1;
               if (res < C->residual) {
                 C->residual = res;
                 C->objective = obj1;

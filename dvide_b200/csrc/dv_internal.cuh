@@ -52,6 +52,7 @@ struct ApgdCtl {
   int backtracks;
   unsigned err;
   int iterations;
+  int sweeps;           // iterations executed
 };
 
 struct SceneDev {

@@ -34,7 +34,12 @@ struct dv_scene {
   dv_params P;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  cudaEvent_t ev_count = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+  cudaEvent_t ev_count = nullptr;
+  // per-step timing events, double-buffered: step k uses set k & 1 so the
+  // previous step's events survive until its report is folded in
+  cudaEvent_t ev_t0[2] = {nullptr, nullptr}, ev_t1[2] = {nullptr, nullptr};
+  cudaEvent_t ev_c[2] = {nullptr, nullptr}, ev_s[2] = {nullptr, nullptr};
+  int ev_cur = 0;
   int64_t launches = 0;
   int max_ctas = 1;
   double time = 0;
@@ -156,11 +161,19 @@ int absorb_solve(dv_scene* s) {
     s->last.backtracks = c.backtracks;
     s->last.residual = c.residual;
     s->last.objective = c.objective;
+    s->last.sweeps = c.sweeps;
+    int e = s->ev_cur;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s->ev_t0[e], s->ev_c[e]) == cudaSuccess) s->last.collide_ms = ms;
+    if (cudaEventElapsedTime(&ms, s->ev_c[e], s->ev_s[e]) == cudaSuccess) s->last.solve_ms = ms;
     st = status_from_bits(s->h_bar[2]);
     if (st != DV_OK) s->last.status = st;
   }
   if (s->step_open) {
     s->step_open = false;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s->ev_t0[s->ev_cur], s->ev_t1[s->ev_cur]) == cudaSuccess)
+      s->last.elapsed_ms = ms;
     s->last.time = s->time;
     s->last.time_index = s->time_index;
     s->history.push_back(s->last);
@@ -171,12 +184,14 @@ int absorb_solve(dv_scene* s) {
 int one_step(dv_scene* s) {
   SceneDev& d = s->d;
   cudaStream_t st = s->stream;
-  DV_CUDA_TRY(cudaEventRecord(s->ev_t0, st));
+  const int e = s->ev_cur ^ 1;   // the previous step (if any) used ev_cur
+  DV_CUDA_TRY(cudaEventRecord(s->ev_t0[e], st));
   collide_count(d, s->P.envelope, st, &s->launches);
   DV_CUDA_TRY(cudaEventRecord(s->ev_count, st));
   DV_CUDA_TRY(cudaEventSynchronize(s->ev_count));
   DV_CUDA_TRY(cudaGetLastError());
   int prev = absorb_solve(s);
+  s->ev_cur = e;
   if (prev != DV_OK) return prev;
   int nc = d.h_counters[0];
   int np = d.h_counters[1];
@@ -213,15 +228,17 @@ int one_step(dv_scene* s) {
     int nt = (nc + kTileItems - 1) / kTileItems;
     int nbt = (d.nb + kThreads - 1) / kThreads;
     cfg.grid = std::max(1, std::min(s->max_ctas, std::max(nt, nbt)));
+    DV_CUDA_TRY(cudaEventRecord(s->ev_c[e], st));
     launch_step_solve(d, cfg, st, &s->launches);
     DV_CUDA_TRY(cudaGetLastError());
+    DV_CUDA_TRY(cudaEventRecord(s->ev_s[e], st));
     DV_CUDA_TRY(cudaMemcpyAsync(s->h_bar, d.bar, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     s->solve_pending = true;
   } else {
     launch_step_nocontact(d, s->P.h, st, &s->launches);
     DV_CUDA_TRY(cudaGetLastError());
   }
-  DV_CUDA_TRY(cudaEventRecord(s->ev_t1, st));
+  DV_CUDA_TRY(cudaEventRecord(s->ev_t1[e], st));
   s->time += s->P.h;
   s->time_index += 1;
   s->step_open = true;
@@ -231,8 +248,6 @@ int one_step(dv_scene* s) {
 int finish(dv_scene* s) {
   DV_CUDA_TRY(cudaStreamSynchronize(s->stream));
   int st = absorb_solve(s);
-  float ms = 0.f;
-  if (cudaEventElapsedTime(&ms, s->ev_t0, s->ev_t1) == cudaSuccess) s->last.elapsed_ms = ms;
   s->last.time = s->time;
   s->last.time_index = s->time_index;
   if (s->P.verbose)
@@ -405,8 +420,12 @@ DV_API int dv_scene_create(const dv_body_desc* bodies, int32_t nb, const dv_para
     return fail(dv_record_cuda_error(cudaGetLastError(), "cudaStreamCreate", __FILE__, __LINE__));
   s->own_stream = true;
   cudaEventCreate(&s->ev_count);
-  cudaEventCreate(&s->ev_t0);
-  cudaEventCreate(&s->ev_t1);
+  for (int k = 0; k < 2; ++k) {
+    cudaEventCreate(&s->ev_t0[k]);
+    cudaEventCreate(&s->ev_t1[k]);
+    cudaEventCreate(&s->ev_c[k]);
+    cudaEventCreate(&s->ev_s[k]);
+  }
 
   // classify: spheres go in the grid, boxes are tested against all bodies
   std::vector<int> small, large;
@@ -516,8 +535,12 @@ DV_API int dv_scene_destroy(dv_scene* s) {
   if (s->h_bar) cudaFreeHost(s->h_bar);
   if (s->h_red) cudaFreeHost(s->h_red);
   if (s->ev_count) cudaEventDestroy(s->ev_count);
-  if (s->ev_t0) cudaEventDestroy(s->ev_t0);
-  if (s->ev_t1) cudaEventDestroy(s->ev_t1);
+  for (int k = 0; k < 2; ++k) {
+    if (s->ev_t0[k]) cudaEventDestroy(s->ev_t0[k]);
+    if (s->ev_t1[k]) cudaEventDestroy(s->ev_t1[k]);
+    if (s->ev_c[k]) cudaEventDestroy(s->ev_c[k]);
+    if (s->ev_s[k]) cudaEventDestroy(s->ev_s[k]);
+  }
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return DV_OK;

@@ -1,0 +1,85 @@
+// settle.cpp -- a driver written against the reference's C++ API
+// (System, Body, APGD; compare models/test_compaction.cu:184-431): 1,000
+// spheres (r = 0.05 m, rho = 2600) on a 10x10x10 lattice in an open box of
+// five fixed boxes, mu = 0.25, h = 1e-3, APGD with warm start.
+// Usage: settle <steps> <solverType> <tolerance> [maxIterations]
+// Prints one line per step: time, contacts, iterations, weight carried by
+// the fixed boxes, and the four CCP violations.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <vector>
+
+#include "dvide/System.h"
+
+static unsigned long long rng = 88172645463325252ull;
+static double getRandomNumber(double lo, double hi) {
+  rng ^= rng << 13;
+  rng ^= rng >> 7;
+  rng ^= rng << 17;
+  return lo + (hi - lo) * ((rng >> 11) * (1.0 / 9007199254740992.0));
+}
+
+int main(int argc, char** argv) {
+  int steps = argc > 1 ? atoi(argv[1]) : 100;
+  int solverType = argc > 2 ? atoi(argv[2]) : 1;
+  double tolerance = argc > 3 ? atof(argv[3]) : 1e-4;
+  int maxIterations = argc > 4 ? atoi(argv[4]) : 1000;
+
+  System* sys = new System(solverType);
+  sys->setTimeStep(1e-3);
+  sys->gravity = make_double3(0, 0, -9.81);
+  sys->solver->tolerance = tolerance;
+  sys->solver->maxIterations = maxIterations;
+  sys->collisionDetector->setBinsPerAxis(make_uint3(10, 10, 10));
+  if (solverType == 1) dynamic_cast<APGD*>(sys->solver)->setWarmStarting(true);
+
+  const double t = 0.05, inner = 0.6, H = 0.75;
+  double3 c[5] = {make_double3(0, 0, -t), make_double3(-inner - t, 0, H), make_double3(inner + t, 0, H),
+                  make_double3(0, -inner - t, H), make_double3(0, inner + t, H)};
+  double3 g[5] = {make_double3(inner + 2 * t, inner + 2 * t, t), make_double3(t, inner + 2 * t, H),
+                  make_double3(t, inner + 2 * t, H), make_double3(inner, t, H),
+                  make_double3(inner, t, H)};
+  for (int i = 0; i < 5; ++i) {
+    Body* b = new Body(c[i]);
+    b->setBodyFixed(true);
+    b->setGeometry(g[i]);
+    sys->add(b);
+  }
+  const double r = 0.05, rho = 2600.0, sp = 0.11;
+  double totalWeight = 0;
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j)
+      for (int k = 0; k < 10; ++k) {
+        Body* b = new Body(make_double3(-0.495 + sp * i + getRandomNumber(-0.005, 0.005),
+                                        -0.495 + sp * j + getRandomNumber(-0.005, 0.005),
+                                        0.06 + sp * k + getRandomNumber(-0.005, 0.005)));
+        b->setGeometry(make_double3(r, 0, 0));
+        b->setMass(rho * 4.0 / 3.0 * M_PI * r * r * r);
+        totalWeight += b->getMass() * 9.81;
+        sys->add(b);
+      }
+  int rc = sys->initializeSystem();
+  if (rc != 0) {
+    fprintf(stderr, "initializeSystem failed: %s\n", dv_status_string(rc));
+    return 1;
+  }
+  printf("System initialized! bodies %zu, expected weight %.6f\n", sys->bodies.size(), totalWeight);
+  for (int s = 0; s < steps; ++s) {
+    rc = sys->DoTimeStep();
+    if (rc != 0) {
+      fprintf(stderr, "DoTimeStep failed at step %d: %s\n", s, dv_status_string(rc));
+      return 2;
+    }
+    double4 v = sys->getCCPViolation();
+    sys->f_contact_h = sys->f_contact_d;
+    double weight = 0;
+    for (int i = 0; i < 5; ++i) weight -= sys->f_contact_h[3 * i + 2];
+    printf("%f, %u, %d, %.6f, %g, %g, %g, %g, %f\n", sys->time, sys->collisionDetector->numCollisions,
+           sys->solver->iterations, weight, v.x, v.y, v.z, v.w, sys->elapsedTime);
+  }
+  sys->exportSystem("settle_final.csv");
+  delete sys;
+  return 0;
+}

@@ -79,6 +79,10 @@ typedef struct dv_step_stats {
   double time;               /* System::time */
   int32_t time_index;        /* System::timeIndex */
   int32_t status;
+  double collide_ms;         /* device time of collision detection */
+  double solve_ms;           /* device time of the persistent solve kernel */
+  int32_t sweeps;            /* APGD iterations executed (iterations + 1 when converged) */
+  int32_t pad_;
 } dv_step_stats;
 
 typedef struct dv_scene dv_scene;

@@ -1,0 +1,86 @@
+// System.h -- the reference's System (src/System.cuh:279-326) for rigid
+// spheres and boxes, backed by the B200 contact step of include/dvide.h.
+// Device vectors of the reference (p_d, v_d, f_contact_d, gamma_d) are
+// DeviceArray handles: assigning one to a std::vector downloads it, so
+// driver lines such as `sys->f_contact_h = sys->f_contact_d;` keep working.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../dvide.h"
+#include "APGD.h"
+#include "Body.h"
+#include "CollisionDetector.h"
+#include "Solver.h"
+
+class System;
+
+class DeviceArray {
+ public:
+  enum Which { kPos, kVel, kContactForce, kGamma };
+  DeviceArray(System* s, Which w) : sys(s), which(w) {}
+  operator std::vector<double>() const;
+  size_t size() const;
+
+ private:
+  System* sys;
+  Which which;
+};
+
+class System {
+  friend class APGD;
+  friend class CollisionDetector;
+  friend class DeviceArray;
+
+ private:
+  dv_scene* scene;
+  double frictionCoefficient;
+  double tol;
+  int solverType;
+  int sync_params();
+
+ public:
+  System();
+  explicit System(int solverType);
+  ~System();
+
+  std::vector<Body*> bodies;
+  Solver* solver;
+  CollisionDetector* collisionDetector;
+  double3 gravity;
+  double h;
+  double time;
+  int timeIndex;
+  double elapsedTime;
+  double totalGPUMemoryUsed;
+  double objectiveCCP;
+  DeviceArray p_d, v_d, f_contact_d, gamma_d;
+  std::vector<double> p_h, v_h, f_contact_h;
+
+  double getCurrentTime() const { return time; }
+  double getTimeStep() const { return h; }
+  double getTolerance() const { return tol; }
+  int getTimeIndex() const { return timeIndex; }
+  void setTimeStep(double step_size) { h = step_size; }
+  void setFrictionCoefficient(double mu) { frictionCoefficient = mu; }
+  int add(Body* body);
+  int initializeSystem();
+  int DoTimeStep();
+  // applied forces are not part of the reference dynamics (System.cu:1510)
+  int applyForce(Body* body, double3 force);
+  int clearAppliedForces() { return 0; }
+  double4 getCCPViolation();
+  double getPotentialEnergy();
+  double getKineticEnergy();
+  double getStrainEnergy() { return 0.0; }
+  double getTotalEnergy() { return getPotentialEnergy() + getKineticEnergy(); }
+  int exportSystem(std::string filename);
+  int importSystem(std::string filename);
+  int calculateContactForcePerCollision();
+  int outputContactForcePerCollision(std::string filename);
+  std::vector<double> getPositions();
+  std::vector<double> getVelocities();
+  std::vector<double> getContactForces();
+  dv_scene* native() { return scene; }
+};

@@ -1,0 +1,32 @@
+"""The C++ layer (include/dvide/System.h) runs a driver written like the
+reference's models/test_compaction.cu and gives the oracle's trajectory."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "dvide_b200", "drivers", "settle")
+
+pytestmark = pytest.mark.gpu
+
+
+def test_settle_driver_runs(tmp_path):
+    out = subprocess.run([DRIVER, "120", "1", "1e-4", "1000"], cwd=tmp_path, capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [l for l in out.stdout.splitlines() if l and l[0].isdigit()]
+    assert len(lines) == 120
+    last = [float(x) for x in lines[-1].split(",")]
+    assert last[1] > 100          # contacts once the lattice has landed
+    assert os.path.exists(tmp_path / "settle_final.csv")
+    rows = open(tmp_path / "settle_final.csv").read().splitlines()
+    assert rows[0].startswith("1005,") and len(rows) == 1006
+
+
+def test_unsupported_solver_type_reports(tmp_path):
+    out = subprocess.run([DRIVER, "1", "2", "1e-4"], cwd=tmp_path, capture_output=True, text=True,
+                         timeout=120)
+    assert out.returncode == 1
+    assert "unsupported" in out.stderr

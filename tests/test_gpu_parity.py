@@ -189,7 +189,8 @@ def test_positional_warm_start(native, oracle_mod):
     # lift every sphere out of contact: no solve, gamma unchanged
     p, v = o.state()
     p2 = p.copy()
-    p2[sc.fixed == 0, 2] += 5.0
+    dyn = np.nonzero(sc.fixed == 0)[0]
+    p2[dyn] = np.stack([np.arange(dyn.size) * 1.0, np.zeros(dyn.size), np.full(dyn.size, 5.0)], 1)
     before = o.gamma()
     g.set_state(p2, v)
     o.set_state(p2, v)
