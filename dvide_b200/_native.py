@@ -27,6 +27,7 @@ EXPORTS = [
     "dv_set_gamma", "dv_get_frames", "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
     "dv_contact_forces_per_collision", "dv_get_step_stats", "dv_status_string", "dv_last_error",
     "dv_scene_launch_count", "dv_get_step_history", "dv_clear_step_history",
+    "dv_ccp_violation_noalloc",
 ]
 
 
@@ -112,6 +113,9 @@ def lib():
     L.dv_status_string.restype = C.c_char_p
     L.dv_last_error.argtypes = []
     L.dv_last_error.restype = C.c_char_p
+    L.dv_ccp_violation_noalloc.argtypes = [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double,
+                                           C.c_double, vp, vp]
+    L.dv_ccp_violation_noalloc.restype = C.c_int
     L.dv_scene_launch_count.argtypes = [vp]
     L.dv_scene_launch_count.restype = C.c_int64
     _lib = L

@@ -182,3 +182,4 @@ constexpr uint64_t kBarrierTimeoutNs = 2000000000ull;
   } while (0)
 
 int dv_record_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+void dv_set_error_text(const char* text);

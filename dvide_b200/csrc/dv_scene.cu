@@ -29,6 +29,8 @@ int dv_record_cuda_error(cudaError_t e, const char* what, const char* file, int 
   return DV_ERR_CUDA;
 }
 
+void dv_set_error_text(const char* text) { g_last_error = text; }
+
 struct dv_scene {
   SceneDev d;
   dv_params P;

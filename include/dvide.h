@@ -150,6 +150,26 @@ DV_API int64_t dv_scene_launch_count(dv_scene* s);
 DV_API int dv_get_step_history(dv_scene* s, dv_step_stats* out, int32_t cap, int32_t* n);
 DV_API int dv_clear_step_history(dv_scene* s);
 
+/* No counterpart in the reference.  dv_ccp_violation without any device
+ * allocation, for callers that may not call cudaMalloc/cudaFree: an
+ * application whose device memory belongs to its own pool allocator, or a
+ * fixed-rate loop that cannot afford an allocation that may synchronise the
+ * device.  All array arguments are caller-owned DEVICE pointers in the reference's
+ * layouts: gamma 3 per contact (System::gamma_d), nP 4 per contact
+ * (normalsAndPenetrations_d: normal B->A, gap), ida/idb per contact, v 3 per
+ * body (System::v_d); out4 receives (min gamma_n, min v_n, gamma_n . v_n,
+ * ||cone violation||) in device memory, queued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream).  Scratch is a fixed 512 KiB array in device
+ * memory that each GPU holds until the process exits; nc above
+ * DV_NOALLOC_MAX_CONTACTS is rejected with DV_ERR_ARG.  The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress); make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (unordered streams) race. */
+#define DV_NOALLOC_MAX_CONTACTS 16777216
+DV_API int dv_ccp_violation_noalloc(int32_t nc, int32_t nb, const double* gamma, const double* nP,
+                                    const uint32_t* ida, const uint32_t* idb, const double* v,
+                                    double mu, double h, double* out4, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
