@@ -232,6 +232,7 @@ def main():
 
     g.step(max(args.warmup, 3))
     g.history(clear=True)
+    g.phase_times(reset=True)
 
     def barrier():
         torch.cuda.synchronize()
@@ -253,6 +254,7 @@ def main():
     launches = g.launches() - l0
     ms = e0.elapsed_time(e1)
     hist = g.history(clear=True)
+    phases = g.phase_times(reset=True)
     contacts = sum(h["num_contacts"] for h in hist)
     t_local = ms / 1e3
 
@@ -310,7 +312,9 @@ def main():
             "apgd": {"iterations_mean": float(its.mean()), "sweeps_mean": float(sweeps.mean()),
                      "backtracks_mean": float(bts.mean()),
                      "residual_last": hist[-1]["residual"], "solve_ms_mean": float(solve_ms.mean()),
-                     "collide_ms_mean": float(np.mean([h["collide_ms"] for h in hist]))},
+                     "collide_ms_mean": float(np.mean([h["collide_ms"] for h in hist])),
+                     "phase_ms_total": {k: round(v[0], 3) for k, v in phases.items()},
+                     "phase_us_mean": {k: round(1e3 * v[0] / v[1], 2) for k, v in phases.items()}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": float(bytes_per_launch.mean() * TRAFFIC_PER_ALGORITHMIC_BYTE),

@@ -27,7 +27,7 @@ EXPORTS = [
     "dv_set_gamma", "dv_get_frames", "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
     "dv_contact_forces_per_collision", "dv_get_step_stats", "dv_status_string", "dv_last_error",
     "dv_scene_launch_count", "dv_get_step_history", "dv_clear_step_history",
-    "dv_ccp_violation_noalloc",
+    "dv_get_phase_times", "dv_ccp_violation_noalloc",
 ]
 
 
@@ -104,6 +104,7 @@ def lib():
         "dv_get_step_stats": [vp, C.POINTER(StepStats)],
         "dv_get_step_history": [vp, C.POINTER(StepStats), C.c_int32, ip],
         "dv_clear_step_history": [vp],
+        "dv_get_phase_times": [vp, dp, C.POINTER(C.c_int64), C.c_int32],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -316,6 +317,16 @@ class NativeScene:
         if clear:
             lib().dv_clear_step_history(self.h)
         return out
+
+    PHASES = ("setup", "step", "backtrack", "body", "product", "final", "unused6", "unused7")
+
+    def phase_times(self, reset=False):
+        ns = np.zeros(8)
+        cnt = np.zeros(8, dtype=np.int64)
+        check(lib().dv_get_phase_times(self.h, dptr(ns), cnt.ctypes.data_as(C.POINTER(C.c_int64)),
+                                       int(reset)))
+        return {name: (float(ns[i]) / 1e6, int(cnt[i])) for i, name in enumerate(self.PHASES)
+                if cnt[i]}
 
     def launches(self):
         return int(lib().dv_scene_launch_count(self.h))

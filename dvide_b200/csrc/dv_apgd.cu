@@ -20,14 +20,20 @@
 //                 then +q_c where b is A, ascending contact order; no atomics)
 //   contact pass: (N x)_c = F_c^T (w_A - w_B), fused with the APGD vector
 //                 updates, the cone projection and the reductions.
-// The reference's per-iteration sequence calls the Schur product four times
-// (APGD.cu:229, 237, 239, 276); the second N y and the residual's N gamma_new
-// repeat a product of the same vector, so they are reused bit-for-bit here:
-// two products per iteration and one per backtrack.
 //
-// Work is split in tiles of 1024 contacts (4 per thread) and 256 bodies;
+// One Schur product per iteration.  The reference evaluates N y_k with its own
+// product (APGD.cu:229, 239) and N gamma_new twice more (:237, :276).  Since
+// y_k = (1 + b) gamma_k - b gamma_{k-1} (APGD.cu:273) or gamma_k after a
+// restart (:315), N y_k is formed here from the stored products of the two
+// previous iterates; N gamma_new is computed once and serves the objective and
+// the residual.  Iterates and their products rotate through four buffers, so
+// y, g and gamma_hat are never copied.  The CPU oracle evaluates the same
+// sequence (apgd_solve_fused), and bit-for-bit the same arithmetic.
+//
+// Work is split in tiles of 512 contacts (2 per thread) and 256 bodies;
 // CTA b owns tiles b, b + G, ...  Every wait has a time limit.
 #include <stdio.h>
+#include <stdlib.h>
 
 #include "dv_internal.cuh"
 
@@ -35,10 +41,18 @@ namespace dv {
 
 namespace {
 
-constexpr int kNQ = 6;          // partial-sum slots per tile
-constexpr int kQMax = kNQ;      // slot of the per-tile maximum
+constexpr int kNQ = 7;      // partial-sum slots per tile
+constexpr int kQMax = kNQ;  // slot of the per-tile maximum
 
-enum HatWhere { kHatNone = 0, kHatBuf = 1, kHatCur = 2, kHatNew = 3 };
+// Phases timed between grid-barrier releases (ApgdCtl::phase_ns).
+enum Phase : int {
+  kPhaseSetup = 0,     // k, r, Lipschitz estimate
+  kPhaseStep = 1,      // gamma_new = P(y - t g), full iteration
+  kPhaseBacktrack = 2, // gamma_new recomputed after L doubled
+  kPhaseBody = 3,      // body gather w = Minv D^T q
+  kPhaseProduct = 4,   // N gamma_new, objective, residual
+  kPhaseFinal = 5,     // gamma = gamma_hat, update
+};
 
 struct KArgs {
   int nb, nc;
@@ -57,13 +71,10 @@ struct KArgs {
   const double* __restrict__ F;
   const double* __restrict__ gap;
   double* r;
-  const int* __restrict__ abase;
-  const int* __restrict__ bstart;
-  const uint32_t* __restrict__ binc;
-  double* G[2];
-  double* Y[2];
-  double* g;
-  double* ghat;
+  const int* __restrict__ inc_start;
+  const uint32_t* __restrict__ inc;
+  double* G[5];
+  double* NG[5];
   double4* q;
   double* gamma;
   double* part;
@@ -78,13 +89,30 @@ struct Frame {
   double n0, n1, n2, u0, u1, u2, v0, v1, v2;
 };
 
+// Frame modes: 0 loads n, u, v; 1 recomputes u and v from n with the
+// narrowphase's own function, so both modes see the same bits.
+__device__ inline void complete_frame(Frame& f, int mode) {
+  if (mode == 1) {
+    d3 u, v;
+    frame_from_normal(mk3(f.n0, f.n1, f.n2), &u, &v);
+    f.u0 = u.x; f.u1 = u.y; f.u2 = u.z;
+    f.v0 = v.x; f.v1 = v.y; f.v2 = v.z;
+  }
+}
+
+template <int kMode>
 __device__ inline Frame load_frame(const KArgs& a, int c) {
   const double* F = a.F;
   size_t S = a.S;
   Frame f;
-  f.n0 = __ldg(F + 0 * S + c); f.n1 = __ldg(F + 1 * S + c); f.n2 = __ldg(F + 2 * S + c);
-  f.u0 = __ldg(F + 3 * S + c); f.u1 = __ldg(F + 4 * S + c); f.u2 = __ldg(F + 5 * S + c);
-  f.v0 = __ldg(F + 6 * S + c); f.v1 = __ldg(F + 7 * S + c); f.v2 = __ldg(F + 8 * S + c);
+  f.n0 = __ldg(F + 0 * S + c);
+  f.n1 = __ldg(F + 1 * S + c);
+  f.n2 = __ldg(F + 2 * S + c);
+  if (kMode == 0) {
+    f.u0 = __ldg(F + 3 * S + c); f.u1 = __ldg(F + 4 * S + c); f.u2 = __ldg(F + 5 * S + c);
+    f.v0 = __ldg(F + 6 * S + c); f.v1 = __ldg(F + 7 * S + c); f.v2 = __ldg(F + 8 * S + c);
+  }
+  complete_frame(f, kMode);
   return f;
 }
 
@@ -131,16 +159,16 @@ __device__ inline void block_fold_multi(double (&v)[NQ], double* scratch) {
   __syncthreads();
 }
 
-// Controller side: folds the per-tile partials of NQ quantities (slots
-// qbase..qbase+NQ-1) in the fixed order; results valid in thread 0.
+// Controller side: folds the per-tile partials of NQ quantities in the fixed
+// order (slot j sums tiles j, j+256, ...; then the 256-slot tree).
 template <int NQ>
-__device__ inline void fold_tiles(const KArgs& a, int qbase, double (&out)[NQ], double* scratch) {
+__device__ inline void fold_tiles(const KArgs& a, double (&out)[NQ], double* scratch) {
   double v[NQ];
 #pragma unroll
   for (int qi = 0; qi < NQ; ++qi) {
     double acc = 0.0;
     for (int t = threadIdx.x; t < a.nt; t += kThreads)
-      acc = acc + __ldcg(a.part + (size_t)(qbase + qi) * a.ptiles + t);
+      acc = acc + __ldcg(a.part + (size_t)qi * a.ptiles + t);
     v[qi] = acc;
   }
   block_fold_multi<NQ>(v, scratch);
@@ -157,11 +185,19 @@ __device__ inline double fold_tiles_max(const KArgs& a, double* scratch) {
   return r;
 }
 
+template <int NQ>
+__device__ inline void write_partials(const KArgs& a, int tile, const double (&v)[NQ]) {
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int qi = 0; qi < NQ; ++qi) a.part[(size_t)qi * a.ptiles + tile] = v[qi];
+  }
+}
+
 // Grid barrier.  The last CTA to arrive runs `ctl_fn` (all its threads),
 // then releases the generation word.  Returns false after a timeout or an
 // error raised by another CTA; the caller then leaves the kernel.
 template <class Fn>
-__device__ inline bool grid_sync(const KArgs& a, Fn ctl_fn) {
+__device__ inline bool grid_sync(const KArgs& a, int phase, Fn ctl_fn) {
   __shared__ unsigned s_last, s_target;
   __shared__ int s_fail;
   __syncthreads();
@@ -178,6 +214,13 @@ __device__ inline bool grid_sync(const KArgs& a, Fn ctl_fn) {
     ctl_fn();
     __syncthreads();
     if (threadIdx.x == 0) {
+      ApgdCtl* C = a.ctl;
+      unsigned long long now = global_ns();
+      if (C->last_release) {
+        C->phase_ns[phase] += now - C->last_release;
+        C->phase_count[phase] += 1;
+      }
+      C->last_release = now;
       __threadfence();
       st_release(&a.bar[1], s_target);
     }
@@ -185,9 +228,9 @@ __device__ inline bool grid_sync(const KArgs& a, Fn ctl_fn) {
     uint64_t t0 = global_ns();
     unsigned polls = 0;
     while (ld_acquire(&a.bar[1]) < s_target) {
-      __nanosleep(32);
+      __nanosleep(20);
       if ((++polls & 1023u) == 0u) {
-        if (ld_acquire(&a.bar[2]) & kErrBarrierTimeout) {
+        if (ld_acquire(&a.bar[2]) & (kErrBarrierTimeout | kErrCopyTimeout)) {
           s_fail = 1;
           break;
         }
@@ -208,19 +251,30 @@ struct NoCtl {
   __device__ void operator()() const {}
 };
 
+// Sum of -q over B-side contacts, then +q over A-side contacts, ascending
+// contact order (the flat incidence list); loads are issued in groups of
+// eight, the additions stay in order.
 __device__ inline double4 gather_q(const KArgs& a, int b) {
   double ax = 0.0, ay = 0.0, az = 0.0;
-  int s = __ldg(a.bstart + b), e = __ldg(a.bstart + b + 1);
-  for (int i = s; i < e; ++i) {
-    int c = (int)__ldg(a.binc + i);
-    double4 q = a.q[c];
-    ax = ax - q.x; ay = ay - q.y; az = az - q.z;
-  }
-  s = __ldg(a.abase + b);
-  e = __ldg(a.abase + b + 1);
-  for (int c = s; c < e; ++c) {
-    double4 q = a.q[c];
-    ax = ax + q.x; ay = ay + q.y; az = az + q.z;
+  const int s = __ldg(a.inc_start + b), e = __ldg(a.inc_start + b + 1);
+  for (int i = s; i < e; i += 8) {
+    uint32_t c[8];
+    double4 q[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) c[j] = (i + j < e) ? __ldg(a.inc + i + j) : 0u;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      q[j] = (i + j < e) ? a.q[c[j] & 0x7fffffffu] : make_double4(0, 0, 0, 0);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (i + j < e) {
+        if (c[j] & 0x80000000u) {
+          ax = ax - q[j].x; ay = ay - q[j].y; az = az - q[j].z;
+        } else {
+          ax = ax + q[j].x; ay = ay + q[j].y; az = az + q[j].z;
+        }
+      }
+    }
   }
   return make_double4(ax, ay, az, 0.0);
 }
@@ -239,15 +293,74 @@ __device__ inline void body_pass_schur(const KArgs& a) {
   }
 }
 
-__device__ inline void write_partials(const KArgs& a, int tile, int qbase, const double* v, int nq) {
-  if (threadIdx.x == 0)
-    for (int qi = 0; qi < nq; ++qi) a.part[(size_t)(qbase + qi) * a.ptiles + tile] = v[qi];
+// A buffer holding none of the iterates in use (5 buffers, at most 4 in use).
+__device__ inline int free_slot(int a, int b, int c, int d) {
+  for (int i = 0; i < 5; ++i)
+    if (i != a && i != b && i != c && i != d) return i;
+  return 0;
 }
 
-__global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
+// ---------------------------------------------------------------------------
+// Shared-memory staging of the look-ahead pass, per warp.  A CTA walks its
+// sub-tiles (256 consecutive contacts, kItemsPerThread per reduction tile) in
+// order; warp w owns contacts [32w, 32w+32) of each sub-tile and two stages of
+// its own.  While the warp computes sub-tile i from one stage, its lane 0 has
+// already issued the bulk copies of sub-tile i+1's plane segments (256 bytes
+// per plane) into the other stage, completed on the warp's own mbarrier, so
+// warps never wait for each other except at the per-tile reduction.
+// ---------------------------------------------------------------------------
+constexpr int kWarps = kThreads / 32;
+constexpr int kSub = kThreads;  // contacts per sub-tile
+__host__ __device__ constexpr int kFramePlanes(int mode) { return mode == 0 ? 9 : 3; }
+__host__ __device__ constexpr int kStagePlanesD(int mode) { return kFramePlanes(mode) + 12; }
+__host__ __device__ constexpr unsigned kWarpStageBytes(int mode) {
+  return (unsigned)kStagePlanesD(mode) * 32u * 8u + 2u * 32u * 4u;
+}
+__host__ __device__ constexpr size_t kDynSmem(int mode) {
+  return (size_t)kWarps * 2 * kWarpStageBytes(mode) + (size_t)kWarps * 2 * 8;
+}
+
+struct Staging {
+  unsigned char* base;  // warp w, stage s at base + (2w + s) * stage_bytes
+  unsigned stage_bytes;
+  uint64_t* bar;        // mbarrier of warp w, stage s: bar[2w + s]
+  unsigned phase;       // bit s: parity the next wait on this warp's stage s expects
+};
+
+// Bounded wait for this warp's stage s; false after a timeout (error recorded).
+__device__ inline bool wait_warp_stage(const KArgs& a, Staging& st, int s) {
+  const int w = threadIdx.x >> 5;
+  unsigned par = (st.phase >> s) & 1u;
+  uint64_t* bar = st.bar + 2 * w + s;
+  bool ok = mbar_try_wait(bar, par);
+  if (!ok) {
+    uint64_t t0 = global_ns();
+    while (!(ok = mbar_try_wait(bar, par))) {
+      if (global_ns() - t0 > kBarrierTimeoutNs) break;
+    }
+  }
+  st.phase ^= (1u << s);
+  if (!ok) atomicOr(&a.bar[2], kErrCopyTimeout);
+  __syncwarp();
+  return ok;
+}
+
+template <int kFrame, int kMinB>
+__global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs a) {
   __shared__ double scratch[kNQ * 8 + 8];
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
   const size_t S = a.S;
   const double h = a.h;
+  Staging stg;
+  stg.base = dyn_smem;
+  stg.stage_bytes = kWarpStageBytes(kFrame);
+  stg.bar = reinterpret_cast<uint64_t*>(dyn_smem + (size_t)kWarps * 2 * stg.stage_bytes);
+  stg.phase = 0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2 * kWarps; ++i) mbar_init(stg.bar + i, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
 
   // ---- applied impulse: k = m v + h f (m = 1/minv, 0 for fixed); w = minv k
   for (int bt = blockIdx.x; bt < a.nbt; bt += gridDim.x) {
@@ -262,15 +375,15 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
       a.w4[b] = make_double4(mi * k.x, mi * k.y, mi * k.z, 0.0);
     }
   }
-  if (!grid_sync(a, NoCtl{})) return;
+  if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
-  // ---- r = D (Minv k) + b; gamma_0; y_0; d = gamma_0 - gamma_hat_0 (= gamma_0 - 1)
+  // ---- r = D (Minv k) + b; gamma_0 -> G[0]; e = gamma_0 - gamma_hat_0 (= gamma_0 - 1)
   for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
     double acc[1] = {0.0};
     for (int m = 0; m < kItemsPerThread; ++m) {
       int c = tile * kTileItems + m * kThreads + threadIdx.x;
       if (c < a.nc) {
-        Frame f = load_frame(a, c);
+        Frame f = load_frame<kFrame>(a, c);
         double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
         double d0, d1, d2;
         ft_times(f, wa, wb, &d0, &d1, &d2);
@@ -287,45 +400,44 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
           g0 = 1.0; g1 = 0.0; g2 = 0.0;
         }
         a.G[0][0 * S + c] = g0; a.G[0][1 * S + c] = g1; a.G[0][2 * S + c] = g2;
-        a.Y[0][0 * S + c] = g0; a.Y[0][1 * S + c] = g1; a.Y[0][2 * S + c] = g2;
         double e0 = g0 + (-1.0), e1 = g1 + (-1.0), e2 = g2 + (-1.0);
         acc[0] = acc[0] + dot3i(e0, e1, e2, e0, e1, e2);
         a.q[c] = f_times(f, e0, e1, e2);
       }
     }
     block_fold_multi<1>(acc, scratch);
-    write_partials(a, tile, 0, acc, 1);
+    write_partials<1>(a, tile, acc);
   }
-  if (!grid_sync(a, [&]() {
+  if (!grid_sync(a, kPhaseSetup, [&]() {
         double s[1];
-        fold_tiles<1>(a, 0, s, scratch);
+        fold_tiles<1>(a, s, scratch);
         if (threadIdx.x == 0) a.ctl->L0 = sqrt(s[0]);
       }))
     return;
   body_pass_schur(a);
-  if (!grid_sync(a, NoCtl{})) return;
+  if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
-  // ---- L = ||N d|| / ||d||; q = F gamma_0 for the first N y
+  // ---- L = ||N e|| / ||e||; q = F gamma_0 for the first N y
   for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
     double acc[1] = {0.0};
     for (int m = 0; m < kItemsPerThread; ++m) {
       int c = tile * kTileItems + m * kThreads + threadIdx.x;
       if (c < a.nc) {
-        Frame f = load_frame(a, c);
+        Frame f = load_frame<kFrame>(a, c);
         double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
         double n0, n1, n2;
         ft_times(f, wa, wb, &n0, &n1, &n2);
         acc[0] = acc[0] + dot3i(n0, n1, n2, n0, n1, n2);
-        double y0 = a.Y[0][0 * S + c], y1 = a.Y[0][1 * S + c], y2 = a.Y[0][2 * S + c];
+        double y0 = a.G[0][0 * S + c], y1 = a.G[0][1 * S + c], y2 = a.G[0][2 * S + c];
         a.q[c] = f_times(f, y0, y1, y2);
       }
     }
     block_fold_multi<1>(acc, scratch);
-    write_partials(a, tile, 0, acc, 1);
+    write_partials<1>(a, tile, acc);
   }
-  if (!grid_sync(a, [&]() {
+  if (!grid_sync(a, kPhaseSetup, [&]() {
         double s[1];
-        fold_tiles<1>(a, 0, s, scratch);
+        fold_tiles<1>(a, s, scratch);
         if (threadIdx.x == 0) {
           ApgdCtl* C = a.ctl;
           double L = sqrt(s[0]) / C->L0;
@@ -347,91 +459,74 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
           C->sweeps = 0;
           C->restart = 0;
           C->cur = 0;
-          C->hat = kHatNone;
-          C->hat_pending = 0;
+          C->prev = -1;
+          C->nw = 1;
+          C->best = -1;
+          C->yr = 1;
+          C->yb = 0.0;
+          C->first = 1;
           C->backtracks = 0;
           C->obj1 = C->obj2 = C->obj2_base = 0.0;
         }
       }))
     return;
   body_pass_schur(a);
-  if (!grid_sync(a, NoCtl{})) return;
+  if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
   // ---- APGD iterations (APGD.cu:227-350)
+  //
+  // Each iteration is one body pass (w = Minv D^T q of gamma_new) and one
+  // contact pass that computes N gamma_new, the objective and the residual of
+  // iteration k, and -- assuming the Lipschitz test accepts gamma_new -- the
+  // whole step of iteration k+1 (y, N y, g, gamma_new = P(y - t g), q).  When
+  // the test fails (backtracking) the look-ahead is discarded and a step pass
+  // recomputes gamma_new with the doubled L; the arithmetic of every value is
+  // the same either way.
+  bool step_pass = true;  // the first iteration's step: N y_0 is a product (w of gamma_0)
   for (;;) {
-    const int done = __ldcg(&a.ctl->done);
-    if (done) break;
-    const int mode = __ldcg(&a.ctl->mode);
-    const int cur = __ldcg(&a.ctl->cur);
-    const double t = __ldcg(&a.ctl->t);
-    const double nt_ = -t;
-    const double* Gc = a.G[cur];
-    double* Gn = a.G[cur ^ 1];
-    const double* Yc = a.Y[cur];
-    if (mode == 0) {
-      // g = N y + r; gamma_new = P(y - t g)
-      const int copy_hat = __ldcg(&a.ctl->hat_pending);
+    if (__ldcg(&a.ctl->done)) break;  // maxIterations reached (0 included)
+    if (step_pass) {
+      const int first = __ldcg(&a.ctl->first);
+      const int cur = __ldcg(&a.ctl->cur);
+      const int prev = __ldcg(&a.ctl->prev);
+      const int nw = __ldcg(&a.ctl->nw);
+      const int yr = __ldcg(&a.ctl->yr);
+      const double yb = __ldcg(&a.ctl->yb);
+      const double ya = 1.0 + yb, ym = -yb;
+      const double nt_ = -__ldcg(&a.ctl->t);
+      const double* Gc = a.G[cur];
+      const double* Gp = a.G[prev < 0 ? cur : prev];
+      double* NGc = a.NG[cur];
+      const double* NGp = a.NG[prev < 0 ? cur : prev];
+      double* Gn = a.G[nw];
       for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         for (int m = 0; m < kItemsPerThread; ++m) {
           int c = tile * kTileItems + m * kThreads + threadIdx.x;
           if (c < a.nc) {
-            Frame f = load_frame(a, c);
-            double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
-            double N0, N1, N2;
-            ft_times(f, wa, wb, &N0, &N1, &N2);
+            Frame f = load_frame<kFrame>(a, c);
+            double c0 = Gc[0 * S + c], c1 = Gc[1 * S + c], c2 = Gc[2 * S + c];
+            double y0, y1, y2, N0, N1, N2;
+            if (yr) {
+              y0 = c0; y1 = c1; y2 = c2;
+            } else {
+              y0 = ya * c0 + ym * Gp[0 * S + c];
+              y1 = ya * c1 + ym * Gp[1 * S + c];
+              y2 = ya * c2 + ym * Gp[2 * S + c];
+            }
+            if (first) {
+              double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
+              ft_times(f, wa, wb, &N0, &N1, &N2);
+              NGc[0 * S + c] = N0; NGc[1 * S + c] = N1; NGc[2 * S + c] = N2;
+            } else if (yr) {
+              N0 = NGc[0 * S + c]; N1 = NGc[1 * S + c]; N2 = NGc[2 * S + c];
+            } else {
+              N0 = ya * NGc[0 * S + c] + ym * NGp[0 * S + c];
+              N1 = ya * NGc[1 * S + c] + ym * NGp[1 * S + c];
+              N2 = ya * NGc[2 * S + c] + ym * NGp[2 * S + c];
+            }
             double r0 = a.r[0 * S + c], r1 = a.r[1 * S + c], r2 = a.r[2 * S + c];
-            double y0 = Yc[0 * S + c], y1 = Yc[1 * S + c], y2 = Yc[2 * S + c];
-            double c0 = Gc[0 * S + c], c1 = Gc[1 * S + c], c2 = Gc[2 * S + c];
             double g0 = N0 + r0, g1 = N1 + r1, g2 = N2 + r2;
-            double x0 = y0 + nt_ * g0, x1 = y1 + nt_ * g1, x2 = y2 + nt_ * g2;
-            project_cone<double>(x0, x1, x2, a.mu);
-            a.g[0 * S + c] = g0; a.g[1 * S + c] = g1; a.g[2 * S + c] = g2;
-            Gn[0 * S + c] = x0; Gn[1 * S + c] = x1; Gn[2 * S + c] = x2;
-            a.q[c] = f_times(f, x0, x1, x2);
-            if (copy_hat) {
-              a.ghat[0 * S + c] = c0; a.ghat[1 * S + c] = c1; a.ghat[2 * S + c] = c2;
-            }
-            double t0 = x0 + (-1.0) * y0, t1 = x1 + (-1.0) * y1, t2 = x2 + (-1.0) * y2;
-            double s0 = x0 + (-1.0) * c0, s1 = x1 + (-1.0) * c1, s2 = x2 + (-1.0) * c2;
-            acc[0] = acc[0] + dot3i(y0, y1, y2, N0, N1, N2);
-            acc[1] = acc[1] + dot3i(y0, y1, y2, r0, r1, r2);
-            acc[2] = acc[2] + dot3i(g0, g1, g2, t0, t1, t2);
-            acc[3] = acc[3] + dot3i(t0, t1, t2, t0, t1, t2);
-            acc[4] = acc[4] + dot3i(g0, g1, g2, s0, s1, s2);
-          }
-        }
-        block_fold_multi<5>(acc, scratch);
-        write_partials(a, tile, 0, acc, 5);
-      }
-      if (!grid_sync(a, [&]() {
-            double s[5];
-            fold_tiles<5>(a, 0, s, scratch);
-            if (threadIdx.x == 0) {
-              ApgdCtl* C = a.ctl;
-              double L = C->L;
-              C->obj2_base = 0.5 * s[0] + s[1];
-              double nr = sqrt(s[3]);
-              C->obj2 = C->obj2_base + (s[2] + 0.5 * L * (nr * nr));
-              C->restart = (s[4] > 0) ? 1 : 0;
-              if (C->hat_pending) {
-                C->hat_pending = 0;
-                C->hat = kHatBuf;
-              }
-            }
-          }))
-        return;
-    } else {
-      // backtracking step: gamma_new = P(y - t g) with the halved step (APGD.cu:246-261)
-      for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
-        double acc[3] = {0.0, 0.0, 0.0};
-        for (int m = 0; m < kItemsPerThread; ++m) {
-          int c = tile * kTileItems + m * kThreads + threadIdx.x;
-          if (c < a.nc) {
-            Frame f = load_frame(a, c);
-            double y0 = Yc[0 * S + c], y1 = Yc[1 * S + c], y2 = Yc[2 * S + c];
-            double c0 = Gc[0 * S + c], c1 = Gc[1 * S + c], c2 = Gc[2 * S + c];
-            double g0 = a.g[0 * S + c], g1 = a.g[1 * S + c], g2 = a.g[2 * S + c];
             double x0 = y0 + nt_ * g0, x1 = y1 + nt_ * g1, x2 = y2 + nt_ * g2;
             project_cone<double>(x0, x1, x2, a.mu);
             Gn[0 * S + c] = x0; Gn[1 * S + c] = x1; Gn[2 * S + c] = x2;
@@ -441,52 +536,121 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
             acc[0] = acc[0] + dot3i(g0, g1, g2, t0, t1, t2);
             acc[1] = acc[1] + dot3i(t0, t1, t2, t0, t1, t2);
             acc[2] = acc[2] + dot3i(g0, g1, g2, s0, s1, s2);
+            if (first) {
+              acc[3] = acc[3] + dot3i(y0, y1, y2, N0, N1, N2);
+              acc[4] = acc[4] + dot3i(y0, y1, y2, r0, r1, r2);
+            }
           }
         }
-        block_fold_multi<3>(acc, scratch);
-        write_partials(a, tile, 0, acc, 3);
+        block_fold_multi<5>(acc, scratch);
+        write_partials<5>(a, tile, acc);
       }
-      if (!grid_sync(a, [&]() {
-            double s[3];
-            fold_tiles<3>(a, 0, s, scratch);
+      if (!grid_sync(a, first ? kPhaseStep : kPhaseBacktrack, [&]() {
+            double s[5];
+            fold_tiles<5>(a, s, scratch);
             if (threadIdx.x == 0) {
               ApgdCtl* C = a.ctl;
-              double L = C->L;
+              if (C->first) C->obj2_base = 0.5 * s[3] + s[4];
               double nr = sqrt(s[1]);
-              C->obj2 = C->obj2_base + (s[0] + 0.5 * L * (nr * nr));
+              C->obj2 = C->obj2_base + (s[0] + 0.5 * C->L * (nr * nr));
               C->restart = (s[2] > 0) ? 1 : 0;
+              C->first = 0;
             }
           }))
         return;
     }
     body_pass_schur(a);
-    if (!grid_sync(a, NoCtl{})) return;
+    if (!grid_sync(a, kPhaseBody, NoCtl{})) return;
 
-    // N gamma_new: objective, residual (APGD.cu:90-102), speculative y_new
+    // N gamma_new, objective (APGD.cu:237-238), residual (:90-102); then the
+    // next iteration's step assuming gamma_new is accepted (:266-273, 312-332)
     {
+      const int cur = __ldcg(&a.ctl->cur);
+      const int prev = __ldcg(&a.ctl->prev);
+      const int nw = __ldcg(&a.ctl->nw);
+      const int best = __ldcg(&a.ctl->best);
+      const int nw2 = free_slot(nw, cur, prev, best);
+      const int restart = __ldcg(&a.ctl->restart);
+      const double beta = __ldcg(&a.ctl->beta);
+      const double ya = 1.0 + beta, ym = -beta;
+      const double Lnext = 0.9 * __ldcg(&a.ctl->L);
+      const double nt2 = -(1.0 / Lnext);
       const double gd = __ldcg(&a.ctl->gdiff);
       const double gA = __ldcg(&a.ctl->ginv);
       const double gB = -1.0 / gd;
-      const int restart = __ldcg(&a.ctl->restart);
-      const double beta = __ldcg(&a.ctl->beta);
-      const double opb = 1.0 + beta, mb = -beta;
-      double* Yn = a.Y[cur ^ 1];
-      for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
-        double acc[2] = {0.0, 0.0};
-        double mx = 0.0;
-        bool bad = false;
-        for (int m = 0; m < kItemsPerThread; ++m) {
-          int c = tile * kTileItems + m * kThreads + threadIdx.x;
-          if (c < a.nc) {
-            Frame f = load_frame(a, c);
-            double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
-            double N0, N1, N2;
-            ft_times(f, wa, wb, &N0, &N1, &N2);
-            double r0 = a.r[0 * S + c], r1 = a.r[1 * S + c], r2 = a.r[2 * S + c];
-            double x0 = Gn[0 * S + c], x1 = Gn[1 * S + c], x2 = Gn[2 * S + c];
-            double c0 = Gc[0 * S + c], c1 = Gc[1 * S + c], c2 = Gc[2 * S + c];
-            acc[0] = acc[0] + dot3i(x0, x1, x2, N0, N1, N2);
-            acc[1] = acc[1] + dot3i(x0, x1, x2, r0, r1, r2);
+      double* NGn = a.NG[nw];
+      double* G2 = a.G[nw2];
+      // staged planes: frame, gamma_new, r, gamma_k, N gamma_k; then ids A, B
+      constexpr int FP = kFramePlanes(kFrame);
+      constexpr int ND = kStagePlanesD(kFrame);
+      const double* dsrc[ND];
+#pragma unroll
+      for (int p = 0; p < FP; ++p) dsrc[p] = a.F + p * S;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        dsrc[FP + k] = a.G[nw] + k * S;
+        dsrc[FP + 3 + k] = a.r + k * S;
+        dsrc[FP + 6 + k] = a.G[cur] + k * S;
+        dsrc[FP + 9 + k] = a.NG[cur] + k * S;
+      }
+      const int nd_copy = restart ? FP + 6 : ND;
+      const unsigned bytes = (unsigned)nd_copy * 32u * 8u + 2u * 32u * 4u;
+      const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int my_tiles =
+          (blockIdx.x < (unsigned)a.nt) ? (a.nt - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+      const int nsub = kItemsPerThread * my_tiles;
+      // first contact of this warp's chunk of sub-tile i
+      auto chunk_c0 = [&](int i) {
+        return ((int)blockIdx.x + (i / kItemsPerThread) * (int)gridDim.x) * kTileItems +
+               (i % kItemsPerThread) * kSub + warp * 32;
+      };
+      auto issue = [&](int i, int sidx) {
+        int cw = chunk_c0(i);
+        if (lane == 0 && cw < a.nc) {
+          unsigned char* dst = stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes;
+          uint64_t* bar = stg.bar + 2 * warp + sidx;
+          // order this warp's earlier generic reads of the stage before the copies
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive_expect_tx(bar, bytes);
+          for (int p = 0; p < nd_copy; ++p) bulk_g2s(dst + (size_t)p * 256, dsrc[p] + cw, 256, bar);
+          bulk_g2s(dst + (size_t)ND * 256, a.ida + cw, 128, bar);
+          bulk_g2s(dst + (size_t)ND * 256 + 128, a.idb + cw, 128, bar);
+        }
+      };
+      double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      double mx = 0.0;
+      bool bad = false, failed = false;
+      if (nsub > 0) issue(0, 0);
+      for (int i = 0; i < nsub; ++i) {
+        const int sidx = i & 1;
+        __syncwarp();  // the warp's reads of stage sidx^1 (sub-tile i-1) are done
+        if (i + 1 < nsub) issue(i + 1, sidx ^ 1);
+        const int cw = chunk_c0(i);
+        if (cw < a.nc && !failed) {
+          if (!wait_warp_stage(a, stg, sidx)) failed = true;
+        }
+        const int c = cw + lane;
+        if (c < a.nc && !failed) {
+          const double* sd =
+              reinterpret_cast<const double*>(stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes);
+          const uint32_t* su = reinterpret_cast<const uint32_t*>(sd + (size_t)ND * 32);
+          const int j = lane;
+          Frame f;
+          f.n0 = sd[0 * 32 + j]; f.n1 = sd[1 * 32 + j]; f.n2 = sd[2 * 32 + j];
+          if (kFrame == 0) {
+            f.u0 = sd[3 * 32 + j]; f.u1 = sd[4 * 32 + j]; f.u2 = sd[5 * 32 + j];
+            f.v0 = sd[6 * 32 + j]; f.v1 = sd[7 * 32 + j]; f.v2 = sd[8 * 32 + j];
+          }
+          complete_frame(f, kFrame);
+          double4 wa = a.w4[su[j]], wb = a.w4[su[32 + j]];
+          double N0, N1, N2;
+          ft_times(f, wa, wb, &N0, &N1, &N2);
+          NGn[0 * S + c] = N0; NGn[1 * S + c] = N1; NGn[2 * S + c] = N2;
+          double x0 = sd[(FP + 0) * 32 + j], x1 = sd[(FP + 1) * 32 + j], x2 = sd[(FP + 2) * 32 + j];
+          double r0 = sd[(FP + 3) * 32 + j], r1 = sd[(FP + 4) * 32 + j], r2 = sd[(FP + 5) * 32 + j];
+          acc[0] = acc[0] + dot3i(x0, x1, x2, N0, N1, N2);
+          acc[1] = acc[1] + dot3i(x0, x1, x2, r0, r1, r2);
+          {
             double T0 = r0 + N0, T1 = r1 + N1, T2 = r2 + N2;
             T0 = x0 + (-gd) * T0; T1 = x1 + (-gd) * T1; T2 = x2 + (-gd) * T2;
             project_cone<double>(T0, T1, T2, a.mu);
@@ -494,27 +658,49 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
             double m0 = fabs(T0), m1 = fabs(T1), m2 = fabs(T2);
             bad |= (m0 != m0) || (m1 != m1) || (m2 != m2);
             mx = fmax(mx, fmax(m0, fmax(m1, m2)));
-            double y0, y1, y2;
-            if (restart) {
-              y0 = x0; y1 = x1; y2 = x2;
-            } else {
-              y0 = opb * x0 + mb * c0; y1 = opb * x1 + mb * c1; y2 = opb * x2 + mb * c2;
-            }
-            Yn[0 * S + c] = y0; Yn[1 * S + c] = y1; Yn[2 * S + c] = y2;
-            a.q[c] = f_times(f, y0, y1, y2);
           }
+          // look-ahead step of iteration k+1: y = (1+b) x - b gamma_k, or x after a restart
+          double y0, y1, y2, M0, M1, M2;
+          if (restart) {
+            y0 = x0; y1 = x1; y2 = x2;
+            M0 = N0; M1 = N1; M2 = N2;
+          } else {
+            double c0v = sd[(FP + 6) * 32 + j], c1v = sd[(FP + 7) * 32 + j], c2v = sd[(FP + 8) * 32 + j];
+            y0 = ya * x0 + ym * c0v; y1 = ya * x1 + ym * c1v; y2 = ya * x2 + ym * c2v;
+            M0 = ya * N0 + ym * sd[(FP + 9) * 32 + j];
+            M1 = ya * N1 + ym * sd[(FP + 10) * 32 + j];
+            M2 = ya * N2 + ym * sd[(FP + 11) * 32 + j];
+          }
+          double g0 = M0 + r0, g1 = M1 + r1, g2 = M2 + r2;
+          double z0 = y0 + nt2 * g0, z1 = y1 + nt2 * g1, z2 = y2 + nt2 * g2;
+          project_cone<double>(z0, z1, z2, a.mu);
+          G2[0 * S + c] = z0; G2[1 * S + c] = z1; G2[2 * S + c] = z2;
+          a.q[c] = f_times(f, z0, z1, z2);
+          double t0 = z0 + (-1.0) * y0, t1 = z1 + (-1.0) * y1, t2 = z2 + (-1.0) * y2;
+          double s0 = z0 + (-1.0) * x0, s1 = z1 + (-1.0) * x1, s2 = z2 + (-1.0) * x2;
+          acc[2] = acc[2] + dot3i(g0, g1, g2, t0, t1, t2);
+          acc[3] = acc[3] + dot3i(t0, t1, t2, t0, t1, t2);
+          acc[4] = acc[4] + dot3i(g0, g1, g2, s0, s1, s2);
+          acc[5] = acc[5] + dot3i(y0, y1, y2, M0, M1, M2);
+          acc[6] = acc[6] + dot3i(y0, y1, y2, r0, r1, r2);
         }
-        if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&a.bar[2], kErrNaN);
-        block_fold_multi<2>(acc, scratch);
-        write_partials(a, tile, 0, acc, 2);
-        double bm = block_max256(mx, scratch);
-        if (threadIdx.x == 0) a.part[(size_t)kQMax * a.ptiles + tile] = bm;
-        __syncthreads();
+        if ((i % kItemsPerThread) == kItemsPerThread - 1) {
+          const int tile = (int)blockIdx.x + (i / kItemsPerThread) * (int)gridDim.x;
+          if (__syncthreads_or(failed)) return;
+          if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&a.bar[2], kErrNaN);
+          block_fold_multi<7>(acc, scratch);
+          write_partials<7>(a, tile, acc);
+          double bm = block_max256(mx, scratch);
+          if (threadIdx.x == 0) a.part[(size_t)kQMax * a.ptiles + tile] = bm;
+          for (int qq = 0; qq < 7; ++qq) acc[qq] = 0.0;
+          mx = 0.0;
+          bad = false;
+        }
       }
     }
-    if (!grid_sync(a, [&]() {
-          double s[2];
-          fold_tiles<2>(a, 0, s, scratch);
+    if (!grid_sync(a, kPhaseProduct, [&]() {
+          double s[7];
+          fold_tiles<7>(a, s, scratch);
           double res = fold_tiles_max(a, scratch);
           if (threadIdx.x == 0) {
             ApgdCtl* C = a.ctl;
@@ -535,24 +721,26 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
             } else {
               C->mode = 0;
               C->sweeps += 1;
+              int old_best = C->best;
               if (res < C->residual) {
                 C->residual = res;
                 C->objective = obj1;
-                C->hat = kHatNew;
+                C->best = C->nw;
               }
               if (C->residual < a.tol) {
                 C->done = 1;
                 C->iterations = C->k;
               } else {
                 double th = C->restart ? 1.0 : C->theta_new;
+                C->yb = C->beta;
+                C->yr = C->restart;
                 C->L = 0.9 * C->L;
                 C->t = 1.0 / C->L;
                 C->theta = th;
-                C->cur ^= 1;
-                if (C->hat == kHatNew) {
-                  C->hat = kHatCur;
-                  C->hat_pending = 1;
-                }
+                int nw2 = free_slot(C->nw, C->cur, C->prev, old_best);
+                C->prev = C->cur;
+                C->cur = C->nw;
+                C->nw = nw2;
                 C->k += 1;
                 if (C->k >= a.max_iter) {
                   C->done = 1;
@@ -560,28 +748,25 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
                 } else {
                   C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
                   C->beta = th * (1.0 - th) / (th * th + C->theta_new);
+                  // the look-ahead step is now iteration k's step
+                  C->obj2_base = 0.5 * s[5] + s[6];
+                  double nr = sqrt(s[3]);
+                  C->obj2 = C->obj2_base + (s[2] + 0.5 * C->L * (nr * nr));
+                  C->restart = (s[4] > 0) ? 1 : 0;
                 }
               }
             }
           }
         }))
       return;
-    const int mode2 = __ldcg(&a.ctl->mode);
-    const int done2 = __ldcg(&a.ctl->done);
-    if (done2) break;
-    if (mode2 == 1) continue;
-    body_pass_schur(a);
-    if (!grid_sync(a, NoCtl{})) return;
+    if (__ldcg(&a.ctl->done)) break;
+    step_pass = (__ldcg(&a.ctl->mode) == 1);
   }
 
   // ---- gamma = gamma_hat (APGD.cu:358); q = F gamma for D^T gamma
   {
-    const int hat = __ldcg(&a.ctl->hat);
-    const int cur = __ldcg(&a.ctl->cur);
-    const double* src = nullptr;
-    if (hat == kHatBuf) src = a.ghat;
-    else if (hat == kHatCur) src = a.G[cur];
-    else if (hat == kHatNew) src = a.G[cur ^ 1];
+    const int best = __ldcg(&a.ctl->best);
+    const double* src = best >= 0 ? a.G[best] : nullptr;
     for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
       for (int m = 0; m < kItemsPerThread; ++m) {
         int c = tile * kTileItems + m * kThreads + threadIdx.x;
@@ -593,13 +778,13 @@ __global__ void __launch_bounds__(kThreads) k_step_solve(KArgs a) {
           a.gamma[0 * a.GS + c] = x0;
           a.gamma[1 * a.GS + c] = x1;
           a.gamma[2 * a.GS + c] = x2;
-          Frame f = load_frame(a, c);
+          Frame f = load_frame<kFrame>(a, c);
           a.q[c] = f_times(f, x0, x1, x2);
         }
       }
     }
   }
-  if (!grid_sync(a, NoCtl{})) return;
+  if (!grid_sync(a, kPhaseFinal, NoCtl{})) return;
 
   // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v
   const double invh = 1.0 / h;
@@ -639,6 +824,46 @@ __global__ void __launch_bounds__(kThreads) k_step_nocontact(int nb, double h,
   p4[b] = make_double4(h * v.x + p.x, h * v.y + p.y, h * v.z + p.z, 0.0);
 }
 
+// Frame mode and register budget of the solve kernel; DVIDE_FRAME_MODE=0
+// (frames loaded) and DVIDE_MIN_BLOCKS=3 select the other variants for timing
+// comparisons.
+int frame_mode_selected() {
+  static int sel = -1;
+  if (sel < 0) {
+    const char* e = getenv("DVIDE_FRAME_MODE");
+    sel = (e && e[0] == '0') ? 0 : 1;
+  }
+  return sel;
+}
+
+// CTAs per SM the register budget is set for (2: 128 registers; 3: 80);
+// DVIDE_MIN_BLOCKS=3 selects the second for timing comparisons.
+int min_blocks_selected() {
+  static int sel = -1;
+  if (sel < 0) {
+    const char* e = getenv("DVIDE_MIN_BLOCKS");
+    sel = (e && e[0] == '3') ? 3 : 2;
+  }
+  return sel;
+}
+
+const void* solve_kernel() {
+  int fm = frame_mode_selected();
+  if (min_blocks_selected() == 3)
+    return fm == 0 ? (const void*)k_step_solve<0, 3> : (const void*)k_step_solve<1, 3>;
+  return fm == 0 ? (const void*)k_step_solve<0, 2> : (const void*)k_step_solve<1, 2>;
+}
+
+size_t solve_smem() { return kDynSmem(frame_mode_selected()); }
+
+void prepare_solve_kernel() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(solve_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)solve_smem());
+  done = true;
+}
+
 }  // namespace
 
 int apgd_max_ctas(int precision) {
@@ -646,7 +871,8 @@ int apgd_max_ctas(int precision) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve, kThreads, 0);
+  prepare_solve_kernel();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_kernel(), kThreads, solve_smem());
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
@@ -671,15 +897,12 @@ void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, in
   a.F = sd.F;
   a.gap = sd.gap;
   a.r = sd.r;
-  a.abase = sd.cbase;
-  a.bstart = sd.binc_start;
-  a.binc = sd.binc;
-  a.G[0] = sd.G0;
-  a.G[1] = sd.G1;
-  a.Y[0] = sd.Y0;
-  a.Y[1] = sd.Y1;
-  a.g = sd.gv;
-  a.ghat = sd.ghat;
+  a.inc_start = sd.inc_start;
+  a.inc = sd.inc;
+  for (int k = 0; k < 5; ++k) {
+    a.G[k] = sd.G[k];
+    a.NG[k] = sd.NG[k];
+  }
   a.q = sd.q;
   a.gamma = sd.gamma;
   a.part = sd.part;
@@ -694,8 +917,10 @@ void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, in
   a.warm = cfg.warm;
   int grid = cfg.grid;
   cudaMemsetAsync(sd.bar, 0, 4 * sizeof(unsigned), st);
+  cudaMemsetAsync(sd.ctl, 0, sizeof(ApgdCtl), st);
   void* params[] = {&a};
-  cudaLaunchCooperativeKernel((const void*)k_step_solve, dim3(grid), dim3(kThreads), params, 0, st);
+  prepare_solve_kernel();
+  cudaLaunchCooperativeKernel(solve_kernel(), dim3(grid), dim3(kThreads), params, solve_smem(), st);
   ++*launches;
   cudaMemcpyAsync(sd.h_ctl, sd.ctl, sizeof(ApgdCtl), cudaMemcpyDeviceToHost, st);
 }

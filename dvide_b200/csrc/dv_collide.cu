@@ -444,6 +444,29 @@ __global__ void __launch_bounds__(kThreads) k_count_b(const uint32_t* __restrict
   vals[c] = (uint32_t)c;
 }
 
+// Per-body incidence length: contacts where the body is B plus where it is A.
+__global__ void __launch_bounds__(kThreads) k_inc_count(int nb, const int* __restrict__ bstart,
+                                                       const int* __restrict__ abase,
+                                                       int* __restrict__ cnt) {
+  int b = blockIdx.x * kThreads + threadIdx.x;
+  if (b >= nb) return;
+  cnt[b] = (bstart[b + 1] - bstart[b]) + (abase[b + 1] - abase[b]);
+}
+
+// B-side contacts (flagged, ascending) then the A-side range: the ascending
+// contact order of the body's column of D.
+__global__ void __launch_bounds__(kThreads) k_inc_fill(int nb, const int* __restrict__ bstart,
+                                                      const uint32_t* __restrict__ binc,
+                                                      const int* __restrict__ abase,
+                                                      const int* __restrict__ istart,
+                                                      uint32_t* __restrict__ inc) {
+  int b = blockIdx.x * kThreads + threadIdx.x;
+  if (b >= nb) return;
+  int o = istart[b];
+  for (int i = bstart[b]; i < bstart[b + 1]; ++i) inc[o++] = binc[i] | 0x80000000u;
+  for (int c = abase[b]; c < abase[b + 1]; ++c) inc[o++] = (uint32_t)c;
+}
+
 CollideArgs make_args(SceneDev& sd, double env) {
   CollideArgs a;
   a.nb = sd.nb;
@@ -549,6 +572,17 @@ void collide_write(SceneDev& sd, double env, cudaStream_t st, int64_t* launches)
   exclusive_scan_i32(sd.cnt_cand, sd.binc_start, nb, sd.scan_tmp, st, launches);
   if (nc > 0)
     cudaMemcpyAsync(sd.binc, sd.valA, sizeof(uint32_t) * (size_t)nc, cudaMemcpyDeviceToDevice, st);
+  int gb = (nb + kThreads - 1) / kThreads;
+  if (nb > 0) {
+    k_inc_count<<<gb, kThreads, 0, st>>>(nb, sd.binc_start, sd.cbase, sd.cnt_cand);
+    ++*launches;
+  }
+  exclusive_scan_i32(sd.cnt_cand, sd.inc_start, nb, sd.scan_tmp, st, launches);
+  if (nb > 0 && nc > 0) {
+    k_inc_fill<<<gb, kThreads, 0, st>>>(nb, sd.binc_start, sd.binc, sd.cbase, sd.inc_start,
+                                        sd.inc);
+    ++*launches;
+  }
 }
 
 }  // namespace dv

@@ -10,13 +10,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/dvide.h"
+#include "dvide.h"
 
 namespace dv {
 
 constexpr int kThreads = 256;       // threads per CTA in every pass
-constexpr int kTileItems = 1024;    // items per reduction tile (4 per thread)
-constexpr int kItemsPerThread = 4;
+constexpr int kTileItems = 512;     // items per reduction tile (2 per thread)
+constexpr int kItemsPerThread = 2;
 
 // ---------------------------------------------------------------------------
 // helper_math_double.h semantics (host build): length = (double)sqrtf(float),
@@ -160,6 +160,43 @@ __device__ inline uint64_t global_ns() {
   return t;
 }
 
+// ---------------------------------------------------------------------------
+// Bulk asynchronous copies (TMA, no multicast) into shared memory, completed
+// on an mbarrier.  Addresses and sizes must be multiples of 16 bytes.
+// ---------------------------------------------------------------------------
+__device__ inline uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ inline void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ inline void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ inline void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ inline void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ inline bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Error bits recorded by kernels (host reads them after the step).
 enum : unsigned {
   kErrBarrierTimeout = 1u,
@@ -167,6 +204,7 @@ enum : unsigned {
   kErrBacktrackCap = 4u,
   kErrCapacity = 8u,
   kErrAborted = 16u,
+  kErrCopyTimeout = 32u,
 };
 
 // Longest a CTA waits at a grid barrier before it records a timeout and

@@ -34,7 +34,10 @@ struct GridInfo {
 };
 
 // Scalar state of one APGD solve, owned by the controller CTA of the
-// persistent kernel (APGD.cu:208-223, 266-332).
+// persistent kernel (APGD.cu:208-223, 266-332).  Iterates live in five
+// rotating buffers G[0..4] with their Schur products NG[0..4]: cur = gamma_k,
+// prev = gamma_{k-1}, nw = target of gamma_new, best = gamma_hat (-1 before the
+// first accepted iterate); the fifth holds the next iterate computed ahead.
 struct ApgdCtl {
   double L, t, theta, theta_new, beta;
   double obj1, obj2, obj2_base;
@@ -42,17 +45,23 @@ struct ApgdCtl {
   double objective;     // objective of the best iterate (APGD.cu:353-354)
   double gdiff, ginv;   // 1 / nc^2 and its reciprocal (APGD.cu:92, 98)
   double L0;
+  double yb;            // beta used for y_k = (1+yb) gamma_k - yb gamma_{k-1}
   int k;                // iteration index
   int mode;             // next contact pass: 0 full iteration, 1 backtrack
   int done;
   int restart;          // g.(gamma_new - gamma) > 0 for the current gamma_new
-  int cur;              // buffer parity: G[cur] = gamma_k, Y[cur] = y_k
-  int hat;              // where gamma_hat lives: 0 none (fill 1), 1 ghat, 2 G[cur], 3 G[cur^1]
-  int hat_pending;      // copy G[cur] into ghat during the next full pass
+  int cur, prev, nw, best;
+  int yr;               // y_k = gamma_k (first iteration or after a restart)
+  int first;            // first iteration: N y_0 is a Schur product
   int backtracks;
   unsigned err;
   int iterations;
   int sweeps;           // iterations executed
+  // device time between consecutive grid-barrier releases, by the phase that
+  // ended at the barrier (globaltimer ns): see kPhase* in dv_apgd.cu
+  unsigned long long last_release;
+  unsigned long long phase_ns[8];
+  unsigned long long phase_count[8];
 };
 
 struct SceneDev {
@@ -97,8 +106,13 @@ struct SceneDev {
   double* r = nullptr;        // 3 planes
   int* binc_start = nullptr;  // nb + 1
   uint32_t* binc = nullptr;   // contact ids sorted by B
-  // APGD work (3 planes each, stride ccap)
-  double *G0 = nullptr, *G1 = nullptr, *Y0 = nullptr, *Y1 = nullptr, *gv = nullptr, *ghat = nullptr;
+  // flat incidence per body in ascending contact order: B-side contacts with
+  // bit 31 set (sign -1), then A-side contacts; body b owns [inc_start[b], inc_start[b+1])
+  int* inc_start = nullptr;   // nb + 1
+  uint32_t* inc = nullptr;    // 2 * ccap
+  // APGD work: iterates and their Schur products, 3 planes each (stride ccap)
+  double* G[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  double* NG[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double4* q = nullptr;
   double* part = nullptr;     // reduction partials
   int part_tiles = 0;
@@ -109,12 +123,6 @@ struct SceneDev {
   ApgdCtl* ctl = nullptr;
   ApgdCtl* h_ctl = nullptr;   // pinned mirror
   unsigned* bar = nullptr;    // grid barrier words
-  // mixed precision buffers
-  float* Ff = nullptr;
-  float *G0f = nullptr, *G1f = nullptr, *Y0f = nullptr, *Y1f = nullptr, *gvf = nullptr, *ghatf = nullptr;
-  float* rf = nullptr;
-  float4* qf = nullptr;
-  float4* wf = nullptr;
 };
 
 // ---- sort / scan (dv_sort.cu) ----

@@ -11,9 +11,9 @@
 // buffers; the only scratch is the fixed-size array below, which exists once
 // per device for the lifetime of the process.
 //
-// Scratch: s_tile_scratch holds 4 partial results per reduction tile of 1024
+// Scratch: s_tile_scratch holds 4 partial results per reduction tile of 512
 // contacts, so one call handles at most DV_NOALLOC_MAX_CONTACTS contacts
-// (16,777,216, i.e. 16,384 tiles; 512 KiB of device memory per device).
+// (16,777,216, i.e. 32,768 tiles; 1 MiB of device memory per device).
 // Every slot a call reads is written earlier in the same call, so no state
 // carries over between calls and nothing needs clearing; but all calls share
 // the one array, so two calls whose kernels overlap on the GPU (different

@@ -50,6 +50,8 @@ struct dv_scene {
   bool solve_pending = false;
   bool step_open = false;
   std::vector<dv_step_stats> history;
+  double phase_ns[8] = {0};       // accumulated since the last dv_get_phase_times reset
+  long long phase_count[8] = {0};
   unsigned* h_bar = nullptr;
   double* h_red = nullptr;     // pinned results of diagnostic reductions
   double* d_red = nullptr;     // device partials for diagnostics
@@ -90,9 +92,16 @@ void dfree(dv_scene* s, T*& p) {
 
 int alloc_contacts(dv_scene* s, size_t cap) {
   SceneDev& d = s->d;
+  // planes start on 2 KiB boundaries: the solve kernel copies 256-contact
+  // plane segments with bulk asynchronous copies (16-byte alignment rule)
+  cap = (cap + 255) / 256 * 256;
   dfree(s, d.ida); dfree(s, d.idb); dfree(s, d.F); dfree(s, d.gap); dfree(s, d.loc);
-  dfree(s, d.r); dfree(s, d.G0); dfree(s, d.G1); dfree(s, d.Y0); dfree(s, d.Y1);
-  dfree(s, d.gv); dfree(s, d.ghat); dfree(s, d.q); dfree(s, d.binc); dfree(s, d.part);
+  dfree(s, d.r);
+  for (int k = 0; k < 5; ++k) {
+    dfree(s, d.G[k]);
+    dfree(s, d.NG[k]);
+  }
+  dfree(s, d.q); dfree(s, d.binc); dfree(s, d.inc); dfree(s, d.part);
   d.ccap = cap;
   TRY(dalloc(s, &d.ida, cap));
   TRY(dalloc(s, &d.idb, cap));
@@ -100,16 +109,15 @@ int alloc_contacts(dv_scene* s, size_t cap) {
   TRY(dalloc(s, &d.gap, cap));
   TRY(dalloc(s, &d.loc, 3 * cap));
   TRY(dalloc(s, &d.r, 3 * cap));
-  TRY(dalloc(s, &d.G0, 3 * cap));
-  TRY(dalloc(s, &d.G1, 3 * cap));
-  TRY(dalloc(s, &d.Y0, 3 * cap));
-  TRY(dalloc(s, &d.Y1, 3 * cap));
-  TRY(dalloc(s, &d.gv, 3 * cap));
-  TRY(dalloc(s, &d.ghat, 3 * cap));
+  for (int k = 0; k < 5; ++k) {
+    TRY(dalloc(s, &d.G[k], 3 * cap));
+    TRY(dalloc(s, &d.NG[k], 3 * cap));
+  }
   TRY(dalloc(s, &d.q, cap));
   TRY(dalloc(s, &d.binc, cap));
+  TRY(dalloc(s, &d.inc, 2 * cap));
   d.part_tiles = (int)((cap + kTileItems - 1) / kTileItems) + 1;
-  TRY(dalloc(s, &d.part, (size_t)(7) * d.part_tiles));
+  TRY(dalloc(s, &d.part, (size_t)(9) * d.part_tiles));
   size_t rc = std::max((size_t)d.nb, cap);
   if (rc > d.radix_cap) {
     dfree(s, d.keyA); dfree(s, d.valA); dfree(s, d.keyB); dfree(s, d.valB);
@@ -164,6 +172,10 @@ int absorb_solve(dv_scene* s) {
     s->last.residual = c.residual;
     s->last.objective = c.objective;
     s->last.sweeps = c.sweeps;
+    for (int i = 0; i < 8; ++i) {
+      s->phase_ns[i] += (double)c.phase_ns[i];
+      s->phase_count[i] += (long long)c.phase_count[i];
+    }
     int e = s->ev_cur;
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, s->ev_t0[e], s->ev_c[e]) == cudaSuccess) s->last.collide_ms = ms;
@@ -481,6 +493,7 @@ DV_API int dv_scene_create(const dv_body_desc* bodies, int32_t nb, const dv_para
       (rc = dalloc(s, &d.amax, nbz)) || (rc = dalloc(s, &d.cell, nbz)) ||
       (rc = dalloc(s, &d.cnt_cont, nbz)) || (rc = dalloc(s, &d.cnt_cand, nbz)) ||
       (rc = dalloc(s, &d.cbase, nbz + 1)) || (rc = dalloc(s, &d.binc_start, nbz + 1)) ||
+      (rc = dalloc(s, &d.inc_start, nbz + 1)) ||
       (rc = dalloc(s, &d.grid, 1)) || (rc = dalloc(s, &d.counters, 4)) ||
       (rc = dalloc(s, &d.ctl, 1)) || (rc = dalloc(s, &d.bar, 4)))
     return fail(rc);
@@ -814,6 +827,20 @@ DV_API int dv_get_step_history(dv_scene* s, dv_step_stats* out, int32_t cap, int
   if (n) *n = m;
   if (out)
     for (int i = 0; i < std::min(cap, m); ++i) out[i] = s->history[i];
+  return rc;
+}
+
+DV_API int dv_get_phase_times(dv_scene* s, double* ns, int64_t* counts, int32_t reset) {
+  if (!s) return DV_ERR_ARG;
+  int rc = finish(s);
+  for (int i = 0; i < 8; ++i) {
+    if (ns) ns[i] = s->phase_ns[i];
+    if (counts) counts[i] = s->phase_count[i];
+    if (reset) {
+      s->phase_ns[i] = 0;
+      s->phase_count[i] = 0;
+    }
+  }
   return rc;
 }
 

@@ -149,6 +149,12 @@ DV_API int64_t dv_scene_launch_count(dv_scene* s);
  * reference prints at System.cu:592 and APGD.cu:351). */
 DV_API int dv_get_step_history(dv_scene* s, dv_step_stats* out, int32_t cap, int32_t* n);
 DV_API int dv_clear_step_history(dv_scene* s);
+/* Device time of the solve kernel's phases summed over the steps so far (ns
+ * between grid-barrier releases, 8 slots: setup, step, backtrack step, body
+ * gather, product + residual, final) and how often each ran; reset != 0
+ * clears the sums.  The reference's elapsedTime (System.cu:586-590) times the
+ * whole step only. */
+DV_API int dv_get_phase_times(dv_scene* s, double* ns, int64_t* counts, int32_t reset);
 
 /* No counterpart in the reference.  dv_ccp_violation without any device
  * allocation, for callers that may not call cudaMalloc/cudaFree: an
@@ -159,7 +165,7 @@ DV_API int dv_clear_step_history(dv_scene* s);
  * (normalsAndPenetrations_d: normal B->A, gap), ida/idb per contact, v 3 per
  * body (System::v_d); out4 receives (min gamma_n, min v_n, gamma_n . v_n,
  * ||cone violation||) in device memory, queued on `stream` (a cudaStream_t,
- * NULL = legacy default stream).  Scratch is a fixed 512 KiB array in device
+ * NULL = legacy default stream).  Scratch is a fixed 1 MiB array in device
  * memory that each GPU holds until the process exits; nc above
  * DV_NOALLOC_MAX_CONTACTS is rejected with DV_ERR_ARG.  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress); make it

@@ -77,8 +77,8 @@ inline V3 cross3(V3 a, V3 b) {
 
 /* ---------------------------------------------------------------------
  * Ordered reduction shared with the GPU.
- * Items are grouped in tiles of 1024.  In tile t, slot j (0..255) sums
- * items 1024t + j + 256m for m = 0..3, starting from 0.0; the 256 slots are
+ * Items are grouped in tiles of 512.  In tile t, slot j (0..255) sums
+ * items 512t + j + 256m for m = 0..1, starting from 0.0; the 256 slots are
  * folded as 8 warps of 32 by halving strides 16,8,4,2,1 (slot l += slot
  * l+off), then the 8 warp results by strides 4,2,1.  The tile partials are
  * folded the same way: slot j sums tiles j, j+256, ... then the 256-tree.
@@ -98,15 +98,15 @@ double tree256(double* s) {
 
 double ordered_sum(const double* v, int64_t n) {
   if (n <= 0) return 0.0;
-  int64_t T = (n + 1023) / 1024;
+  int64_t T = (n + 511) / 512;
   std::vector<double> P(T);
 #pragma omp parallel for schedule(static)
   for (int64_t t = 0; t < T; ++t) {
     double s[256];
     for (int j = 0; j < 256; ++j) {
       double acc = 0.0;
-      for (int m = 0; m < 4; ++m) {
-        int64_t i = 1024 * t + j + 256 * m;
+      for (int m = 0; m < 2; ++m) {
+        int64_t i = 512 * t + j + 256 * m;
         if (i < n) acc = acc + v[i];
       }
       s[j] = acc;
@@ -549,7 +549,132 @@ double get_residual(const Scene& S, const double* src, std::vector<double>& T,
   return nrmmaxv(T.data(), nc, nan_flag);
 }
 
-/* APGD.cu:164-361 */
+/* APGD.cu:90-102 with N src already available. */
+double residual_from(const Scene& S, const double* src, const double* Nsrc, std::vector<double>& T,
+                     int* nan_flag) {
+  int nc = S.nc;
+  double gdiff = 1.0 / ((double)nc * (double)nc);
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = S.r[i] + Nsrc[i];
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = src[i] + (-gdiff) * T[i];
+  for (int c = 0; c < nc; ++c) project3(&T[3 * c], S.P.mu);
+  double a = 1.0 / gdiff, b = -1.0 / gdiff;
+  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = a * src[i] + b * T[i];
+  return nrmmaxv(T.data(), nc, nan_flag);
+}
+
+void resize_gamma(Scene& S) {
+  int nc = S.nc;
+  int64_t n3 = 3 * (int64_t)nc;
+  /* thrust resize keeps the prefix and zero-fills growth (APGD.cu:166). */
+  if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
+  if (S.gsize < nc)
+    for (int64_t i = 3 * (int64_t)S.gsize; i < n3; ++i) S.gamma[i] = 0.0;
+  S.gsize = nc;
+  if (!S.P.warm_start)
+    for (int c = 0; c < nc; ++c) {
+      S.gamma[3 * c] = 1.0;
+      S.gamma[3 * c + 1] = 0.0;
+      S.gamma[3 * c + 2] = 0.0;
+    }
+}
+
+/* APGD.cu:164-361 in the order the GPU evaluates it.  The reference computes
+ * N y with a Schur product (APGD.cu:229, 239); y_k = (1+b) g_k - b g_{k-1}
+ * (APGD.cu:273, or g_k after a restart, :315), so here N y_k is formed from the
+ * stored products of the two iterates, (1+b) N g_k - b N g_{k-1}: one Schur
+ * product per iteration (N gamma_new, reused by the objective and the
+ * residual) plus one per backtrack.  The first iteration's N y_0 is a product. */
+void apgd_solve_fused(Scene& S) {
+  int nc = S.nc;
+  int64_t n3 = 3 * (int64_t)nc;
+  resize_gamma(S);
+  double* gamma = S.gamma.data();
+  std::vector<double> Gc(gamma, gamma + n3), Gp(n3, 0.0), NGc(n3), NGp(n3, 0.0);
+  std::vector<double> gNew(n3), NgNew(n3), g(n3), y(n3), Ny(n3), T(n3), best(n3, 1.0), bt;
+  double theta = 1.0, thetaNew = theta, Beta = 0.0, obj1 = 0.0, obj2 = 0.0;
+  double residual = 10e30;
+  int nan_flag = 0, status = 0, backtracks = 0;
+  bool have_best = false;
+  double L, t;
+  for (int64_t i = 0; i < n3; ++i) T[i] = Gc[i] + (-1.0);
+  L = nrm2v(S, T.data(), nc);
+  schur(S, T.data(), T.data(), bt);
+  L = nrm2v(S, T.data(), nc) / L;
+  t = 1.0 / L;
+  const double mu = S.P.mu;
+  bool y_restart = true;  // y_0 = gamma_0
+  double yb = 0.0;
+  int k;
+  for (k = 0; k < S.P.max_iterations; ++k) {
+    if (k == 0) {
+      for (int64_t i = 0; i < n3; ++i) y[i] = Gc[i];
+      schur(S, y.data(), NGc.data(), bt);
+      for (int64_t i = 0; i < n3; ++i) Ny[i] = NGc[i];
+    } else if (y_restart) {
+      for (int64_t i = 0; i < n3; ++i) { y[i] = Gc[i]; Ny[i] = NGc[i]; }
+    } else {
+      double a = 1.0 + yb, b = -yb;
+      for (int64_t i = 0; i < n3; ++i) {
+        y[i] = a * Gc[i] + b * Gp[i];
+        Ny[i] = a * NGc[i] + b * NGp[i];
+      }
+    }
+    for (int64_t i = 0; i < n3; ++i) g[i] = Ny[i] + S.r[i];
+    double obj2_base = 0.5 * dotv(S, y.data(), Ny.data(), nc) + dotv(S, y.data(), S.r.data(), nc);
+    bool first = true;
+    for (;;) {
+      if (!first) {
+        if (backtracks >= S.P.max_backtracks) { status = 3; break; }
+        ++backtracks;
+        L = 2.0 * L;
+        t = 1.0 / L;
+      }
+      first = false;
+      for (int64_t i = 0; i < n3; ++i) gNew[i] = y[i] + (-t) * g[i];
+      for (int c = 0; c < nc; ++c) project3(&gNew[3 * c], mu);
+      schur(S, gNew.data(), NgNew.data(), bt);
+      obj1 = 0.5 * dotv(S, gNew.data(), NgNew.data(), nc) + dotv(S, gNew.data(), S.r.data(), nc);
+      for (int64_t i = 0; i < n3; ++i) T[i] = gNew[i] + (-1.0) * y[i];
+      double nr = nrm2v(S, T.data(), nc);
+      obj2 = obj2_base + (dotv(S, g.data(), T.data(), nc) + 0.5 * L * (nr * nr));
+      if (!(obj1 >= obj2)) break;
+    }
+    if (status) break;
+    thetaNew = (-(theta * theta) + theta * sqrt(theta * theta + 4.0)) / 2.0;
+    Beta = theta * (1.0 - theta) / (theta * theta + thetaNew);
+    double res = residual_from(S, gNew.data(), NgNew.data(), T, &nan_flag);
+    if (res < residual) {
+      residual = res;
+      best = gNew;
+      have_best = true;
+    }
+    if (residual < S.P.tolerance) break;
+    for (int64_t i = 0; i < n3; ++i) T[i] = gNew[i] + (-1.0) * Gc[i];
+    bool restart = dotv(S, g.data(), T.data(), nc) > 0;
+    if (restart) thetaNew = 1.0;
+    L = 0.9 * L;
+    t = 1.0 / L;
+    theta = thetaNew;
+    Gp.swap(Gc);
+    NGp.swap(NGc);
+    Gc = gNew;
+    NGc = NgNew;
+    y_restart = restart;
+    yb = Beta;
+  }
+  (void)have_best;
+  schur(S, best.data(), T.data(), bt);
+  double objective = 0.5 * dotv(S, best.data(), T.data(), nc) + dotv(S, best.data(), S.r.data(), nc);
+  for (int64_t i = 0; i < n3; ++i) gamma[i] = best[i];
+  S.st.iterations = k;
+  S.st.backtracks = backtracks;
+  S.st.residual = residual;
+  S.st.objective = objective;
+  if (nan_flag) status = status ? status : 2;
+  S.st.status = status;
+}
+
+/* APGD.cu:164-361, literally: four Schur products per iteration. */
 void apgd_solve(Scene& S) {
   int nc = S.nc;
   int64_t n3 = 3 * (int64_t)nc;
@@ -671,7 +796,8 @@ int do_step(Scene& S) {
   if (S.nc) {
     build_frames(S);
     build_r(S);
-    apgd_solve(S);
+    if (S.P.apgd_mode == 1) apgd_solve(S);
+    else apgd_solve_fused(S);
     std::vector<double> fc(n);
     apply_DT(S, S.gamma.data(), fc.data());
     for (int i = 0; i < n; ++i) {

@@ -35,6 +35,7 @@ typedef struct or_params {
   int spmv_mode;          /* 0 = grouped matrix-free product, 1 = literal COO entry order */
   int max_backtracks;     /* cap on Lipschitz doublings per iteration (unbounded in the reference) */
   int threads;            /* OpenMP threads, 0 = runtime default */
+  int apgd_mode;          /* 0 = fused sequence shared with the GPU, 1 = literal reference sequence */
 } or_params;
 
 typedef struct or_stats {

@@ -36,7 +36,7 @@ class OrParams(C.Structure):
                 ("envelope", C.c_double), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int), ("warm_start", C.c_int),
                 ("reduce_mode", C.c_int), ("spmv_mode", C.c_int),
-                ("max_backtracks", C.c_int), ("threads", C.c_int)]
+                ("max_backtracks", C.c_int), ("threads", C.c_int), ("apgd_mode", C.c_int)]
 
 
 class OrStats(C.Structure):
@@ -102,7 +102,7 @@ def _up(a):
     return a.ctypes.data_as(C.POINTER(C.c_uint32))
 
 
-def make_params(p: dict, reduce_mode=0, spmv_mode=0, threads=0) -> OrParams:
+def make_params(p: dict, reduce_mode=0, spmv_mode=0, threads=0, apgd_mode=0) -> OrParams:
     o = OrParams()
     o.h = p["h"]
     o.mu = p["mu"]
@@ -115,13 +115,14 @@ def make_params(p: dict, reduce_mode=0, spmv_mode=0, threads=0) -> OrParams:
     o.spmv_mode = spmv_mode
     o.max_backtracks = int(p.get("max_backtracks", 4096))
     o.threads = threads
+    o.apgd_mode = apgd_mode
     return o
 
 
 class OracleScene:
     """One scene held by the CPU oracle; mirrors the state a System keeps."""
 
-    def __init__(self, scene, reduce_mode=0, spmv_mode=0, threads=0):
+    def __init__(self, scene, reduce_mode=0, spmv_mode=0, threads=0, apgd_mode=0):
         L = lib()
         self.nb = scene.nb
         self._arrs = [np.ascontiguousarray(scene.pos, dtype=np.float64),
@@ -131,7 +132,7 @@ class OracleScene:
                       np.ascontiguousarray(scene.fixed, dtype=np.int32),
                       np.ascontiguousarray(scene.family, dtype=np.int32)]
         a = self._arrs
-        self.params = make_params(scene.params, reduce_mode, spmv_mode, threads)
+        self.params = make_params(scene.params, reduce_mode, spmv_mode, threads, apgd_mode)
         self.h = L.or_create(self.nb, _dp(a[0]), _dp(a[1]), _dp(a[2]), _dp(a[3]), _ip(a[4]),
                              _ip(a[5]), C.byref(self.params))
 

@@ -94,14 +94,14 @@ def _ordered_sum_py(v):
     n = len(v)
     if n == 0:
         return 0.0
-    T = (n + 1023) // 1024
+    T = (n + 511) // 512
     P = []
     for t in range(T):
         s = []
         for j in range(256):
             acc = 0.0
-            for m in range(4):
-                i = 1024 * t + j + 256 * m
+            for m in range(2):
+                i = 512 * t + j + 256 * m
                 if i < n:
                     acc = acc + float(v[i])
             s.append(acc)
@@ -213,16 +213,23 @@ def test_schur_matches_dense(oracle_mod):
         assert np.allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
 
 
-def test_summation_order_within_parity_bar(oracle_mod):
-    """The GPU's fixed reduction order (mode 0) and CUSP's sequential host order
-    with literal COO SpMV (mode 1) give per-step gamma and v within 1e-10
-    relative (teacher-forced from the same state each step)."""
-    sc = scenes.settling_box(n_side=4, max_iterations=300)
-    o0 = oracle_mod.OracleScene(sc, reduce_mode=0, spmv_mode=0)
-    o1 = oracle_mod.OracleScene(sc, reduce_mode=1, spmv_mode=1)
+def test_evaluation_order_within_parity_bar(oracle_mod):
+    """The evaluation order shared with the GPU (mode 0: tiled reductions,
+    grouped matrix-free product, N y formed from the stored products of the
+    last two iterates) and the reference's literal sequence (mode 1: CUSP's
+    sequential host sums, COO entry order, four Schur products per iteration)
+    take the same APGD decisions and give gamma within 1e-10 relative per step
+    (teacher-forced from the same state).  Velocities of a pile at rest are
+    near zero, so their difference is measured against the velocity change of
+    one step under gravity (h g per dynamic body), the scale of the update."""
+    sc = scenes.settling_box(n_side=5, max_iterations=500)
+    o0 = oracle_mod.OracleScene(sc, reduce_mode=0, spmv_mode=0, apgd_mode=0)
+    o1 = oracle_mod.OracleScene(sc, reduce_mode=1, spmv_mode=1, apgd_mode=1)
+    ndyn = int((sc.fixed == 0).sum())
+    vscale = sc.params["h"] * 9.81 * np.sqrt(ndyn)
     worst_g = worst_v = 0.0
     active = 0
-    for step in range(120):
+    for step in range(160):
         p, v = o0.state()
         o1.set_state(p, v)
         o1.set_gamma(o0.gamma())
@@ -235,10 +242,10 @@ def test_summation_order_within_parity_bar(oracle_mod):
         _, v1 = o1.state()
         if s0["num_contacts"] and np.abs(g0).max() > 0:
             active += 1
-            if s0["iterations"] == s1["iterations"]:
-                worst_g = max(worst_g, np.linalg.norm(g0 - g1) / np.linalg.norm(g0))
-        worst_v = max(worst_v, np.linalg.norm(v0 - v1) / max(np.linalg.norm(v0), 1e-300))
-    assert active > 10
+            assert s0["iterations"] == s1["iterations"] and s0["backtracks"] == s1["backtracks"]
+            worst_g = max(worst_g, np.linalg.norm(g0 - g1) / np.linalg.norm(g0))
+        worst_v = max(worst_v, np.linalg.norm(v0 - v1) / max(np.linalg.norm(v0), vscale))
+    assert active > 100
     assert worst_g <= 1e-10
     assert worst_v <= 1e-10
 
