@@ -185,6 +185,150 @@ def cpu_baseline_sample(sc, budget_s):
                       f"buffer, {dt:.1f} s"}
 
 
+def run_batched(args, N, torch, stream):
+    """512 independent settling scenes (sphere counts log-uniform in [100, 20000],
+    r ~ U[0.004, 0.006], mu ~ U[0.1, 0.5], own containers; h 1e-3, tol 1e-4,
+    maxIter 500, warm start) stepped as one batch: mixed precision, CUDA-graph
+    replay, autotuned launch shape.  Beside it, the plain FP64 path stepping a
+    size-stratified sample of the same scenes one at a time."""
+    from dvide_b200 import scenes
+    scs = scenes.batch_scenes(seed=3, count=args.batch_scenes)
+    total_steps = args.batch_steps
+    timed = max(1, min(args.batch_timed, total_steps - 1))
+    pre = total_steps - timed
+    b = N.NativeBatch(scs, precision=N.DV_PREC_MIXED)
+    b.set_stream(stream.cuda_stream)
+    graph = b.set_graph(True) == 0
+    b.step(pre)
+    tune = b.autotune(steps_per_trial=2)
+    torch.cuda.synchronize()
+    l0 = b.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(timed)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    hist, step_ms = b.history()
+    contacts = sum(s["num_contacts"] for st in hist for s in st)
+    iters = [s["iterations"] for st in hist for s in st if s["num_contacts"] > 0]
+    res = [s["residual"] for st in hist for s in st if s["num_contacts"] > 0]
+    conv = sum(1 for r in res if r < 1e-4)
+    launches = b.launches() - l0
+    nb = b.nb
+    b.close()
+    # plain FP64 path, one scene at a time, on a size-stratified sample
+    order = np.argsort([sc.nb for sc in scs])
+    sample = [scs[i] for i in order[::max(1, len(scs) // args.plain_sample)]]
+    p_contacts = 0
+    p_ms = 0.0
+    for sc in sample:
+        g = N.NativeScene.from_scene(sc)
+        g.set_stream(stream.cuda_stream)
+        g.step(pre)
+        g.history(clear=True)
+        g.step(timed)
+        h = g.history(clear=True)
+        p_contacts += sum(x["num_contacts"] for x in h)
+        p_ms += sum(x["elapsed_ms"] for x in h)
+        g.close()
+    batched = contacts / (ms / 1e3)
+    plain = p_contacts / (p_ms / 1e3) if p_ms > 0 else None
+    return {
+        "workload": (f"{len(scs)} settling scenes, {nb} bodies, steps {pre + 1}-{total_steps} of "
+                     f"{total_steps} timed (h 1e-3), mixed precision, per-scene convergence"),
+        "value": batched, "unit": "contact-steps/s", "ms_per_step": ms / timed,
+        "contacts_per_step": contacts / timed,
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                       "p99": float(np.percentile(step_ms, 99))},
+        "scene_iterations_mean": float(np.mean(iters)) if iters else 0.0,
+        "scene_solves_converged": f"{conv}/{len(res)}",
+        "graph": graph, "autotune": {"best": tune["candidates"][tune["best"]],
+                                      "identical": tune["identical"]},
+        "gpu_launches": int(launches),
+        "plain_fp64_one_at_a_time": {
+            "value": plain, "unit": "contact-steps/s",
+            "sample": f"{len(sample)} of {len(scs)} scenes (every {len(scs) // len(sample)}th by "
+                      f"size), same steps, device time"},
+        "speedup_vs_plain": (batched / plain) if plain else None,
+    }
+
+
+def run_served(args, N, stream):
+    """Poisson arrivals of settling scenes (sphere counts log-uniform in
+    [500, 50000], r ~ U[0.004, 0.006], mu ~ U[0.1, 0.5], own containers),
+    each asking for `serve_steps` steps at h 1e-3 with residual 1e-4, served by
+    continuous batching in mixed precision under a 150 GB admission budget.
+    Arrivals run in real time.  Beside it, the plain FP64 path serving a
+    size-stratified sample of the same requests one at a time."""
+    from dvide_b200 import scenes
+    rng = np.random.default_rng(11)
+    n_req = max(1, int(args.serve_rate * args.serve_seconds))
+    gaps = rng.exponential(1.0 / args.serve_rate, size=n_req)
+    arrive = np.cumsum(gaps) - gaps[0]
+    sizes = np.exp(rng.uniform(np.log(500), np.log(50000), size=n_req)).astype(np.int64)
+    reqs = [scenes.lattice_container(rng, int(n), name=f"req{i}") for i, n in enumerate(sizes)]
+    srv = N.NativeServer(precision=N.DV_PREC_MIXED, hbm_budget_bytes=150e9,
+                         steps_per_round=args.serve_round, keep_states=False)
+    srv.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    i = 0
+    results = []
+    busy = False
+    while i < n_req or busy:
+        now = time.perf_counter() - t0
+        while i < n_req and arrive[i] <= now:
+            srv.submit(reqs[i], args.serve_steps)
+            i += 1
+        if not busy and i < n_req and arrive[i] > now:
+            time.sleep(min(arrive[i] - now, 0.01))
+            busy = srv.stats()["active"] > 0 or srv.stats()["pending"] > 0
+            continue
+        busy = srv.round()
+        results += srv.poll()
+    wall = time.perf_counter() - t0
+    results += srv.poll()
+    st = srv.stats()
+    srv.close()
+    lat = np.array([r["t_done"] - r["t_submit"] for r in results])
+    step_p50 = np.array([r["step_ms_p50"] for r in results])
+    step_p99 = np.array([r["step_ms_p99"] for r in results])
+    contact_steps = st["contact_steps"]
+    # plain FP64 one request at a time on a stratified sample
+    order = np.argsort(sizes)
+    pick = order[::max(1, n_req // args.plain_sample)]
+    p_cs, p_ms = 0.0, 0.0
+    for j in pick:
+        g = N.NativeScene.from_scene(reqs[j])
+        g.set_stream(stream.cuda_stream)
+        g.step(args.serve_steps)
+        h = g.history(clear=True)
+        p_cs += sum(x["num_contacts"] for x in h)
+        p_ms += sum(x["elapsed_ms"] for x in h)
+        g.close()
+    plain = p_cs / (p_ms / 1e3) if p_ms > 0 else None
+    served = contact_steps / wall
+    return {
+        "workload": (f"{n_req} requests, Poisson {args.serve_rate}/s for {args.serve_seconds} s, "
+                     f"{args.serve_steps} steps each (h 1e-3), spheres log-uniform [500, 50000], "
+                     f"mixed precision, 150 GB budget"),
+        "value": served, "unit": "contact-steps/s (wall clock, arrivals included)",
+        "device_contact_steps_per_s": contact_steps / (st["device_ms"] / 1e3),
+        "wall_s": wall, "completed": int(st["completed"]), "rounds": int(st["rounds"]),
+        "layout_changes": int(st["reconfigures"]),
+        "time_per_step_ms": {"p50": float(np.percentile(step_p50, 50)),
+                             "p99": float(np.percentile(step_p99, 99))},
+        "completion_latency_s": {"p50": float(np.percentile(lat, 50)),
+                                 "p99": float(np.percentile(lat, 99))},
+        "plain_fp64_one_at_a_time": {
+            "value": plain, "unit": "contact-steps/s (device time)",
+            "sample": f"{len(pick)} of {n_req} requests (every {max(1, n_req // args.plain_sample)}th "
+                      f"by size)"},
+        "speedup_vs_plain": (served / plain) if plain else None,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +341,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iterations", type=int, default=None,
                     help="override the APGD iteration cap (profiling runs only)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes line")
+    ap.add_argument("--batch-scenes", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-timed", type=int, default=40)
+    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--no-served", action="store_true", help="skip the served line")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-steps", type=int, default=200)
+    ap.add_argument("--serve-round", type=int, default=4)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -328,6 +482,10 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(sc, args.cpu_budget_s)
+        if world == 1 and not args.no_batched:
+            line["batched"] = run_batched(args, N, torch, stream)
+        if world == 1 and not args.no_served:
+            line["served"] = run_served(args, N, stream)
         print(json.dumps(line), flush=True)
     g.close()
     if dist is not None:

@@ -28,6 +28,14 @@ EXPORTS = [
     "dv_contact_forces_per_collision", "dv_get_step_stats", "dv_status_string", "dv_last_error",
     "dv_scene_launch_count", "dv_get_step_history", "dv_clear_step_history",
     "dv_get_phase_times", "dv_ccp_violation_noalloc",
+    "dv_batch_create", "dv_batch_destroy", "dv_batch_set_stream", "dv_batch_step",
+    "dv_batch_num_scenes", "dv_batch_get_state", "dv_batch_set_state", "dv_batch_scene_stats",
+    "dv_batch_step_history", "dv_batch_get_gamma", "dv_batch_ccp_violation",
+    "dv_batch_set_launch", "dv_batch_get_launch", "dv_batch_set_graph", "dv_batch_autotune",
+    "dv_batch_launch_count",
+    "dv_server_default_config", "dv_server_create", "dv_server_destroy", "dv_server_set_stream",
+    "dv_server_clock", "dv_server_submit", "dv_server_round", "dv_server_poll",
+    "dv_server_result_state", "dv_server_get_stats",
 ]
 
 
@@ -69,6 +77,64 @@ class StepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SceneStats(C.Structure):
+    _fields_ = [("num_contacts", C.c_int32), ("num_possible", C.c_int32),
+                ("iterations", C.c_int32), ("backtracks", C.c_int32), ("residual", C.c_double),
+                ("objective", C.c_double), ("status", C.c_int32), ("sweeps", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneCandidate(C.Structure):
+    _fields_ = [("grid", C.c_int32), ("chunk", C.c_int32), ("contiguous", C.c_int32),
+                ("ms_per_step", C.c_float)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("num_candidates", C.c_int32), ("best", C.c_int32), ("identical", C.c_int32),
+                ("steps_per_trial", C.c_int32), ("cand", TuneCandidate * 16)]
+
+    def as_dict(self):
+        return {"best": self.best, "identical": bool(self.identical),
+                "steps_per_trial": self.steps_per_trial,
+                "candidates": [{"grid": c.grid, "chunk": c.chunk, "contiguous": c.contiguous,
+                                "ms_per_step": c.ms_per_step}
+                               for c in self.cand[:self.num_candidates]]}
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_double), ("max_active", C.c_int32),
+                ("steps_per_round", C.c_int32), ("precision", C.c_int32), ("use_graph", C.c_int32),
+                ("keep_states", C.c_int32), ("pad_", C.c_int32)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("id", C.c_int64), ("nb", C.c_int32), ("nsteps", C.c_int32),
+                ("status", C.c_int32), ("rounds", C.c_int32), ("t_submit", C.c_double),
+                ("t_admit", C.c_double), ("t_done", C.c_double), ("contact_steps", C.c_double),
+                ("step_ms_mean", C.c_double), ("step_ms_p50", C.c_double),
+                ("step_ms_p99", C.c_double), ("bytes", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("pending", C.c_int64), ("active", C.c_int64), ("rounds", C.c_int64),
+                ("reconfigures", C.c_int64), ("steps", C.c_int64), ("bytes_in_use", C.c_double),
+                ("contact_steps", C.c_double), ("device_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# numpy layout of dv_body_desc (88 bytes, no padding)
+BODY_DTYPE = np.dtype([("pos", "<f8", 3), ("vel", "<f8", 3), ("mass", "<f8"), ("geom", "<f8", 3),
+                       ("fixed", "<i4"), ("family", "<i4")])
+assert BODY_DTYPE.itemsize == C.sizeof(BodyDesc)
+
 _lib = None
 
 
@@ -105,6 +171,32 @@ def lib():
         "dv_get_step_history": [vp, C.POINTER(StepStats), C.c_int32, ip],
         "dv_clear_step_history": [vp],
         "dv_get_phase_times": [vp, dp, C.POINTER(C.c_int64), C.c_int32],
+        "dv_batch_create": [C.POINTER(BodyDesc), ip, C.c_int32, C.POINTER(Params), C.c_int32,
+                            C.POINTER(vp)],
+        "dv_batch_destroy": [vp],
+        "dv_batch_set_stream": [vp, vp],
+        "dv_batch_step": [vp, C.c_int32],
+        "dv_batch_num_scenes": [vp, ip, ip],
+        "dv_batch_get_state": [vp, C.c_int32, dp, dp],
+        "dv_batch_set_state": [vp, C.c_int32, dp, dp],
+        "dv_batch_scene_stats": [vp, C.POINTER(SceneStats)],
+        "dv_batch_step_history": [vp, C.POINTER(SceneStats), C.POINTER(C.c_float), C.c_int32, ip],
+        "dv_batch_get_gamma": [vp, C.c_int32, dp, C.c_int32, ip],
+        "dv_batch_ccp_violation": [vp, C.c_int32, dp],
+        "dv_batch_set_launch": [vp, C.c_int32, C.c_int32, C.c_int32],
+        "dv_batch_get_launch": [vp, ip, ip, ip, ip],
+        "dv_batch_set_graph": [vp, C.c_int32],
+        "dv_batch_autotune": [vp, C.c_int32, C.POINTER(TuneReport)],
+        "dv_server_default_config": [C.POINTER(ServerConfig)],
+        "dv_server_create": [C.POINTER(ServerConfig), C.POINTER(vp)],
+        "dv_server_destroy": [vp],
+        "dv_server_set_stream": [vp, vp],
+        "dv_server_submit": [vp, C.POINTER(BodyDesc), C.c_int32, C.POINTER(Params), C.c_int32,
+                             C.POINTER(C.c_int64)],
+        "dv_server_round": [vp, ip],
+        "dv_server_poll": [vp, C.POINTER(RequestResult), C.c_int32, ip],
+        "dv_server_result_state": [vp, C.c_int64, dp, dp],
+        "dv_server_get_stats": [vp, C.POINTER(ServerStats)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -119,6 +211,10 @@ def lib():
     L.dv_ccp_violation_noalloc.restype = C.c_int
     L.dv_scene_launch_count.argtypes = [vp]
     L.dv_scene_launch_count.restype = C.c_int64
+    L.dv_batch_launch_count.argtypes = [vp]
+    L.dv_batch_launch_count.restype = C.c_int64
+    L.dv_server_clock.argtypes = [vp]
+    L.dv_server_clock.restype = C.c_double
     _lib = L
     return L
 
@@ -153,21 +249,24 @@ def make_params(p: dict, precision=DV_PREC_FP64) -> Params:
     return o
 
 
+def body_records(pos, vel, mass, geom, fixed, family):
+    """dv_body_desc records as a numpy structured array."""
+    pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    nb = pos.shape[0]
+    rec = np.zeros(max(nb, 1), dtype=BODY_DTYPE)
+    if nb:
+        rec["pos"][:nb] = pos
+        rec["vel"][:nb] = np.asarray(vel, dtype=np.float64).reshape(-1, 3)
+        rec["mass"][:nb] = np.asarray(mass, dtype=np.float64)
+        rec["geom"][:nb] = np.asarray(geom, dtype=np.float64).reshape(-1, 3)
+        rec["fixed"][:nb] = np.asarray(fixed, dtype=np.int32)
+        rec["family"][:nb] = np.asarray(family, dtype=np.int32)
+    return rec, nb
+
+
 def body_array(pos, vel, mass, geom, fixed, family):
-    nb = int(np.asarray(pos).shape[0])
-    arr = (BodyDesc * max(nb, 1))()
-    pos = np.asarray(pos, dtype=np.float64)
-    vel = np.asarray(vel, dtype=np.float64)
-    geom = np.asarray(geom, dtype=np.float64)
-    for i in range(nb):
-        b = arr[i]
-        b.pos[:] = pos[i].tolist()
-        b.vel[:] = vel[i].tolist()
-        b.mass = float(mass[i])
-        b.geom[:] = geom[i].tolist()
-        b.fixed = int(fixed[i])
-        b.family = int(family[i])
-    return arr, nb
+    rec, nb = body_records(pos, vel, mass, geom, fixed, family)
+    return rec.ctypes.data_as(C.POINTER(BodyDesc)), nb, rec
 
 
 class NativeScene:
@@ -176,7 +275,7 @@ class NativeScene:
     def __init__(self, pos, vel, mass, geom, fixed, family, params: dict,
                  precision=DV_PREC_FP64):
         L = lib()
-        arr, nb = body_array(pos, vel, mass, geom, fixed, family)
+        arr, nb, self._rec = body_array(pos, vel, mass, geom, fixed, family)
         self.nb = nb
         self.params = make_params(params, precision)
         h = C.c_void_p()
@@ -330,3 +429,189 @@ class NativeScene:
 
     def launches(self):
         return int(lib().dv_scene_launch_count(self.h))
+
+
+class NativeBatch:
+    """Many scenes stepped together (dv_batch*): one collision pipeline and one
+    persistent solve kernel per step for all of them."""
+
+    def __init__(self, scenes_list, precision=DV_PREC_FP64, **overrides):
+        L = lib()
+        recs = []
+        counts = []
+        params = (Params * len(scenes_list))()
+        for i, sc in enumerate(scenes_list):
+            rec, nb = body_records(sc.pos, sc.vel, sc.mass, sc.geom, sc.fixed, sc.family)
+            recs.append(rec[:nb])
+            counts.append(nb)
+            p = dict(sc.params)
+            p.update(overrides)
+            params[i] = make_params(p, precision)
+        self._rec = np.concatenate(recs)
+        self.counts = np.asarray(counts, dtype=np.int32)
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.nscenes = len(scenes_list)
+        self.nb = int(self.offsets[-1])
+        h = C.c_void_p()
+        check(L.dv_batch_create(self._rec.ctypes.data_as(C.POINTER(BodyDesc)),
+                                self.counts.ctypes.data_as(C.POINTER(C.c_int32)), self.nscenes,
+                                params, int(precision), C.byref(h)), "dv_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dv_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        check(lib().dv_batch_step(self.h, int(n)), "dv_batch_step")
+
+    def set_stream(self, stream_ptr):
+        check(lib().dv_batch_set_stream(self.h, C.c_void_p(stream_ptr)), "dv_batch_set_stream")
+
+    def state(self, scene=-1):
+        n = self.nb if scene < 0 else int(self.counts[scene])
+        p = np.zeros((n, 3))
+        v = np.zeros((n, 3))
+        check(lib().dv_batch_get_state(self.h, int(scene), dptr(p), dptr(v)), "dv_batch_get_state")
+        return p, v
+
+    def state_into(self, p, v):
+        check(lib().dv_batch_get_state(self.h, -1, dptr(p), dptr(v)), "dv_batch_get_state")
+
+    def set_state(self, scene, p=None, v=None):
+        pp = np.ascontiguousarray(p, dtype=np.float64) if p is not None else None
+        vv = np.ascontiguousarray(v, dtype=np.float64) if v is not None else None
+        check(lib().dv_batch_set_state(self.h, int(scene), dptr(pp) if pp is not None else None,
+                                       dptr(vv) if vv is not None else None), "dv_batch_set_state")
+
+    def scene_stats(self):
+        arr = (SceneStats * self.nscenes)()
+        check(lib().dv_batch_scene_stats(self.h, arr), "dv_batch_scene_stats")
+        return [arr[i].as_dict() for i in range(self.nscenes)]
+
+    def history(self):
+        n = C.c_int32()
+        check(lib().dv_batch_step_history(self.h, None, None, 0, C.byref(n)))
+        steps = n.value
+        arr = (SceneStats * max(steps * self.nscenes, 1))()
+        ms = (C.c_float * max(steps, 1))()
+        check(lib().dv_batch_step_history(self.h, arr, ms, steps, C.byref(n)))
+        out = [[arr[i * self.nscenes + s].as_dict() for s in range(self.nscenes)]
+               for i in range(steps)]
+        return out, [float(ms[i]) for i in range(steps)]
+
+    def gamma(self, scene):
+        n = C.c_int32()
+        check(lib().dv_batch_get_gamma(self.h, int(scene), None, 0, C.byref(n)))
+        g = np.zeros((max(n.value, 0), 3))
+        if n.value:
+            check(lib().dv_batch_get_gamma(self.h, int(scene), dptr(g), n.value, C.byref(n)))
+        return g
+
+    def ccp_violation(self, scene):
+        o = np.zeros(4)
+        check(lib().dv_batch_ccp_violation(self.h, int(scene), dptr(o)))
+        return o
+
+    def set_launch(self, grid=0, chunk=1, contiguous=0):
+        check(lib().dv_batch_set_launch(self.h, int(grid), int(chunk), int(contiguous)))
+
+    def launch(self):
+        g, c, k, m = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().dv_batch_get_launch(self.h, C.byref(g), C.byref(c), C.byref(k), C.byref(m)))
+        return {"grid": g.value, "chunk": c.value, "contiguous": k.value, "max_grid": m.value}
+
+    def set_graph(self, on=True):
+        return lib().dv_batch_set_graph(self.h, int(bool(on)))
+
+    def autotune(self, steps_per_trial=2):
+        rep = TuneReport()
+        st = lib().dv_batch_autotune(self.h, int(steps_per_trial), C.byref(rep))
+        out = rep.as_dict()
+        out["status"] = st
+        return out
+
+    def launches(self):
+        return int(lib().dv_batch_launch_count(self.h))
+
+
+class NativeServer:
+    """Continuous-batching server (dv_server*): requests are admitted as slots and
+    the HBM budget allow, resident scenes step together, finished ones leave."""
+
+    def __init__(self, precision=DV_PREC_MIXED, hbm_budget_bytes=150e9, max_active=4096,
+                 steps_per_round=4, use_graph=True, keep_states=True):
+        L = lib()
+        cfg = ServerConfig()
+        check(L.dv_server_default_config(C.byref(cfg)))
+        cfg.hbm_budget_bytes = float(hbm_budget_bytes)
+        cfg.max_active = int(max_active)
+        cfg.steps_per_round = int(steps_per_round)
+        cfg.precision = int(precision)
+        cfg.use_graph = int(bool(use_graph))
+        cfg.keep_states = int(bool(keep_states))
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(L.dv_server_create(C.byref(cfg), C.byref(h)), "dv_server_create")
+        self.h = h
+        self.sizes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dv_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        check(lib().dv_server_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def clock(self):
+        return float(lib().dv_server_clock(self.h))
+
+    def submit(self, scene, nsteps, **overrides):
+        rec, nb = body_records(scene.pos, scene.vel, scene.mass, scene.geom, scene.fixed,
+                               scene.family)
+        p = dict(scene.params)
+        p.update(overrides)
+        prm = make_params(p, self.cfg.precision)
+        rid = C.c_int64()
+        check(lib().dv_server_submit(self.h, rec.ctypes.data_as(C.POINTER(BodyDesc)), nb,
+                                     C.byref(prm), int(nsteps), C.byref(rid)), "dv_server_submit")
+        self.sizes[rid.value] = nb
+        return rid.value
+
+    def round(self):
+        busy = C.c_int32()
+        check(lib().dv_server_round(self.h, C.byref(busy)), "dv_server_round")
+        return bool(busy.value)
+
+    def poll(self, cap=4096):
+        arr = (RequestResult * cap)()
+        n = C.c_int32()
+        check(lib().dv_server_poll(self.h, arr, cap, C.byref(n)))
+        return [arr[i].as_dict() for i in range(n.value)]
+
+    def result_state(self, rid):
+        nb = self.sizes[rid]
+        p = np.zeros((nb, 3))
+        v = np.zeros((nb, 3))
+        check(lib().dv_server_result_state(self.h, int(rid), dptr(p), dptr(v)))
+        return p, v
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().dv_server_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
+

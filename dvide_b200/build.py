@@ -12,6 +12,7 @@ repository snapshot.
 from __future__ import annotations
 
 import os
+import concurrent.futures
 import subprocess
 import sys
 
@@ -20,8 +21,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
-CUDA_SOURCES = ["dv_sort.cu", "dv_collide.cu", "dv_apgd.cu", "dv_scene.cu", "dv_noalloc.cu"]
-CUDA_HEADERS = ["dv_common.cuh", "dv_internal.cuh"]
+CUDA_SOURCES = ["dv_sort.cu", "dv_collide.cu", "dv_apgd.cu", "dv_engine.cu", "dv_diag.cu", "dv_scene.cu", "dv_batch.cu", "dv_server.cu", "dv_noalloc.cu"]
+CUDA_HEADERS = ["dv_common.cuh", "dv_internal.cuh", "dv_engine.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden"]
@@ -51,15 +52,14 @@ def build_cuda(force=False, verbose=False):
     deps = srcs + [os.path.join(CSRC, h) for h in CUDA_HEADERS] + [os.path.join(INCLUDE, "dvide.h")]
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
     os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
-    for s in srcs:
-        o = os.path.join(HERE, "_build", os.path.basename(s) + ".o")
-        cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-c", s, "-o", o]
-        if verbose:
+    objs = [os.path.join(HERE, "_build", os.path.basename(s) + ".o") for s in srcs]
+    cmds = [[_nvcc(), *ARCH, *NVCC_FLAGS, "-I", INCLUDE, "-c", s, "-o", o] for s, o in zip(srcs, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd))
-        subprocess.check_call(cmd)
-        objs.append(o)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, len(cmds))) as ex:
+        list(ex.map(subprocess.check_call, cmds))
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-lcudart_static"]
     subprocess.check_call(cmd)

@@ -1,5 +1,5 @@
-// dv_apgd.cu -- the time step after collision detection, as ONE persistent
-// cooperative kernel per step:
+// dv_apgd.cu -- the time step after collision detection, for every segment
+// (scene) of an engine, as ONE persistent cooperative kernel per step:
 //
 //   applied impulse k = M v + h f             System.cu:1411-1417, 1502-1514
 //   Schur vector r = D Minv k + b             System.cu:1516-1524, 1561-1580
@@ -9,9 +9,11 @@
 // The reference runs each BLAS-1 call, SpMV and projection as its own launch
 // and brings every dot/nrm2/nrmmax back to the host (APGD.cu:227-350).  Here
 // the scalar control (step size, Lipschitz backtracking, restart, best
-// iterate, convergence) runs on the device: the last CTA to reach each grid
-// barrier folds the per-tile partial sums in a fixed order, executes the
-// control logic and releases the others.
+// iterate, convergence) runs on the device, per segment: the CTA that finishes
+// a segment's last tile of a pass folds that segment's per-tile partial sums in
+// a fixed order and executes its control logic; a grid barrier then starts the
+// next pass.  Segments converge independently (their tiles and bodies are
+// skipped once done); the kernel ends when every segment is done.
 //
 // Matrix-free N x = D Minv D^T x (D's block of contact c is [+F_c^T | -F_c^T],
 // F_c = [n u v]):
@@ -26,12 +28,19 @@
 // y_k = (1 + b) gamma_k - b gamma_{k-1} (APGD.cu:273) or gamma_k after a
 // restart (:315), N y_k is formed here from the stored products of the two
 // previous iterates; N gamma_new is computed once and serves the objective and
-// the residual.  Iterates and their products rotate through four buffers, so
+// the residual.  Iterates and their products rotate through five buffers, so
 // y, g and gamma_hat are never copied.  The CPU oracle evaluates the same
 // sequence (apgd_solve_fused), and bit-for-bit the same arithmetic.
 //
-// Work is split in tiles of 512 contacts (2 per thread) and 256 bodies;
-// CTA b owns tiles b, b + G, ...  Every wait has a time limit.
+// Precision: the kernel is a template on the iterate type T.  T = double is
+// the FP64 path (bit-exact against the oracle).  T = float is the mixed path:
+// frames, Jacobian and N gamma products, iterates and the cone projection in
+// FP32; the Schur vector r (computed in FP64, stored in FP32), the objective
+// and Lipschitz-test sums, the residual, the final D^T gamma and the
+// integration in FP64.
+//
+// Work is split in tiles of 512 contacts (2 per thread) and 256 bodies.
+// Every wait has a time limit.
 #include <stdio.h>
 #include <stdlib.h>
 
@@ -43,96 +52,147 @@ namespace {
 
 constexpr int kNQ = 7;      // partial-sum slots per tile
 constexpr int kQMax = kNQ;  // slot of the per-tile maximum
+constexpr int kWarps = kThreads / 32;
+constexpr int kSub = kThreads;  // contacts per sub-tile
 
-// Phases timed between grid-barrier releases (ApgdCtl::phase_ns).
+// Phases timed between grid-barrier releases (EngineWords::phase_ns).
 enum Phase : int {
   kPhaseSetup = 0,     // k, r, Lipschitz estimate
-  kPhaseStep = 1,      // gamma_new = P(y - t g), full iteration
-  kPhaseBacktrack = 2, // gamma_new recomputed after L doubled
+  kPhaseStep = 1,      // gamma_new = P(y - t g): first iteration or backtrack
   kPhaseBody = 3,      // body gather w = Minv D^T q
-  kPhaseProduct = 4,   // N gamma_new, objective, residual
+  kPhaseProduct = 4,   // N gamma_new, objective, residual, look-ahead step
   kPhaseFinal = 5,     // gamma = gamma_hat, update
 };
 
+template <class T> struct Vec4;
+template <> struct Vec4<double> { using type = double4; };
+template <> struct Vec4<float> { using type = float4; };
+
+template <class T>
 struct KArgs {
-  int nb, nc;
-  int nt, nbt;
-  size_t S;    // plane stride of contact arrays
-  size_t GS;   // plane stride of the warm-start buffer
+  int nb, nseg;
+  int tcap;           // plane stride of the partials
+  int chunk, contiguous;
+  size_t S;           // plane stride of contact arrays
+  size_t WS;          // plane stride of the warm-start arena
   double4* p4;
   double4* v4;
   double4* k4;
   const double4* __restrict__ f4;
-  double4* w4;
   double4* fc4;
+  double4* wd;        // body vector, double4 (setup); reinterpreted as Vec4<T> in iterations
   const double* __restrict__ minv;
+  const int* __restrict__ bseg;
   const uint32_t* __restrict__ ida;
   const uint32_t* __restrict__ idb;
   const double* __restrict__ F;
+  const float* __restrict__ nf;
   const double* __restrict__ gap;
-  double* r;
+  T* r;
   const int* __restrict__ inc_start;
   const uint32_t* __restrict__ inc;
-  double* G[5];
-  double* NG[5];
-  double4* q;
+  T* G[5];
+  T* NG[5];
+  double4* qd;        // contact vector q, double4 (final pass); Vec4<T> in iterations
   double* gamma;
   double* part;
-  int ptiles;
-  ApgdCtl* ctl;
-  unsigned* bar;   // [0] arrivals, [1] generation, [2] error bits
-  double h, mu, tol;
-  int max_iter, max_bt, warm;
+  const SegParams* __restrict__ seg;
+  SegState* sst;
+  const int* __restrict__ tseg;
+  unsigned* donemask;
+  EngineWords* ew;
 };
 
+template <class T>
 struct Frame {
-  double n0, n1, n2, u0, u1, u2, v0, v1, v2;
+  T n0, n1, n2, u0, u1, u2, v0, v1, v2;
 };
 
-// Frame modes: 0 loads n, u, v; 1 recomputes u and v from n with the
-// narrowphase's own function, so both modes see the same bits.
-__device__ inline void complete_frame(Frame& f, int mode) {
-  if (mode == 1) {
-    d3 u, v;
-    frame_from_normal(mk3(f.n0, f.n1, f.n2), &u, &v);
-    f.u0 = u.x; f.u1 = u.y; f.u2 = u.z;
-    f.v0 = v.x; f.v1 = v.y; f.v2 = v.z;
+// System.cu:753-762 in float arithmetic (mixed path).
+__device__ inline void frame_from_normal_f(float n0, float n1, float n2, Frame<float>& f) {
+  float ux, uy, uz;
+  if (n2 != 0.0f) {
+    ux = 1.0f; uy = 0.0f; uz = __fdiv_rn(-n0, n2);
+  } else if (n0 != 0.0f) {
+    ux = __fdiv_rn(-n2, n0); uy = 0.0f; uz = 1.0f;
+  } else {
+    ux = 1.0f; uy = __fdiv_rn(-n0, n1); uz = 0.0f;
   }
+  float iu = __fdiv_rn(1.0f, __fsqrt_rn(ux * ux + uy * uy + uz * uz));
+  ux *= iu; uy *= iu; uz *= iu;
+  float vx = n1 * uz - n2 * uy, vy = n2 * ux - n0 * uz, vz = n0 * uy - n1 * ux;
+  float iv = __fdiv_rn(1.0f, __fsqrt_rn(vx * vx + vy * vy + vz * vz));
+  f.n0 = n0; f.n1 = n1; f.n2 = n2;
+  f.u0 = ux; f.u1 = uy; f.u2 = uz;
+  f.v0 = vx * iv; f.v1 = vy * iv; f.v2 = vz * iv;
 }
 
-template <int kMode>
-__device__ inline Frame load_frame(const KArgs& a, int c) {
-  const double* F = a.F;
-  size_t S = a.S;
-  Frame f;
-  f.n0 = __ldg(F + 0 * S + c);
-  f.n1 = __ldg(F + 1 * S + c);
-  f.n2 = __ldg(F + 2 * S + c);
-  if (kMode == 0) {
-    f.u0 = __ldg(F + 3 * S + c); f.u1 = __ldg(F + 4 * S + c); f.u2 = __ldg(F + 5 * S + c);
-    f.v0 = __ldg(F + 6 * S + c); f.v1 = __ldg(F + 7 * S + c); f.v2 = __ldg(F + 8 * S + c);
-  }
-  complete_frame(f, kMode);
+// The FP64 frame, recomputed from the stored normal with the narrowphase's own
+// function (same bits as the stored u, v planes).
+__device__ inline Frame<double> frame_d(double n0, double n1, double n2) {
+  d3 u, v;
+  frame_from_normal(mk3(n0, n1, n2), &u, &v);
+  Frame<double> f;
+  f.n0 = n0; f.n1 = n1; f.n2 = n2;
+  f.u0 = u.x; f.u1 = u.y; f.u2 = u.z;
+  f.v0 = v.x; f.v1 = v.y; f.v2 = v.z;
   return f;
 }
 
+template <class T> __device__ inline Frame<T> make_frame(T n0, T n1, T n2);
+template <> __device__ inline Frame<double> make_frame<double>(double n0, double n1, double n2) {
+  return frame_d(n0, n1, n2);
+}
+template <> __device__ inline Frame<float> make_frame<float>(float n0, float n1, float n2) {
+  Frame<float> f;
+  frame_from_normal_f(n0, n1, n2, f);
+  return f;
+}
+
+// Normal planes in the solve's precision.
+template <class T> __device__ inline const T* normal_planes(const KArgs<T>& a);
+template <> __device__ inline const double* normal_planes<double>(const KArgs<double>& a) {
+  return a.F;
+}
+template <> __device__ inline const float* normal_planes<float>(const KArgs<float>& a) {
+  return a.nf;
+}
+
+template <class T>
+__device__ inline Frame<T> load_frame(const KArgs<T>& a, int c) {
+  const T* n = normal_planes<T>(a);
+  return make_frame<T>(n[c], n[a.S + c], n[2 * a.S + c]);
+}
+
+template <class T>
+__device__ inline Frame<double> load_frame_fp64(const KArgs<T>& a, int c) {
+  return frame_d(__ldg(a.F + c), __ldg(a.F + a.S + c), __ldg(a.F + 2 * a.S + c));
+}
+
 // q = F x : q_k = (n_k x0 + u_k x1) + v_k x2
-__device__ inline double4 f_times(const Frame& f, double x0, double x1, double x2) {
-  return make_double4((f.n0 * x0 + f.u0 * x1) + f.v0 * x2, (f.n1 * x0 + f.u1 * x1) + f.v1 * x2,
-                      (f.n2 * x0 + f.u2 * x1) + f.v2 * x2, 0.0);
+template <class T, class V>
+__device__ inline V f_times(const Frame<T>& f, T x0, T x1, T x2) {
+  V q;
+  q.x = (f.n0 * x0 + f.u0 * x1) + f.v0 * x2;
+  q.y = (f.n1 * x0 + f.u1 * x1) + f.v1 * x2;
+  q.z = (f.n2 * x0 + f.u2 * x1) + f.v2 * x2;
+  q.w = T(0);
+  return q;
 }
 
 // (F^T d)_row = (f_x d_x + f_y d_y) + f_z d_z with d = w_A - w_B
-__device__ inline void ft_times(const Frame& f, double4 wa, double4 wb, double* o0, double* o1,
-                                double* o2) {
-  double d0 = wa.x - wb.x, d1 = wa.y - wb.y, d2 = wa.z - wb.z;
+template <class T, class V>
+__device__ inline void ft_times(const Frame<T>& f, V wa, V wb, T* o0, T* o1, T* o2) {
+  T d0 = wa.x - wb.x, d1 = wa.y - wb.y, d2 = wa.z - wb.z;
   *o0 = (f.n0 * d0 + f.n1 * d1) + f.n2 * d2;
   *o1 = (f.u0 * d0 + f.u1 * d1) + f.u2 * d2;
   *o2 = (f.v0 * d0 + f.v1 * d1) + f.v2 * d2;
 }
 
-__device__ inline double dot3i(double a0, double a1, double a2, double b0, double b1, double b2) {
-  return (a0 * b0 + a1 * b1) + a2 * b2;
+// Dot products of the reductions, always in FP64.
+template <class A, class B>
+__device__ inline double dot3i(A a0, A a1, A a2, B b0, B b1, B b2) {
+  return ((double)a0 * (double)b0 + (double)a1 * (double)b1) + (double)a2 * (double)b2;
 }
 
 // Folds NQ values of each thread; thread 0 gets the results.
@@ -159,16 +219,17 @@ __device__ inline void block_fold_multi(double (&v)[NQ], double* scratch) {
   __syncthreads();
 }
 
-// Controller side: folds the per-tile partials of NQ quantities in the fixed
-// order (slot j sums tiles j, j+256, ...; then the 256-slot tree).
-template <int NQ>
-__device__ inline void fold_tiles(const KArgs& a, double (&out)[NQ], double* scratch) {
+// Segment controller side: folds the segment's per-tile partials of NQ
+// quantities in the fixed order (slot j sums the segment's tiles j, j+256,
+// ...; then the 256-slot tree).
+template <int NQ, class K>
+__device__ inline void fold_tiles(const K& a, int t0, int nt, double (&out)[NQ], double* scratch) {
   double v[NQ];
 #pragma unroll
   for (int qi = 0; qi < NQ; ++qi) {
     double acc = 0.0;
-    for (int t = threadIdx.x; t < a.nt; t += kThreads)
-      acc = acc + __ldcg(a.part + (size_t)qi * a.ptiles + t);
+    for (int t = threadIdx.x; t < nt; t += kThreads)
+      acc = acc + __ldcg(a.part + (size_t)qi * a.tcap + t0 + t);
     v[qi] = acc;
   }
   block_fold_multi<NQ>(v, scratch);
@@ -176,34 +237,94 @@ __device__ inline void fold_tiles(const KArgs& a, double (&out)[NQ], double* scr
   for (int qi = 0; qi < NQ; ++qi) out[qi] = v[qi];
 }
 
-__device__ inline double fold_tiles_max(const KArgs& a, double* scratch) {
+template <class K>
+__device__ inline double fold_tiles_max(const K& a, int t0, int nt, double* scratch) {
   double m = 0.0;
-  for (int t = threadIdx.x; t < a.nt; t += kThreads)
-    m = fmax(m, __ldcg(a.part + (size_t)kQMax * a.ptiles + t));
+  for (int t = threadIdx.x; t < nt; t += kThreads)
+    m = fmax(m, __ldcg(a.part + (size_t)kQMax * a.tcap + t0 + t));
   double r = block_max256(m, scratch);
   __syncthreads();
   return r;
 }
 
-template <int NQ>
-__device__ inline void write_partials(const KArgs& a, int tile, const double (&v)[NQ]) {
+template <int NQ, class K>
+__device__ inline void write_partials(const K& a, int tile, const double (&v)[NQ]) {
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int qi = 0; qi < NQ; ++qi) a.part[(size_t)qi * a.ptiles + tile] = v[qi];
+    for (int qi = 0; qi < NQ; ++qi) a.part[(size_t)qi * a.tcap + tile] = v[qi];
   }
+}
+
+// Tile arrivals of one segment: a CTA delivers the count of its consecutive
+// tiles of segment s at once (after their partials are written).  True, in
+// every thread, in the CTA whose delivery completes the segment's tiles.
+template <class K>
+__device__ inline bool seg_arrive(const K& a, int s, int n) {
+  __shared__ int s_flag;
+  // thread 0 wrote the tiles' partials itself: no CTA barrier needed before it
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned nt = (unsigned)a.sst[s].nt;
+    unsigned old = atom_add_acq_rel(&a.sst[s].arrive, (unsigned)n);
+    int last = (old + (unsigned)n == nt);
+    if (last) a.sst[s].arrive = 0u;  // the next pass starts after a grid barrier
+    s_flag = last;
+  }
+  __syncthreads();
+  const bool last = s_flag != 0;
+  if (last) __threadfence();
+  return last;
+}
+
+// The segment of a tile and its ranges, cached per CTA for the whole kernel
+// (they do not change during a step): tiles of the cached segment need no
+// loads to find their contacts.
+struct SegCache {
+  int s = -1;
+  int t0 = 0, t1 = 0;   // tiles [t0, t1)
+  int c0 = 0, nc = 0;   // contacts [c0, c0 + nc)
+  int gsize = 0;
+};
+
+template <class K>
+__device__ inline void locate(const K& a, SegCache& c, int t) {
+  if (t >= c.t0 && t < c.t1) return;
+  const int s = a.tseg[t];
+  const SegState& X = a.sst[s];
+  c.s = s;
+  c.t0 = X.t0;
+  c.t1 = X.t0 + X.nt;
+  c.c0 = X.c0;
+  c.nc = X.nc;
+  c.gsize = X.gsize;
+}
+
+struct SegRun {
+  int s = -1;  // segment of the current run of tiles
+  int n = 0;   // tiles of it processed since the last delivery
+};
+
+// Delivers the run's arrivals; the CTA that completes the segment runs ctl(s).
+template <class K, class Fn>
+__device__ inline void flush_run(const K& a, SegRun& run, Fn ctl) {
+  if (run.n == 0) return;
+  const int s = run.s, n = run.n;
+  run.n = 0;
+  if (seg_arrive(a, s, n)) ctl(s);
 }
 
 // Grid barrier.  The last CTA to arrive runs `ctl_fn` (all its threads),
 // then releases the generation word.  Returns false after a timeout or an
 // error raised by another CTA; the caller then leaves the kernel.
-template <class Fn>
-__device__ inline bool grid_sync(const KArgs& a, int phase, Fn ctl_fn) {
+template <class K, class Fn>
+__device__ inline bool grid_sync(const K& a, int phase, Fn ctl_fn) {
   __shared__ unsigned s_last, s_target;
   __shared__ int s_fail;
+  unsigned* bar = a.ew->bar;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    unsigned ticket = atom_add_acq_rel(&a.bar[0], 1u);
+    unsigned ticket = atom_add_acq_rel(&bar[0], 1u);
     s_target = ticket / gridDim.x + 1u;
     s_last = (ticket % gridDim.x) == gridDim.x - 1u;
     s_fail = 0;
@@ -214,28 +335,29 @@ __device__ inline bool grid_sync(const KArgs& a, int phase, Fn ctl_fn) {
     ctl_fn();
     __syncthreads();
     if (threadIdx.x == 0) {
-      ApgdCtl* C = a.ctl;
+      // written by whichever CTA arrives last: no L1-cached copies
+      volatile EngineWords* E = a.ew;
       unsigned long long now = global_ns();
-      if (C->last_release) {
-        C->phase_ns[phase] += now - C->last_release;
-        C->phase_count[phase] += 1;
+      if (E->last_release) {
+        E->phase_ns[phase] += now - E->last_release;
+        E->phase_count[phase] += 1;
       }
-      C->last_release = now;
+      E->last_release = now;
       __threadfence();
-      st_release(&a.bar[1], s_target);
+      st_release(&bar[1], s_target);
     }
   } else if (threadIdx.x == 0) {
     uint64_t t0 = global_ns();
     unsigned polls = 0;
-    while (ld_acquire(&a.bar[1]) < s_target) {
+    while (ld_acquire(&bar[1]) < s_target) {
       __nanosleep(20);
       if ((++polls & 1023u) == 0u) {
-        if (ld_acquire(&a.bar[2]) & (kErrBarrierTimeout | kErrCopyTimeout)) {
+        if (ld_acquire(&a.ew->err) & (kErrBarrierTimeout | kErrCopyTimeout)) {
           s_fail = 1;
           break;
         }
         if (global_ns() - t0 > kBarrierTimeoutNs) {
-          atomicOr(&a.bar[2], kErrBarrierTimeout);
+          atomicOr(&a.ew->err, kErrBarrierTimeout);
           s_fail = 1;
           break;
         }
@@ -251,43 +373,119 @@ struct NoCtl {
   __device__ void operator()() const {}
 };
 
+// Tile i of this CTA's sequence (-1 past the end): round robin in chunks of
+// `chunk` consecutive tiles, or one contiguous range per CTA.
+template <class K>
+__device__ inline int cta_tile(const K& a, int nt, int i) {
+  if (a.contiguous) {
+    long long lo = (long long)nt * blockIdx.x / gridDim.x;
+    long long hi = (long long)nt * (blockIdx.x + 1) / gridDim.x;
+    long long t = lo + i;
+    return t < hi ? (int)t : -1;
+  }
+  const int k = a.chunk;
+  long long t = ((long long)blockIdx.x + (long long)(i / k) * gridDim.x) * k + (i % k);
+  return t < nt ? (int)t : -1;
+}
+
 // Sum of -q over B-side contacts, then +q over A-side contacts, ascending
 // contact order (the flat incidence list); loads are issued in groups of
 // eight, the additions stay in order.
-__device__ inline double4 gather_q(const KArgs& a, int b) {
-  double ax = 0.0, ay = 0.0, az = 0.0;
+template <class T, class V, class K>
+__device__ inline V gather_q(const K& a, const V* q, int b) {
+  T ax = T(0), ay = T(0), az = T(0);
   const int s = __ldg(a.inc_start + b), e = __ldg(a.inc_start + b + 1);
   for (int i = s; i < e; i += 8) {
     uint32_t c[8];
-    double4 q[8];
+    V qq[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) c[j] = (i + j < e) ? __ldg(a.inc + i + j) : 0u;
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-      q[j] = (i + j < e) ? a.q[c[j] & 0x7fffffffu] : make_double4(0, 0, 0, 0);
+    for (int j = 0; j < 8; ++j) {
+      if (i + j < e) {
+        qq[j] = q[c[j] & 0x7fffffffu];
+      } else {
+        qq[j].x = T(0); qq[j].y = T(0); qq[j].z = T(0); qq[j].w = T(0);
+      }
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       if (i + j < e) {
         if (c[j] & 0x80000000u) {
-          ax = ax - q[j].x; ay = ay - q[j].y; az = az - q[j].z;
+          ax = ax - qq[j].x; ay = ay - qq[j].y; az = az - qq[j].z;
         } else {
-          ax = ax + q[j].x; ay = ay + q[j].y; az = az + q[j].z;
+          ax = ax + qq[j].x; ay = ay + qq[j].y; az = az + qq[j].z;
         }
       }
     }
   }
-  return make_double4(ax, ay, az, 0.0);
+  V r;
+  r.x = ax; r.y = ay; r.z = az; r.w = T(0);
+  return r;
 }
 
-// Schur body pass: w_b = minv_b * (D^T x)_b; fixed bodies keep w = 0.
-__device__ inline void body_pass_schur(const KArgs& a) {
-  for (int bt = blockIdx.x; bt < a.nbt; bt += gridDim.x) {
+// A solver error of segment s; with stop_on_seg_err it also stops the steps
+// that follow (every kernel checks EngineWords::err first).
+template <class K>
+__device__ inline void seg_error(const K& a, int s, unsigned bit) {
+  atomicOr(&a.sst[s].err, bit);
+  if (a.ew->stop_on_seg_err) atomicOr(&a.ew->err, bit);
+}
+
+// Done mask: bit s set when segment s is not iterating.  Each pass starts
+// with a copy in shared memory (segments beyond kMaskWords * 32 read it from
+// global memory).
+constexpr int kMaskWords = 256;
+
+template <class K>
+__device__ inline void load_mask(const K& a, unsigned* s_mask, int mwords) {
+  if (a.nseg == 1) return;  // a single segment iterates while the loop runs
+  __syncthreads();
+  for (int i = threadIdx.x; i < mwords && i < kMaskWords; i += kThreads)
+    s_mask[i] = __ldcg(a.donemask + i);
+  __syncthreads();
+}
+
+template <class K>
+__device__ inline bool mask_done(const K& a, const unsigned* s_mask, int mwords, int s) {
+  if (a.nseg == 1) return false;
+  const int w = s >> 5;
+  const unsigned m = (w < kMaskWords) ? s_mask[w] : __ldcg(a.donemask + w);
+  return (m >> (s & 31)) & 1u;
+}
+
+// Segment s stops iterating (controller thread).
+template <class K>
+__device__ inline void mark_done(const K& a, int s) {
+  volatile ApgdCtl* C = &a.sst[s].ctl;
+  C->done = 1;
+  atomicOr(a.donemask + (s >> 5), 1u << (s & 31));
+}
+
+// Schur body pass: w_b = minv_b * (D^T x)_b for bodies of iterating
+// segments; fixed bodies keep w = 0.
+template <class T>
+__device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask) {
+  using V = typename Vec4<T>::type;
+  V* w = reinterpret_cast<V*>(a.wd);
+  const V* q = reinterpret_cast<const V*>(a.qd);
+  const int nbt = (a.nb + kThreads - 1) / kThreads;
+  const int mwords = (a.nseg + 31) >> 5;
+  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
-    if (b < a.nb) {
+    if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b)))) {
       double mi = __ldg(a.minv + b);
       if (mi != 0.0) {
-        double4 s = gather_q(a, b);
-        a.w4[b] = make_double4(mi * s.x, mi * s.y, mi * s.z, 0.0);
+        V s = gather_q<T, V>(a, q, b);
+        T m = (T)mi;
+        V o;
+        o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
+        w[b] = o;
+      } else if (sizeof(T) != sizeof(double)) {
+        // the FP32 view of w overlays the FP64 setup values: store the zero
+        V o;
+        o.x = T(0); o.y = T(0); o.z = T(0); o.w = T(0);
+        w[b] = o;
       }
     }
   }
@@ -305,19 +503,21 @@ __device__ inline int free_slot(int a, int b, int c, int d) {
 // sub-tiles (256 consecutive contacts, kItemsPerThread per reduction tile) in
 // order; warp w owns contacts [32w, 32w+32) of each sub-tile and two stages of
 // its own.  While the warp computes sub-tile i from one stage, its lane 0 has
-// already issued the bulk copies of sub-tile i+1's plane segments (256 bytes
+// already issued the bulk copies of sub-tile i+1's plane segments (32 values
 // per plane) into the other stage, completed on the warp's own mbarrier, so
 // warps never wait for each other except at the per-tile reduction.
+// Planes: n (3), gamma_new (3), r (3), gamma_k (3), N gamma_k (3); ids A, B.
+// A segment's contacts start on a multiple of 256, so every copy starts on a
+// 128-byte boundary.
 // ---------------------------------------------------------------------------
-constexpr int kWarps = kThreads / 32;
-constexpr int kSub = kThreads;  // contacts per sub-tile
-__host__ __device__ constexpr int kFramePlanes(int mode) { return mode == 0 ? 9 : 3; }
-__host__ __device__ constexpr int kStagePlanesD(int mode) { return kFramePlanes(mode) + 12; }
-__host__ __device__ constexpr unsigned kWarpStageBytes(int mode) {
-  return (unsigned)kStagePlanesD(mode) * 32u * 8u + 2u * 32u * 4u;
+constexpr int kStagePlanes = 15;
+template <class T>
+__host__ __device__ constexpr unsigned warp_stage_bytes() {
+  return (unsigned)kStagePlanes * 32u * (unsigned)sizeof(T) + 2u * 32u * 4u;
 }
-__host__ __device__ constexpr size_t kDynSmem(int mode) {
-  return (size_t)kWarps * 2 * kWarpStageBytes(mode) + (size_t)kWarps * 2 * 8;
+template <class T>
+__host__ __device__ constexpr size_t dyn_smem_bytes() {
+  return (size_t)kWarps * 2 * warp_stage_bytes<T>() + (size_t)kWarps * 2 * 8;
 }
 
 struct Staging {
@@ -328,7 +528,8 @@ struct Staging {
 };
 
 // Bounded wait for this warp's stage s; false after a timeout (error recorded).
-__device__ inline bool wait_warp_stage(const KArgs& a, Staging& st, int s) {
+template <class K>
+__device__ inline bool wait_warp_stage(const K& a, Staging& st, int s) {
   const int w = threadIdx.x >> 5;
   unsigned par = (st.phase >> s) & 1u;
   uint64_t* bar = st.bar + 2 * w + s;
@@ -340,20 +541,181 @@ __device__ inline bool wait_warp_stage(const KArgs& a, Staging& st, int s) {
     }
   }
   st.phase ^= (1u << s);
-  if (!ok) atomicOr(&a.bar[2], kErrCopyTimeout);
+  if (!ok) atomicOr(&a.ew->err, kErrCopyTimeout);
   __syncwarp();
   return ok;
 }
 
-template <int kFrame, int kMinB>
-__global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs a) {
+// Scalars of a segment's product pass.
+// Per-segment scalars of the step and product passes, kept in shared memory
+// (written by thread 0 when the CTA moves to another segment) so that they
+// take no registers in the contact loops.
+struct ProdScalars {
+  int cur, nw, nw2, restart;
+  double ya, ym, nt2, gd, gA, gB, mu;
+};
+struct StepScalars {
+  int part, first, cur, prev, nw, yr;
+  double ya, ym, nt, mu;
+};
+
+// What the segment controllers read and write, passed by value.
+struct CtlArgs {
+  double* part;
+  int tcap;
+  SegState* sst;
+  const SegParams* seg;
+  EngineWords* ew;
+  unsigned* donemask;
+};
+
+// Segment controllers, run by the CTA that completes a segment's tiles of a
+// pass (all its threads; thread 0 writes).  Kept out of line so that their
+// registers do not weigh on the contact-pass loops.
+__device__ __noinline__ void ctl_setup(CtlArgs a, int s, double* scratch) {
+  double sm[1];
+  fold_tiles<1>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
+  if (threadIdx.x == 0) {
+    volatile ApgdCtl* C = &a.sst[s].ctl;
+    C->L0 = sqrt(sm[0]);
+  }
+}
+
+__device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
+  double sm[1];
+  fold_tiles<1>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
+  if (threadIdx.x == 0) {
+    const SegParams& P = a.seg[s];
+    volatile ApgdCtl* C = &a.sst[s].ctl;
+    double L = sqrt(sm[0]) / C->L0;
+    C->L = L;
+    C->t = 1.0 / L;
+    C->theta = 1.0;
+    double th = 1.0;
+    C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
+    C->beta = th * (1.0 - th) / (th * th + C->theta_new);
+    C->residual = 10e30;
+    C->objective = 0.0;
+    double ncd = (double)a.sst[s].nc;
+    C->gdiff = 1.0 / (ncd * ncd);
+    C->ginv = 1.0 / C->gdiff;
+    C->k = 0;
+    C->mode = 0;
+    C->iterations = 0;
+    C->sweeps = 0;
+    C->restart = 0;
+    C->cur = 0;
+    C->prev = -1;
+    C->nw = 1;
+    C->best = -1;
+    C->yr = 1;
+    C->yb = 0.0;
+    C->first = 1;
+    C->backtracks = 0;
+    C->obj1 = C->obj2 = C->obj2_base = 0.0;
+    if (P.max_iter <= 0) {
+      mark_done(a, s);
+    } else {
+      C->done = 0;
+      atomicAdd(&a.ew->active, 1);
+      atomicAdd(&a.ew->step_count, 1);
+    }
+  }
+}
+
+__device__ __noinline__ void ctl_step(CtlArgs a, int s, double* scratch) {
+  double sm[5];
+  fold_tiles<5>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
+  if (threadIdx.x == 0) {
+    volatile ApgdCtl* W = &a.sst[s].ctl;
+    if (W->first) W->obj2_base = 0.5 * sm[3] + sm[4];
+    double nr = sqrt(sm[1]);
+    W->obj2 = W->obj2_base + (sm[0] + 0.5 * W->L * (nr * nr));
+    W->restart = (sm[2] > 0) ? 1 : 0;
+    W->first = 0;
+  }
+}
+
+__device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
+  double sm[7];
+  fold_tiles<7>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
+  double res = fold_tiles_max(a, a.sst[s].t0, a.sst[s].nt, scratch);
+  if (threadIdx.x == 0) {
+    const SegParams& P = a.seg[s];
+    volatile ApgdCtl* C = &a.sst[s].ctl;
+    double obj1 = 0.5 * sm[0] + sm[1];
+    C->obj1 = obj1;
+    bool finished = false;
+    if (obj1 >= C->obj2) {
+      // (10)-(14): double L and retry the projection
+      if (C->backtracks >= P.max_bt) {
+        seg_error(a, s, kErrBacktrackCap);
+        finished = true;
+      } else {
+        C->backtracks += 1;
+        C->L = 2.0 * C->L;
+        C->t = 1.0 / C->L;
+        C->mode = 1;
+        atomicAdd(&a.ew->step_count, 1);
+      }
+    } else {
+      C->mode = 0;
+      C->sweeps += 1;
+      int old_best = C->best;
+      if (res < C->residual) {
+        C->residual = res;
+        C->objective = obj1;
+        C->best = C->nw;
+      }
+      if (C->residual < P.tol) {
+        finished = true;
+      } else {
+        double th = C->restart ? 1.0 : C->theta_new;
+        C->yb = C->beta;
+        C->yr = C->restart;
+        C->L = 0.9 * C->L;
+        C->t = 1.0 / C->L;
+        C->theta = th;
+        int nw2 = free_slot(C->nw, C->cur, C->prev, old_best);
+        C->prev = C->cur;
+        C->cur = C->nw;
+        C->nw = nw2;
+        C->k += 1;
+        if (C->k >= P.max_iter) {
+          finished = true;
+        } else {
+          C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
+          C->beta = th * (1.0 - th) / (th * th + C->theta_new);
+          // the look-ahead step is now iteration k's step
+          C->obj2_base = 0.5 * sm[5] + sm[6];
+          double nr = sqrt(sm[3]);
+          C->obj2 = C->obj2_base + (sm[2] + 0.5 * C->L * (nr * nr));
+          C->restart = (sm[4] > 0) ? 1 : 0;
+        }
+      }
+    }
+    if (finished) {
+      C->iterations = C->k;
+      mark_done(a, s);
+      atomicSub(&a.ew->active, 1);
+    }
+  }
+}
+
+template <class T, int kMinB>
+__global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
+  using V = typename Vec4<T>::type;
   __shared__ double scratch[kNQ * 8 + 8];
+  __shared__ unsigned s_mask[kMaskWords];
+  __shared__ ProdScalars s_ps;
+  __shared__ StepScalars s_st;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   const size_t S = a.S;
-  const double h = a.h;
+  V* wv = reinterpret_cast<V*>(a.wd);
+  V* qv = reinterpret_cast<V*>(a.qd);
   Staging stg;
   stg.base = dyn_smem;
-  stg.stage_bytes = kWarpStageBytes(kFrame);
+  stg.stage_bytes = warp_stage_bytes<T>();
   stg.bar = reinterpret_cast<uint64_t*>(dyn_smem + (size_t)kWarps * 2 * stg.stage_bytes);
   stg.phase = 0;
   if (threadIdx.x == 0) {
@@ -361,116 +723,164 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs a) {
     fence_mbar_init();
   }
   __syncthreads();
+  if (ld_acquire(&a.ew->err)) return;  // an error of collision detection: nothing to do
+  const int NT = a.ew->ntiles;
+  const int nbt = (a.nb + kThreads - 1) / kThreads;
+  const int mwords = (a.nseg + 31) >> 5;
+  SegCache sc;  // segment of the CTA's current tile
+  const CtlArgs ca{a.part, a.tcap, a.sst, a.seg, a.ew, a.donemask};
+
+  // ---- per-segment solve state; done mask (bit set: not iterating)
+  for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.nseg; s += gridDim.x * kThreads) {
+    SegState& X = a.sst[s];
+    X.err = 0u;
+    X.arrive = 0u;
+    ApgdCtl& C = X.ctl;
+    const bool live = a.seg[s].active && X.nc > 0;
+    C.done = live ? 0 : 1;
+    C.iterations = 0;
+    C.sweeps = 0;
+    C.backtracks = 0;
+    C.residual = 0.0;
+    C.objective = 0.0;
+    C.best = -1;
+  }
+  for (int wi = blockIdx.x * kThreads + threadIdx.x; wi < mwords; wi += gridDim.x * kThreads) {
+    unsigned m = 0u;
+    for (int j = 0; j < 32; ++j) {
+      const int s = wi * 32 + j;
+      if (s >= a.nseg || !(a.seg[s].active && a.sst[s].nc > 0)) m |= 1u << j;
+    }
+    a.donemask[wi] = m;
+  }
 
   // ---- applied impulse: k = m v + h f (m = 1/minv, 0 for fixed); w = minv k
-  for (int bt = blockIdx.x; bt < a.nbt; bt += gridDim.x) {
+  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
     if (b < a.nb) {
-      double mi = __ldg(a.minv + b);
-      double m = mi;
-      if (m) m = 1.0 / m;
-      double4 v = a.v4[b], f = a.f4[b];
-      double4 k = make_double4(h * f.x + m * v.x, h * f.y + m * v.y, h * f.z + m * v.z, 0.0);
-      a.k4[b] = k;
-      a.w4[b] = make_double4(mi * k.x, mi * k.y, mi * k.z, 0.0);
-    }
-  }
-  if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
-
-  // ---- r = D (Minv k) + b; gamma_0 -> G[0]; e = gamma_0 - gamma_hat_0 (= gamma_0 - 1)
-  for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
-    double acc[1] = {0.0};
-    for (int m = 0; m < kItemsPerThread; ++m) {
-      int c = tile * kTileItems + m * kThreads + threadIdx.x;
-      if (c < a.nc) {
-        Frame f = load_frame<kFrame>(a, c);
-        double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
-        double d0, d1, d2;
-        ft_times(f, wa, wb, &d0, &d1, &d2);
-        double bn = __ldg(a.gap + c) / h;
-        a.r[0 * S + c] = bn + d0;
-        a.r[1 * S + c] = 0.0 + d1;
-        a.r[2 * S + c] = 0.0 + d2;
-        double g0, g1, g2;
-        if (a.warm) {
-          g0 = a.gamma[0 * a.GS + c];
-          g1 = a.gamma[1 * a.GS + c];
-          g2 = a.gamma[2 * a.GS + c];
-        } else {
-          g0 = 1.0; g1 = 0.0; g2 = 0.0;
-        }
-        a.G[0][0 * S + c] = g0; a.G[0][1 * S + c] = g1; a.G[0][2 * S + c] = g2;
-        double e0 = g0 + (-1.0), e1 = g1 + (-1.0), e2 = g2 + (-1.0);
-        acc[0] = acc[0] + dot3i(e0, e1, e2, e0, e1, e2);
-        a.q[c] = f_times(f, e0, e1, e2);
+      const SegParams& P = a.seg[__ldg(a.bseg + b)];
+      if (P.active) {
+        const double h = P.h;
+        double mi = __ldg(a.minv + b);
+        double m = mi;
+        if (m) m = 1.0 / m;
+        double4 v = a.v4[b], f = a.f4[b];
+        double4 k = make_double4(h * f.x + m * v.x, h * f.y + m * v.y, h * f.z + m * v.z, 0.0);
+        a.k4[b] = k;
+        a.wd[b] = make_double4(mi * k.x, mi * k.y, mi * k.z, 0.0);
       }
     }
-    block_fold_multi<1>(acc, scratch);
-    write_partials<1>(a, tile, acc);
   }
   if (!grid_sync(a, kPhaseSetup, [&]() {
-        double s[1];
-        fold_tiles<1>(a, s, scratch);
-        if (threadIdx.x == 0) a.ctl->L0 = sqrt(s[0]);
+        if (threadIdx.x == 0) {
+          atomicExch(&a.ew->active, 0);
+          atomicExch(&a.ew->step_count, 0);
+          *(volatile int*)&a.ew->step_needed = 0;
+        }
       }))
     return;
-  body_pass_schur(a);
+
+  // ---- r = D (Minv k) + b; gamma_0 -> G[0]; e = gamma_0 - gamma_hat_0 (= gamma_0 - 1)
+  {
+    SegRun run;
+    auto ctl = [&](int s) { ctl_setup(ca, s, scratch); };
+    for (int i = 0;; ++i) {
+      const int t = cta_tile(a, NT, i);
+      if (t < 0) break;
+      locate(a, sc, t);
+      const int s = sc.s;
+      if (s != run.s) {
+        flush_run(a, run, ctl);
+        run.s = s;
+      }
+      const SegParams& P = a.seg[s];
+      const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0, gsize = sc.gsize;
+      const double h = P.h;
+      double acc[1] = {0.0};
+      for (int m = 0; m < kItemsPerThread; ++m) {
+        int k = k0 + m * kThreads + threadIdx.x;
+        if (k < nc) {
+          const int c = c0 + k;
+          Frame<double> fd = load_frame_fp64(a, c);
+          double4 wa = a.wd[__ldg(a.ida + c)], wb = a.wd[__ldg(a.idb + c)];
+          double d0, d1, d2;
+          ft_times<double, double4>(fd, wa, wb, &d0, &d1, &d2);
+          double bn = __ldg(a.gap + c) / h;
+          a.r[0 * S + c] = (T)(bn + d0);
+          a.r[1 * S + c] = (T)(0.0 + d1);
+          a.r[2 * S + c] = (T)(0.0 + d2);
+          double g0, g1, g2;
+          if (P.warm) {
+            const size_t wi = (size_t)P.wbase + k;
+            g0 = k < gsize ? a.gamma[0 * a.WS + wi] : 0.0;
+            g1 = k < gsize ? a.gamma[1 * a.WS + wi] : 0.0;
+            g2 = k < gsize ? a.gamma[2 * a.WS + wi] : 0.0;
+          } else {
+            g0 = 1.0; g1 = 0.0; g2 = 0.0;
+          }
+          const T x0 = (T)g0, x1 = (T)g1, x2 = (T)g2;
+          a.G[0][0 * S + c] = x0; a.G[0][1 * S + c] = x1; a.G[0][2 * S + c] = x2;
+          const T e0 = x0 + T(-1), e1 = x1 + T(-1), e2 = x2 + T(-1);
+          acc[0] = acc[0] + dot3i(e0, e1, e2, e0, e1, e2);
+          Frame<T> f = load_frame<T>(a, c);
+          qv[c] = f_times<T, V>(f, e0, e1, e2);
+        }
+      }
+      block_fold_multi<1>(acc, scratch);
+      write_partials<1>(a, t, acc);
+      ++run.n;
+    }
+    flush_run(a, run, ctl);
+  }
+  if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
+  load_mask(a, s_mask, mwords);
+  body_pass_schur(a, s_mask);
   if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
   // ---- L = ||N e|| / ||e||; q = F gamma_0 for the first N y
-  for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
-    double acc[1] = {0.0};
-    for (int m = 0; m < kItemsPerThread; ++m) {
-      int c = tile * kTileItems + m * kThreads + threadIdx.x;
-      if (c < a.nc) {
-        Frame f = load_frame<kFrame>(a, c);
-        double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
-        double n0, n1, n2;
-        ft_times(f, wa, wb, &n0, &n1, &n2);
-        acc[0] = acc[0] + dot3i(n0, n1, n2, n0, n1, n2);
-        double y0 = a.G[0][0 * S + c], y1 = a.G[0][1 * S + c], y2 = a.G[0][2 * S + c];
-        a.q[c] = f_times(f, y0, y1, y2);
+  {
+    SegRun run;
+    auto ctl = [&](int s) { ctl_lipschitz(ca, s, scratch); };
+    for (int i = 0;; ++i) {
+      const int t = cta_tile(a, NT, i);
+      if (t < 0) break;
+      locate(a, sc, t);
+      const int s = sc.s;
+      if (s != run.s) {
+        flush_run(a, run, ctl);
+        run.s = s;
       }
-    }
-    block_fold_multi<1>(acc, scratch);
-    write_partials<1>(a, tile, acc);
-  }
-  if (!grid_sync(a, kPhaseSetup, [&]() {
-        double s[1];
-        fold_tiles<1>(a, s, scratch);
-        if (threadIdx.x == 0) {
-          ApgdCtl* C = a.ctl;
-          double L = sqrt(s[0]) / C->L0;
-          C->L = L;
-          C->t = 1.0 / L;
-          C->theta = 1.0;
-          double th = 1.0;
-          C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
-          C->beta = th * (1.0 - th) / (th * th + C->theta_new);
-          C->residual = 10e30;
-          C->objective = 0.0;
-          double ncd = (double)a.nc;
-          C->gdiff = 1.0 / (ncd * ncd);
-          C->ginv = 1.0 / C->gdiff;
-          C->k = 0;
-          C->mode = 0;
-          C->done = (a.max_iter <= 0) ? 1 : 0;
-          C->iterations = 0;
-          C->sweeps = 0;
-          C->restart = 0;
-          C->cur = 0;
-          C->prev = -1;
-          C->nw = 1;
-          C->best = -1;
-          C->yr = 1;
-          C->yb = 0.0;
-          C->first = 1;
-          C->backtracks = 0;
-          C->obj1 = C->obj2 = C->obj2_base = 0.0;
+      const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
+      double acc[1] = {0.0};
+      for (int m = 0; m < kItemsPerThread; ++m) {
+        int k = k0 + m * kThreads + threadIdx.x;
+        if (k < nc) {
+          const int c = c0 + k;
+          Frame<T> f = load_frame<T>(a, c);
+          V wa = wv[__ldg(a.ida + c)], wb = wv[__ldg(a.idb + c)];
+          T n0, n1, n2;
+          ft_times<T, V>(f, wa, wb, &n0, &n1, &n2);
+          acc[0] = acc[0] + dot3i(n0, n1, n2, n0, n1, n2);
+          T y0 = a.G[0][0 * S + c], y1 = a.G[0][1 * S + c], y2 = a.G[0][2 * S + c];
+          qv[c] = f_times<T, V>(f, y0, y1, y2);
         }
-      }))
-    return;
-  body_pass_schur(a);
+      }
+      block_fold_multi<1>(acc, scratch);
+      write_partials<1>(a, t, acc);
+      ++run.n;
+    }
+    flush_run(a, run, ctl);
+  }
+  // step_count is raised by atomics of other CTAs: read and clear it atomically
+  auto latch = [&]() {
+    if (threadIdx.x == 0) {
+      int n = atomicExch(&a.ew->step_count, 0);
+      *(volatile int*)&a.ew->step_needed = n;
+    }
+  };
+  if (!grid_sync(a, kPhaseSetup, latch)) return;
+  load_mask(a, s_mask, mwords);
+  body_pass_schur(a, s_mask);
   if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
   // ---- APGD iterations (APGD.cu:227-350)
@@ -481,42 +891,79 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs a) {
   // whole step of iteration k+1 (y, N y, g, gamma_new = P(y - t g), q).  When
   // the test fails (backtracking) the look-ahead is discarded and a step pass
   // recomputes gamma_new with the doubled L; the arithmetic of every value is
-  // the same either way.
-  bool step_pass = true;  // the first iteration's step: N y_0 is a product (w of gamma_0)
+  // the same either way.  A segment's first step is a step pass too (N y_0
+  // is a product: w of gamma_0).  Segment scalars are loaded once per run of
+  // consecutive tiles of one segment.
   for (;;) {
-    if (__ldcg(&a.ctl->done)) break;  // maxIterations reached (0 included)
-    if (step_pass) {
-      const int first = __ldcg(&a.ctl->first);
-      const int cur = __ldcg(&a.ctl->cur);
-      const int prev = __ldcg(&a.ctl->prev);
-      const int nw = __ldcg(&a.ctl->nw);
-      const int yr = __ldcg(&a.ctl->yr);
-      const double yb = __ldcg(&a.ctl->yb);
-      const double ya = 1.0 + yb, ym = -yb;
-      const double nt_ = -__ldcg(&a.ctl->t);
-      const double* Gc = a.G[cur];
-      const double* Gp = a.G[prev < 0 ? cur : prev];
-      double* NGc = a.NG[cur];
-      const double* NGp = a.NG[prev < 0 ? cur : prev];
-      double* Gn = a.G[nw];
-      for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
+    if (__ldcg(&a.ew->active) == 0) break;
+    // the done mask at the start of a pass holds for every tile this CTA has
+    // left in the pass: a segment finishes only after all its tiles
+    load_mask(a, s_mask, mwords);
+    if (__ldcg(&a.ew->step_needed) > 0) {
+      SegRun run;
+      auto ctl = [&](int s) { ctl_step(ca, s, scratch); };
+      int cs = -1;
+      for (int i = 0;; ++i) {
+        const int t = cta_tile(a, NT, i);
+        if (t < 0) break;
+        locate(a, sc, t);
+        const int s = sc.s;
+        if (s != cs) {
+          cs = s;
+          __syncthreads();
+          if (threadIdx.x == 0) {
+            int part = !mask_done(a, s_mask, mwords, s);
+            if (part) {
+              const ApgdCtl* C = &a.sst[s].ctl;
+              const int first = __ldcg(&C->first);
+              part = first || __ldcg(&C->mode) == 1;
+              s_st.first = first;
+              s_st.cur = __ldcg(&C->cur);
+              s_st.prev = __ldcg(&C->prev);
+              s_st.nw = __ldcg(&C->nw);
+              s_st.yr = __ldcg(&C->yr);
+              const double yb = __ldcg(&C->yb);
+              s_st.ya = 1.0 + yb;
+              s_st.ym = -yb;
+              s_st.nt = -__ldcg(&C->t);
+              s_st.mu = a.seg[s].mu;
+            }
+            s_st.part = part;
+          }
+          __syncthreads();
+        }
+        const bool part = s_st.part != 0;
+        if (!part) continue;
+        if (s != run.s) {
+          flush_run(a, run, ctl);
+          run.s = s;
+        }
+        const int cur = s_st.cur, prev = s_st.prev, first = s_st.first, yr = s_st.yr;
+        const T ya = (T)s_st.ya, ym = (T)s_st.ym, nt_ = (T)s_st.nt, mu = (T)s_st.mu;
+        const T* Gc = a.G[cur];
+        const T* Gp = a.G[prev < 0 ? cur : prev];
+        T* NGc = a.NG[cur];
+        const T* NGp = a.NG[prev < 0 ? cur : prev];
+        T* Gn = a.G[s_st.nw];
+        const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         for (int m = 0; m < kItemsPerThread; ++m) {
-          int c = tile * kTileItems + m * kThreads + threadIdx.x;
-          if (c < a.nc) {
-            Frame f = load_frame<kFrame>(a, c);
-            double c0 = Gc[0 * S + c], c1 = Gc[1 * S + c], c2 = Gc[2 * S + c];
-            double y0, y1, y2, N0, N1, N2;
+          int k = k0 + m * kThreads + threadIdx.x;
+          if (k < nc) {
+            const int c = c0 + k;
+            Frame<T> f = load_frame<T>(a, c);
+            T c0v = Gc[0 * S + c], c1v = Gc[1 * S + c], c2v = Gc[2 * S + c];
+            T y0, y1, y2, N0, N1, N2;
             if (yr) {
-              y0 = c0; y1 = c1; y2 = c2;
+              y0 = c0v; y1 = c1v; y2 = c2v;
             } else {
-              y0 = ya * c0 + ym * Gp[0 * S + c];
-              y1 = ya * c1 + ym * Gp[1 * S + c];
-              y2 = ya * c2 + ym * Gp[2 * S + c];
+              y0 = ya * c0v + ym * Gp[0 * S + c];
+              y1 = ya * c1v + ym * Gp[1 * S + c];
+              y2 = ya * c2v + ym * Gp[2 * S + c];
             }
             if (first) {
-              double4 wa = a.w4[__ldg(a.ida + c)], wb = a.w4[__ldg(a.idb + c)];
-              ft_times(f, wa, wb, &N0, &N1, &N2);
+              V wa = wv[__ldg(a.ida + c)], wb = wv[__ldg(a.idb + c)];
+              ft_times<T, V>(f, wa, wb, &N0, &N1, &N2);
               NGc[0 * S + c] = N0; NGc[1 * S + c] = N1; NGc[2 * S + c] = N2;
             } else if (yr) {
               N0 = NGc[0 * S + c]; N1 = NGc[1 * S + c]; N2 = NGc[2 * S + c];
@@ -525,14 +972,14 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs a) {
               N1 = ya * NGc[1 * S + c] + ym * NGp[1 * S + c];
               N2 = ya * NGc[2 * S + c] + ym * NGp[2 * S + c];
             }
-            double r0 = a.r[0 * S + c], r1 = a.r[1 * S + c], r2 = a.r[2 * S + c];
-            double g0 = N0 + r0, g1 = N1 + r1, g2 = N2 + r2;
-            double x0 = y0 + nt_ * g0, x1 = y1 + nt_ * g1, x2 = y2 + nt_ * g2;
-            project_cone<double>(x0, x1, x2, a.mu);
+            T r0 = a.r[0 * S + c], r1 = a.r[1 * S + c], r2 = a.r[2 * S + c];
+            T g0 = N0 + r0, g1 = N1 + r1, g2 = N2 + r2;
+            T x0 = y0 + nt_ * g0, x1 = y1 + nt_ * g1, x2 = y2 + nt_ * g2;
+            project_cone<T>(x0, x1, x2, mu);
             Gn[0 * S + c] = x0; Gn[1 * S + c] = x1; Gn[2 * S + c] = x2;
-            a.q[c] = f_times(f, x0, x1, x2);
-            double t0 = x0 + (-1.0) * y0, t1 = x1 + (-1.0) * y1, t2 = x2 + (-1.0) * y2;
-            double s0 = x0 + (-1.0) * c0, s1 = x1 + (-1.0) * c1, s2 = x2 + (-1.0) * c2;
+            qv[c] = f_times<T, V>(f, x0, x1, x2);
+            T t0 = x0 + T(-1) * y0, t1 = x1 + T(-1) * y1, t2 = x2 + T(-1) * y2;
+            T s0 = x0 + T(-1) * c0v, s1 = x1 + T(-1) * c1v, s2 = x2 + T(-1) * c2v;
             acc[0] = acc[0] + dot3i(g0, g1, g2, t0, t1, t2);
             acc[1] = acc[1] + dot3i(t0, t1, t2, t0, t1, t2);
             acc[2] = acc[2] + dot3i(g0, g1, g2, s0, s1, s2);
@@ -543,392 +990,374 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs a) {
           }
         }
         block_fold_multi<5>(acc, scratch);
-        write_partials<5>(a, tile, acc);
+        write_partials<5>(a, t, acc);
+        ++run.n;
       }
-      if (!grid_sync(a, first ? kPhaseStep : kPhaseBacktrack, [&]() {
-            double s[5];
-            fold_tiles<5>(a, s, scratch);
-            if (threadIdx.x == 0) {
-              ApgdCtl* C = a.ctl;
-              if (C->first) C->obj2_base = 0.5 * s[3] + s[4];
-              double nr = sqrt(s[1]);
-              C->obj2 = C->obj2_base + (s[0] + 0.5 * C->L * (nr * nr));
-              C->restart = (s[2] > 0) ? 1 : 0;
-              C->first = 0;
-            }
-          }))
-        return;
+      flush_run(a, run, ctl);
+      if (!grid_sync(a, kPhaseStep, NoCtl{})) return;
     }
-    body_pass_schur(a);
+    body_pass_schur(a, s_mask);
     if (!grid_sync(a, kPhaseBody, NoCtl{})) return;
 
     // N gamma_new, objective (APGD.cu:237-238), residual (:90-102); then the
     // next iteration's step assuming gamma_new is accepted (:266-273, 312-332)
     {
-      const int cur = __ldcg(&a.ctl->cur);
-      const int prev = __ldcg(&a.ctl->prev);
-      const int nw = __ldcg(&a.ctl->nw);
-      const int best = __ldcg(&a.ctl->best);
-      const int nw2 = free_slot(nw, cur, prev, best);
-      const int restart = __ldcg(&a.ctl->restart);
-      const double beta = __ldcg(&a.ctl->beta);
-      const double ya = 1.0 + beta, ym = -beta;
-      const double Lnext = 0.9 * __ldcg(&a.ctl->L);
-      const double nt2 = -(1.0 / Lnext);
-      const double gd = __ldcg(&a.ctl->gdiff);
-      const double gA = __ldcg(&a.ctl->ginv);
-      const double gB = -1.0 / gd;
-      double* NGn = a.NG[nw];
-      double* G2 = a.G[nw2];
-      // staged planes: frame, gamma_new, r, gamma_k, N gamma_k; then ids A, B
-      constexpr int FP = kFramePlanes(kFrame);
-      constexpr int ND = kStagePlanesD(kFrame);
-      const double* dsrc[ND];
-#pragma unroll
-      for (int p = 0; p < FP; ++p) dsrc[p] = a.F + p * S;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        dsrc[FP + k] = a.G[nw] + k * S;
-        dsrc[FP + 3 + k] = a.r + k * S;
-        dsrc[FP + 6 + k] = a.G[cur] + k * S;
-        dsrc[FP + 9 + k] = a.NG[cur] + k * S;
-      }
-      const int nd_copy = restart ? FP + 6 : ND;
-      const unsigned bytes = (unsigned)nd_copy * 32u * 8u + 2u * 32u * 4u;
       const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      const int my_tiles =
-          (blockIdx.x < (unsigned)a.nt) ? (a.nt - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-      const int nsub = kItemsPerThread * my_tiles;
-      // first contact of this warp's chunk of sub-tile i
-      auto chunk_c0 = [&](int i) {
-        return ((int)blockIdx.x + (i / kItemsPerThread) * (int)gridDim.x) * kTileItems +
-               (i % kItemsPerThread) * kSub + warp * 32;
+      // this CTA's next iterating tile at or after sequence index i (-1: none)
+      auto next_tile = [&](int i, int* tile_out) {
+        for (;; ++i) {
+          int t = cta_tile(a, NT, i);
+          if (t < 0) return -1;
+          locate(a, sc, t);
+          if (!mask_done(a, s_mask, mwords, sc.s)) {
+            *tile_out = t;
+            return i;
+          }
+        }
       };
-      auto issue = [&](int i, int sidx) {
-        int cw = chunk_c0(i);
-        if (lane == 0 && cw < a.nc) {
+      // bulk copies of (tile t of segment s, sub-tile sub) for this warp into stage sidx
+      auto issue = [&](int t, int st0, int sc0, int snc, int sub, int sidx, int cur, int nw,
+                       int restart) {
+        const int kw = (t - st0) * kTileItems + sub * kSub + warp * 32;
+        if (lane == 0 && kw < snc) {
+          const int cw = sc0 + kw;
+          const T* nrm = normal_planes<T>(a);
+          const T* src[kStagePlanes];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            src[k] = nrm + k * S;
+            src[3 + k] = a.G[nw] + k * S;
+            src[6 + k] = a.r + k * S;
+            src[9 + k] = a.G[cur] + k * S;
+            src[12 + k] = a.NG[cur] + k * S;
+          }
+          const int nd = restart ? 9 : kStagePlanes;
+          const unsigned pbytes = 32u * (unsigned)sizeof(T);
           unsigned char* dst = stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes;
           uint64_t* bar = stg.bar + 2 * warp + sidx;
           // order this warp's earlier generic reads of the stage before the copies
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          mbar_arrive_expect_tx(bar, bytes);
-          for (int p = 0; p < nd_copy; ++p) bulk_g2s(dst + (size_t)p * 256, dsrc[p] + cw, 256, bar);
-          bulk_g2s(dst + (size_t)ND * 256, a.ida + cw, 128, bar);
-          bulk_g2s(dst + (size_t)ND * 256 + 128, a.idb + cw, 128, bar);
+          mbar_arrive_expect_tx(bar, (unsigned)nd * pbytes + 256u);
+          for (int p = 0; p < nd; ++p) bulk_g2s(dst + (size_t)p * pbytes, src[p] + cw, pbytes, bar);
+          unsigned char* ids = dst + (size_t)kStagePlanes * pbytes;
+          bulk_g2s(ids, a.ida + cw, 128, bar);
+          bulk_g2s(ids + 128, a.idb + cw, 128, bar);
         }
       };
+      auto load_ps = [&](int s) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          const ApgdCtl* C = &a.sst[s].ctl;
+          const int cur = __ldcg(&C->cur), prev = __ldcg(&C->prev), nw = __ldcg(&C->nw);
+          const int best = __ldcg(&C->best);
+          const double beta = __ldcg(&C->beta), gd = __ldcg(&C->gdiff);
+          s_ps.cur = cur;
+          s_ps.nw = nw;
+          s_ps.nw2 = free_slot(nw, cur, prev, best);
+          s_ps.restart = __ldcg(&C->restart);
+          s_ps.ya = 1.0 + beta;
+          s_ps.ym = -beta;
+          s_ps.nt2 = -(1.0 / (0.9 * __ldcg(&C->L)));
+          s_ps.gd = gd;
+          s_ps.gA = __ldcg(&C->ginv);
+          s_ps.gB = -1.0 / gd;
+          s_ps.mu = a.seg[s].mu;
+        }
+        __syncthreads();
+      };
+      SegRun run;
+      auto ctl = [&](int s) { ctl_product(ca, s, scratch); };
+
       double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       double mx = 0.0;
       bool bad = false, failed = false;
-      if (nsub > 0) issue(0, 0);
-      for (int i = 0; i < nsub; ++i) {
-        const int sidx = i & 1;
-        __syncwarp();  // the warp's reads of stage sidx^1 (sub-tile i-1) are done
-        if (i + 1 < nsub) issue(i + 1, sidx ^ 1);
-        const int cw = chunk_c0(i);
-        if (cw < a.nc && !failed) {
+      int tcur = -1;
+      int seq = next_tile(0, &tcur);
+      int sub = 0, sidx = 0;
+      const ProdScalars& ps = s_ps;
+      int s = -1, sc0 = 0, st0 = 0, snc = 0;
+      if (seq >= 0) {
+        locate(a, sc, tcur);
+        s = sc.s;
+        load_ps(s);
+        sc0 = sc.c0; st0 = sc.t0; snc = sc.nc;
+        issue(tcur, st0, sc0, snc, 0, 0, ps.cur, ps.nw, ps.restart);
+      }
+      while (seq >= 0) {
+        const int ti = tcur;
+        if (sub == 0 && s != run.s) {
+          flush_run(a, run, ctl);
+          run.s = s;
+        }
+        // the following sub-tile: this tile's second half, or the next tile
+        // (next_tile leaves that tile's segment in sc)
+        int nseq = seq, ntile = tcur, nsub = sub + 1;
+        if (nsub == kItemsPerThread) {
+          nsub = 0;
+          nseq = next_tile(seq + 1, &ntile);
+        }
+        const int ns = (nseq >= 0 && nsub == 0) ? sc.s : s;
+        __syncwarp();  // the warp's reads of stage sidx^1 are done
+        if (nseq >= 0) {
+          if (ns == s) {
+            issue(ntile, st0, sc0, snc, nsub, sidx ^ 1, ps.cur, ps.nw, ps.restart);
+          } else {
+            const ApgdCtl* C = &a.sst[ns].ctl;
+            issue(ntile, sc.t0, sc.c0, sc.nc, nsub, sidx ^ 1, __ldcg(&C->cur), __ldcg(&C->nw),
+                  __ldcg(&C->restart));
+          }
+        }
+        const int kw = (ti - st0) * kTileItems + sub * kSub + warp * 32;
+        if (kw < snc && !failed) {
           if (!wait_warp_stage(a, stg, sidx)) failed = true;
         }
-        const int c = cw + lane;
-        if (c < a.nc && !failed) {
-          const double* sd =
-              reinterpret_cast<const double*>(stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes);
-          const uint32_t* su = reinterpret_cast<const uint32_t*>(sd + (size_t)ND * 32);
+        const int k = kw + lane;
+        if (k < snc && !failed) {
+          const int c = sc0 + k;
+          const T* sd =
+              reinterpret_cast<const T*>(stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes);
+          const uint32_t* su = reinterpret_cast<const uint32_t*>(sd + (size_t)kStagePlanes * 32);
           const int j = lane;
-          Frame f;
-          f.n0 = sd[0 * 32 + j]; f.n1 = sd[1 * 32 + j]; f.n2 = sd[2 * 32 + j];
-          if (kFrame == 0) {
-            f.u0 = sd[3 * 32 + j]; f.u1 = sd[4 * 32 + j]; f.u2 = sd[5 * 32 + j];
-            f.v0 = sd[6 * 32 + j]; f.v1 = sd[7 * 32 + j]; f.v2 = sd[8 * 32 + j];
-          }
-          complete_frame(f, kFrame);
-          double4 wa = a.w4[su[j]], wb = a.w4[su[32 + j]];
-          double N0, N1, N2;
-          ft_times(f, wa, wb, &N0, &N1, &N2);
+          Frame<T> f = make_frame<T>(sd[0 * 32 + j], sd[1 * 32 + j], sd[2 * 32 + j]);
+          V wa = wv[su[j]], wb = wv[su[32 + j]];
+          T N0, N1, N2;
+          ft_times<T, V>(f, wa, wb, &N0, &N1, &N2);
+          T* NGn = a.NG[ps.nw];
           NGn[0 * S + c] = N0; NGn[1 * S + c] = N1; NGn[2 * S + c] = N2;
-          double x0 = sd[(FP + 0) * 32 + j], x1 = sd[(FP + 1) * 32 + j], x2 = sd[(FP + 2) * 32 + j];
-          double r0 = sd[(FP + 3) * 32 + j], r1 = sd[(FP + 4) * 32 + j], r2 = sd[(FP + 5) * 32 + j];
+          T x0 = sd[3 * 32 + j], x1 = sd[4 * 32 + j], x2 = sd[5 * 32 + j];
+          T r0 = sd[6 * 32 + j], r1 = sd[7 * 32 + j], r2 = sd[8 * 32 + j];
           acc[0] = acc[0] + dot3i(x0, x1, x2, N0, N1, N2);
           acc[1] = acc[1] + dot3i(x0, x1, x2, r0, r1, r2);
           {
-            double T0 = r0 + N0, T1 = r1 + N1, T2 = r2 + N2;
-            T0 = x0 + (-gd) * T0; T1 = x1 + (-gd) * T1; T2 = x2 + (-gd) * T2;
-            project_cone<double>(T0, T1, T2, a.mu);
-            T0 = gA * x0 + gB * T0; T1 = gA * x1 + gB * T1; T2 = gA * x2 + gB * T2;
+            // residual, FP64 in both paths (gd = 1/nc^2 is far below float
+            // resolution).  The mixed path takes it at the FP64 projection of
+            // the FP32 iterate: the residual divides by gd, which would
+            // otherwise magnify the iterate's float rounding off the cone.
+            double X0 = x0, X1 = x1, X2 = x2;
+            if (sizeof(T) != sizeof(double)) project_cone<double>(X0, X1, X2, ps.mu);
+            double T0 = (double)r0 + (double)N0, T1 = (double)r1 + (double)N1,
+                   T2 = (double)r2 + (double)N2;
+            T0 = X0 + (-ps.gd) * T0; T1 = X1 + (-ps.gd) * T1; T2 = X2 + (-ps.gd) * T2;
+            project_cone<double>(T0, T1, T2, ps.mu);
+            const double gA = ps.gA, gB = ps.gB;
+            T0 = gA * X0 + gB * T0; T1 = gA * X1 + gB * T1; T2 = gA * X2 + gB * T2;
             double m0 = fabs(T0), m1 = fabs(T1), m2 = fabs(T2);
             bad |= (m0 != m0) || (m1 != m1) || (m2 != m2);
             mx = fmax(mx, fmax(m0, fmax(m1, m2)));
           }
           // look-ahead step of iteration k+1: y = (1+b) x - b gamma_k, or x after a restart
-          double y0, y1, y2, M0, M1, M2;
-          if (restart) {
+          const T ya = (T)ps.ya, ym = (T)ps.ym;
+          const T nt2 = (T)ps.nt2;
+          T y0, y1, y2, M0, M1, M2;
+          if (ps.restart) {
             y0 = x0; y1 = x1; y2 = x2;
             M0 = N0; M1 = N1; M2 = N2;
           } else {
-            double c0v = sd[(FP + 6) * 32 + j], c1v = sd[(FP + 7) * 32 + j], c2v = sd[(FP + 8) * 32 + j];
+            T c0v = sd[9 * 32 + j], c1v = sd[10 * 32 + j], c2v = sd[11 * 32 + j];
             y0 = ya * x0 + ym * c0v; y1 = ya * x1 + ym * c1v; y2 = ya * x2 + ym * c2v;
-            M0 = ya * N0 + ym * sd[(FP + 9) * 32 + j];
-            M1 = ya * N1 + ym * sd[(FP + 10) * 32 + j];
-            M2 = ya * N2 + ym * sd[(FP + 11) * 32 + j];
+            M0 = ya * N0 + ym * sd[12 * 32 + j];
+            M1 = ya * N1 + ym * sd[13 * 32 + j];
+            M2 = ya * N2 + ym * sd[14 * 32 + j];
           }
-          double g0 = M0 + r0, g1 = M1 + r1, g2 = M2 + r2;
-          double z0 = y0 + nt2 * g0, z1 = y1 + nt2 * g1, z2 = y2 + nt2 * g2;
-          project_cone<double>(z0, z1, z2, a.mu);
+          T g0 = M0 + r0, g1 = M1 + r1, g2 = M2 + r2;
+          T z0 = y0 + nt2 * g0, z1 = y1 + nt2 * g1, z2 = y2 + nt2 * g2;
+          project_cone<T>(z0, z1, z2, (T)ps.mu);
+          T* G2 = a.G[ps.nw2];
           G2[0 * S + c] = z0; G2[1 * S + c] = z1; G2[2 * S + c] = z2;
-          a.q[c] = f_times(f, z0, z1, z2);
-          double t0 = z0 + (-1.0) * y0, t1 = z1 + (-1.0) * y1, t2 = z2 + (-1.0) * y2;
-          double s0 = z0 + (-1.0) * x0, s1 = z1 + (-1.0) * x1, s2 = z2 + (-1.0) * x2;
+          qv[c] = f_times<T, V>(f, z0, z1, z2);
+          T t0 = z0 + T(-1) * y0, t1 = z1 + T(-1) * y1, t2 = z2 + T(-1) * y2;
+          T s0 = z0 + T(-1) * x0, s1 = z1 + T(-1) * x1, s2 = z2 + T(-1) * x2;
           acc[2] = acc[2] + dot3i(g0, g1, g2, t0, t1, t2);
           acc[3] = acc[3] + dot3i(t0, t1, t2, t0, t1, t2);
           acc[4] = acc[4] + dot3i(g0, g1, g2, s0, s1, s2);
           acc[5] = acc[5] + dot3i(y0, y1, y2, M0, M1, M2);
           acc[6] = acc[6] + dot3i(y0, y1, y2, r0, r1, r2);
         }
-        if ((i % kItemsPerThread) == kItemsPerThread - 1) {
-          const int tile = (int)blockIdx.x + (i / kItemsPerThread) * (int)gridDim.x;
+        if (sub == kItemsPerThread - 1) {
           if (__syncthreads_or(failed)) return;
-          if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&a.bar[2], kErrNaN);
+          if (__syncthreads_or(bad) && threadIdx.x == 0) seg_error(a, s, kErrNaN);
           block_fold_multi<7>(acc, scratch);
-          write_partials<7>(a, tile, acc);
+          write_partials<7>(a, ti, acc);
           double bm = block_max256(mx, scratch);
-          if (threadIdx.x == 0) a.part[(size_t)kQMax * a.ptiles + tile] = bm;
+          if (threadIdx.x == 0) a.part[(size_t)kQMax * a.tcap + ti] = bm;
           for (int qq = 0; qq < 7; ++qq) acc[qq] = 0.0;
           mx = 0.0;
           bad = false;
+          ++run.n;
+        }
+        seq = nseq;
+        tcur = ntile;
+        sub = nsub;
+        sidx ^= 1;
+        if (ns != s) {
+          s = ns;
+          load_ps(s);
+          sc0 = sc.c0; st0 = sc.t0; snc = sc.nc;
         }
       }
+      flush_run(a, run, ctl);
     }
-    if (!grid_sync(a, kPhaseProduct, [&]() {
-          double s[7];
-          fold_tiles<7>(a, s, scratch);
-          double res = fold_tiles_max(a, scratch);
-          if (threadIdx.x == 0) {
-            ApgdCtl* C = a.ctl;
-            double obj1 = 0.5 * s[0] + s[1];
-            C->obj1 = obj1;
-            if (obj1 >= C->obj2) {
-              // (10)-(14): double L and retry the projection
-              if (C->backtracks >= a.max_bt) {
-                atomicOr(&a.bar[2], kErrBacktrackCap);
-                C->done = 1;
-                C->iterations = C->k;
-              } else {
-                C->backtracks += 1;
-                C->L = 2.0 * C->L;
-                C->t = 1.0 / C->L;
-                C->mode = 1;
-              }
-            } else {
-              C->mode = 0;
-              C->sweeps += 1;
-              int old_best = C->best;
-              if (res < C->residual) {
-                C->residual = res;
-                C->objective = obj1;
-                C->best = C->nw;
-              }
-              if (C->residual < a.tol) {
-                C->done = 1;
-                C->iterations = C->k;
-              } else {
-                double th = C->restart ? 1.0 : C->theta_new;
-                C->yb = C->beta;
-                C->yr = C->restart;
-                C->L = 0.9 * C->L;
-                C->t = 1.0 / C->L;
-                C->theta = th;
-                int nw2 = free_slot(C->nw, C->cur, C->prev, old_best);
-                C->prev = C->cur;
-                C->cur = C->nw;
-                C->nw = nw2;
-                C->k += 1;
-                if (C->k >= a.max_iter) {
-                  C->done = 1;
-                  C->iterations = C->k;
-                } else {
-                  C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
-                  C->beta = th * (1.0 - th) / (th * th + C->theta_new);
-                  // the look-ahead step is now iteration k's step
-                  C->obj2_base = 0.5 * s[5] + s[6];
-                  double nr = sqrt(s[3]);
-                  C->obj2 = C->obj2_base + (s[2] + 0.5 * C->L * (nr * nr));
-                  C->restart = (s[4] > 0) ? 1 : 0;
-                }
-              }
-            }
-          }
-        }))
-      return;
-    if (__ldcg(&a.ctl->done)) break;
-    step_pass = (__ldcg(&a.ctl->mode) == 1);
+    if (!grid_sync(a, kPhaseProduct, latch)) return;
   }
 
-  // ---- gamma = gamma_hat (APGD.cu:358); q = F gamma for D^T gamma
+  // ---- gamma = gamma_hat (APGD.cu:358) into the warm-start region; q = F gamma (FP64)
   {
-    const int best = __ldcg(&a.ctl->best);
-    const double* src = best >= 0 ? a.G[best] : nullptr;
-    for (int tile = blockIdx.x; tile < a.nt; tile += gridDim.x) {
+    int cs = -1;
+    const T* src = nullptr;
+    for (int i = 0;; ++i) {
+      const int t = cta_tile(a, NT, i);
+      if (t < 0) break;
+      locate(a, sc, t);
+      const int s = sc.s;
+      if (s != cs) {
+        cs = s;
+        const int best = __ldcg(&a.sst[s].ctl.best);
+        src = best >= 0 ? a.G[best] : nullptr;
+      }
+      const SegParams& P = a.seg[s];
+      const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
       for (int m = 0; m < kItemsPerThread; ++m) {
-        int c = tile * kTileItems + m * kThreads + threadIdx.x;
-        if (c < a.nc) {
+        int k = k0 + m * kThreads + threadIdx.x;
+        if (k < nc) {
+          const int c = c0 + k;
           double x0 = 1.0, x1 = 1.0, x2 = 1.0;
           if (src) {
-            x0 = src[0 * S + c]; x1 = src[1 * S + c]; x2 = src[2 * S + c];
+            x0 = (double)src[0 * S + c]; x1 = (double)src[1 * S + c]; x2 = (double)src[2 * S + c];
           }
-          a.gamma[0 * a.GS + c] = x0;
-          a.gamma[1 * a.GS + c] = x1;
-          a.gamma[2 * a.GS + c] = x2;
-          Frame f = load_frame<kFrame>(a, c);
-          a.q[c] = f_times(f, x0, x1, x2);
+          const size_t wi = (size_t)P.wbase + k;
+          a.gamma[0 * a.WS + wi] = x0;
+          a.gamma[1 * a.WS + wi] = x1;
+          a.gamma[2 * a.WS + wi] = x2;
+          Frame<double> f = load_frame_fp64(a, c);
+          a.qd[c] = f_times<double, double4>(f, x0, x1, x2);
         }
       }
     }
   }
-  if (!grid_sync(a, kPhaseFinal, NoCtl{})) return;
+  if (!grid_sync(a, kPhaseFinal, [&]() {
+        if (threadIdx.x == 0) atomicAdd(&a.ew->steps_done, 1);
+      }))
+    return;
 
-  // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v
-  const double invh = 1.0 / h;
-  for (int bt = blockIdx.x; bt < a.nbt; bt += gridDim.x) {
+  // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v.
+  // Segments without contacts: v = Minv k, f_contact = 0 (System.cu:577-581).
+  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
     if (b < a.nb) {
-      double4 fc = gather_q(a, b);
-      double4 k = a.k4[b];
-      double mi = __ldg(a.minv + b);
-      double4 v = make_double4(mi * (k.x + fc.x), mi * (k.y + fc.y), mi * (k.z + fc.z), 0.0);
-      a.v4[b] = v;
-      a.fc4[b] = make_double4(invh * fc.x, invh * fc.y, invh * fc.z, 0.0);
-      double4 p = a.p4[b];
-      a.p4[b] = make_double4(h * v.x + p.x, h * v.y + p.y, h * v.z + p.z, 0.0);
+      const int s = __ldg(a.bseg + b);
+      const SegParams& P = a.seg[s];
+      if (P.active) {
+        const double h = P.h;
+        const int nc = a.sst[s].nc;
+        double4 k = a.k4[b];
+        double mi = __ldg(a.minv + b);
+        double4 v, fcv;
+        if (nc > 0) {
+          double4 fc = gather_q<double, double4>(a, a.qd, b);
+          v = make_double4(mi * (k.x + fc.x), mi * (k.y + fc.y), mi * (k.z + fc.z), 0.0);
+          const double invh = 1.0 / h;
+          fcv = make_double4(invh * fc.x, invh * fc.y, invh * fc.z, 0.0);
+        } else {
+          v = make_double4(mi * k.x, mi * k.y, mi * k.z, 0.0);
+          fcv = make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+        a.v4[b] = v;
+        a.fc4[b] = fcv;
+        double4 p = a.p4[b];
+        a.p4[b] = make_double4(h * v.x + p.x, h * v.y + p.y, h * v.z + p.z, 0.0);
+      }
     }
   }
-}
-
-// System.cu:577-581: no contacts: v = Minv k, f_contact = 0, p += h v.
-__global__ void __launch_bounds__(kThreads) k_step_nocontact(int nb, double h,
-                                                             const double* __restrict__ minv,
-                                                             const double4* __restrict__ f4,
-                                                             double4* k4, double4* v4, double4* p4,
-                                                             double4* fc4) {
-  int b = blockIdx.x * kThreads + threadIdx.x;
-  if (b >= nb) return;
-  double mi = minv[b];
-  double m = mi;
-  if (m) m = 1.0 / m;
-  double4 v = v4[b], f = f4[b];
-  double4 k = make_double4(h * f.x + m * v.x, h * f.y + m * v.y, h * f.z + m * v.z, 0.0);
-  k4[b] = k;
-  v = make_double4(mi * k.x, mi * k.y, mi * k.z, 0.0);
-  v4[b] = v;
-  fc4[b] = make_double4(0.0, 0.0, 0.0, 0.0);
-  double4 p = p4[b];
-  p4[b] = make_double4(h * v.x + p.x, h * v.y + p.y, h * v.z + p.z, 0.0);
-}
-
-// Frame mode and register budget of the solve kernel; DVIDE_FRAME_MODE=0
-// (frames loaded) and DVIDE_MIN_BLOCKS=3 select the other variants for timing
-// comparisons.
-int frame_mode_selected() {
-  static int sel = -1;
-  if (sel < 0) {
-    const char* e = getenv("DVIDE_FRAME_MODE");
-    sel = (e && e[0] == '0') ? 0 : 1;
+  // warm-start length of every segment that solved (System::gamma_d resize)
+  for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.nseg; s += gridDim.x * kThreads) {
+    SegState& X = a.sst[s];
+    if (a.seg[s].active && X.nc > 0) X.gsize = X.nc;
   }
-  return sel;
 }
 
-// CTAs per SM the register budget is set for (2: 128 registers; 3: 80);
-// DVIDE_MIN_BLOCKS=3 selects the second for timing comparisons.
-int min_blocks_selected() {
-  static int sel = -1;
-  if (sel < 0) {
-    const char* e = getenv("DVIDE_MIN_BLOCKS");
-    sel = (e && e[0] == '3') ? 3 : 2;
-  }
-  return sel;
-}
-
-const void* solve_kernel() {
-  int fm = frame_mode_selected();
-  if (min_blocks_selected() == 3)
-    return fm == 0 ? (const void*)k_step_solve<0, 3> : (const void*)k_step_solve<1, 3>;
-  return fm == 0 ? (const void*)k_step_solve<0, 2> : (const void*)k_step_solve<1, 2>;
-}
-
-size_t solve_smem() { return kDynSmem(frame_mode_selected()); }
-
-void prepare_solve_kernel() {
+template <class T>
+void prepare_kernel() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(solve_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)solve_smem());
+  cudaFuncSetAttribute(k_step_solve<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)dyn_smem_bytes<T>());
   done = true;
+}
+
+template <class T>
+KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
+  KArgs<T> a;
+  a.nb = sd.nb;
+  a.nseg = sd.nseg;
+  a.tcap = sd.tcap;
+  a.chunk = cfg.chunk > 0 ? cfg.chunk : 1;
+  a.contiguous = cfg.contiguous;
+  a.S = sd.ccap;
+  a.WS = sd.wtotal;
+  a.p4 = sd.p4;
+  a.v4 = sd.v4;
+  a.k4 = sd.k4;
+  a.f4 = sd.f4;
+  a.fc4 = sd.fc4;
+  a.wd = sd.w4;
+  a.minv = sd.minv;
+  a.bseg = sd.bseg;
+  a.ida = sd.ida;
+  a.idb = sd.idb;
+  a.F = sd.F;
+  a.nf = sd.nf;
+  a.gap = sd.gap;
+  a.r = reinterpret_cast<T*>(sd.r);
+  a.inc_start = sd.inc_start;
+  a.inc = sd.inc;
+  for (int k = 0; k < 5; ++k) {
+    a.G[k] = reinterpret_cast<T*>(sd.G[k]);
+    a.NG[k] = reinterpret_cast<T*>(sd.NG[k]);
+  }
+  a.qd = sd.q;
+  a.gamma = sd.gamma;
+  a.part = sd.part;
+  a.seg = sd.seg;
+  a.sst = sd.sst;
+  a.tseg = sd.tseg;
+  a.donemask = sd.donemask;
+  a.ew = sd.ew;
+  return a;
+}
+
+template <class T>
+void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
+  prepare_kernel<T>();
+  KArgs<T> a = make_kargs<T>(sd, cfg);
+  void* params[] = {&a};
+  cudaLaunchCooperativeKernel((const void*)k_step_solve<T, 2>, cfg.grid, kThreads, params,
+                              dyn_smem_bytes<T>(), st);
 }
 
 }  // namespace
 
 int apgd_max_ctas(int precision) {
-  (void)precision;
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  prepare_solve_kernel();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_kernel(), kThreads, solve_smem());
+  if (precision == DV_PREC_MIXED) {
+    prepare_kernel<float>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<float, 2>, kThreads,
+                                                  dyn_smem_bytes<float>());
+  } else {
+    prepare_kernel<double>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<double, 2>, kThreads,
+                                                  dyn_smem_bytes<double>());
+  }
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
 
 void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches) {
-  KArgs a;
-  a.nb = sd.nb;
-  a.nc = sd.nc;
-  a.nt = (sd.nc + kTileItems - 1) / kTileItems;
-  a.nbt = (sd.nb + kThreads - 1) / kThreads;
-  a.S = sd.ccap;
-  a.GS = sd.gcap;
-  a.p4 = sd.p4;
-  a.v4 = sd.v4;
-  a.k4 = sd.k4;
-  a.f4 = sd.f4;
-  a.w4 = sd.w4;
-  a.fc4 = sd.fc4;
-  a.minv = sd.minv;
-  a.ida = sd.ida;
-  a.idb = sd.idb;
-  a.F = sd.F;
-  a.gap = sd.gap;
-  a.r = sd.r;
-  a.inc_start = sd.inc_start;
-  a.inc = sd.inc;
-  for (int k = 0; k < 5; ++k) {
-    a.G[k] = sd.G[k];
-    a.NG[k] = sd.NG[k];
-  }
-  a.q = sd.q;
-  a.gamma = sd.gamma;
-  a.part = sd.part;
-  a.ptiles = sd.part_tiles;
-  a.ctl = sd.ctl;
-  a.bar = sd.bar;
-  a.h = cfg.h;
-  a.mu = cfg.mu;
-  a.tol = cfg.tol;
-  a.max_iter = cfg.max_iter;
-  a.max_bt = cfg.max_bt;
-  a.warm = cfg.warm;
-  int grid = cfg.grid;
-  cudaMemsetAsync(sd.bar, 0, 4 * sizeof(unsigned), st);
-  cudaMemsetAsync(sd.ctl, 0, sizeof(ApgdCtl), st);
-  void* params[] = {&a};
-  prepare_solve_kernel();
-  cudaLaunchCooperativeKernel(solve_kernel(), dim3(grid), dim3(kThreads), params, solve_smem(), st);
-  ++*launches;
-  cudaMemcpyAsync(sd.h_ctl, sd.ctl, sizeof(ApgdCtl), cudaMemcpyDeviceToHost, st);
-}
-
-void launch_step_nocontact(SceneDev& sd, double h, cudaStream_t st, int64_t* launches) {
-  int nb = sd.nb;
-  k_step_nocontact<<<(nb + kThreads - 1) / kThreads, kThreads, 0, st>>>(nb, h, sd.minv, sd.f4,
-                                                                        sd.k4, sd.v4, sd.p4, sd.fc4);
+  cudaMemsetAsync(sd.ew->bar, 0, sizeof(sd.ew->bar), st);
+  cudaMemsetAsync(&sd.ew->last_release, 0, sizeof(unsigned long long), st);
+  if (sd.precision == DV_PREC_MIXED) launch_typed<float>(sd, cfg, st);
+  else launch_typed<double>(sd, cfg, st);
   ++*launches;
 }
 

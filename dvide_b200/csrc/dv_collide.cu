@@ -1,23 +1,33 @@
-// dv_collide.cu -- collision detection for spheres and boxes.
+// dv_collide.cu -- collision detection for spheres and boxes, for every
+// segment (scene) of an engine at once.
 //
 // Replaces CollisionDetector::generateAxisAlignedBoundingBoxes,
 // detectPossibleCollisions_spatialSubdivision and detectCollisions
 // (CollisionDetector.cu:24-501, 547-665) for rigid bodies.
 //
 // Candidate pairs are exactly the reference's: AABBs (extent + envelope)
-// shifted by the global origin (AABB union min - 0.01), inclusive overlap on
-// all three axes, same-family pairs (family != -1) excluded.  That set does not
-// depend on the binning, so the reference's 20^3 global bins are replaced by:
-//   * spheres in a uniform grid whose cell is wider than any sphere AABB,
-//     keyed on the shifted AABB min corner; (cell, body) keys are radix
-//     sorted; one warp per sphere scans the 27 neighbour cells (one lane per
-//     cell) and lanes 27..31 scan the box list;
-//   * boxes tested against every body by a block-parallel compaction.
-// Each body's partners with larger id are sorted, so contacts come out in
-// lexicographic (A, B) order, the order of the reference's sorted unique
+// shifted by the segment's origin (AABB union min - 0.01), inclusive overlap
+// on all three axes, same-family pairs (family != -1) excluded.  That set does
+// not depend on the binning, so the reference's 20^3 global bins are replaced
+// by:
+//   * spheres in a uniform grid per segment whose cell is wider than any
+//     sphere AABB of the segment, keyed on the shifted AABB min corner; the
+//     segments' cells are numbered consecutively and (cell, body) keys of all
+//     segments are radix sorted together; one warp per sphere scans the 27
+//     neighbour cells (one lane per cell) and lanes 27..31 scan the
+//     segment's box list;
+//   * boxes tested against every body of their segment by a block-parallel
+//     compaction.
+// Each body's partners with larger id are sorted, so a segment's contacts come
+// out in lexicographic (A, B) order, the order of the reference's sorted unique
 // 64-bit pair keys (CollisionDetector.cu:319-325).  The narrowphase
 // (sphere-sphere, sphere-box; box-box is never a contact) also emits the
 // tangent frame of System.cu:753-762, so no separate Jacobian is built.
+//
+// Sizes that change every step (contacts, tiles) are read on the device, so
+// the whole pipeline runs without a host round trip and can be captured in a
+// CUDA graph.  EngineWords::err is sticky: once set, every later kernel of the
+// step returns at once.
 #include <stdio.h>
 
 #include <algorithm>
@@ -48,58 +58,83 @@ __device__ inline void aabb_of(double4 p, double4 g, double env, double4* mn, do
   *mx = make_double4(p.x + ex, p.y + ey, p.z + ez, 0.0);
 }
 
-__global__ void k_bounds_init(GridInfo* g) {
+__global__ void k_seg_reset(int nseg, GridInfo* __restrict__ grid, SegState* __restrict__ sst,
+                            EngineWords* __restrict__ ew) {
+  if (ew->err) return;
+  int s = blockIdx.x * kThreads + threadIdx.x;
+  if (s == 0) ew->npossible = 0;
+  if (s >= nseg) return;
   for (int d = 0; d < 3; ++d) {
-    g->lo[d] = ~0ull;
-    g->hi[d] = 0ull;
+    grid[s].lo[d] = ~0ull;
+    grid[s].hi[d] = 0ull;
   }
+  sst[s].nc = 0;
+  sst[s].npossible = 0;
 }
 
-// CollisionDetector.cu:24-79 (rigid-body branch): aabb = pos -+ (extent + envelope).
+// CollisionDetector.cu:24-79 (rigid-body branch): aabb = pos -+ (extent +
+// envelope); per-segment AABB union by warp folds when the warp's bodies share
+// a segment, per-body atomics otherwise.
 __global__ void __launch_bounds__(kThreads) k_aabb(const double4* __restrict__ p4,
-                                                  const double4* __restrict__ g4, int nb,
-                                                  double env, double4* __restrict__ amin,
-                                                  double4* __restrict__ amax, GridInfo* grid) {
-  __shared__ unsigned long long s_lo[3][kWarpsPerCta], s_hi[3][kWarpsPerCta];
-  int i = blockIdx.x * kThreads + threadIdx.x;
+                                                  const double4* __restrict__ g4,
+                                                  const int* __restrict__ bseg,
+                                                  const SegParams* __restrict__ seg, int nb,
+                                                  double4* __restrict__ amin,
+                                                  double4* __restrict__ amax,
+                                                  GridInfo* __restrict__ grid,
+                                                  const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int s = -1;
   unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
   if (i < nb) {
-    double4 mn, mx;
-    aabb_of(p4[i], g4[i], env, &mn, &mx);
-    amin[i] = mn;
-    amax[i] = mx;
-    lo[0] = ordered_bits(mn.x); lo[1] = ordered_bits(mn.y); lo[2] = ordered_bits(mn.z);
-    hi[0] = ordered_bits(mx.x); hi[1] = ordered_bits(mx.y); hi[2] = ordered_bits(mx.z);
-  }
-  for (int d = 0; d < 3; ++d) {
-    unsigned long long a = lo[d], b = hi[d];
-    for (int off = 16; off >= 1; off >>= 1) {
-      unsigned long long oa = __shfl_down_sync(0xffffffffu, a, off);
-      unsigned long long ob = __shfl_down_sync(0xffffffffu, b, off);
-      a = oa < a ? oa : a;
-      b = ob > b ? ob : b;
-    }
-    if ((threadIdx.x & 31) == 0) {
-      s_lo[d][threadIdx.x >> 5] = a;
-      s_hi[d][threadIdx.x >> 5] = b;
+    s = bseg[i];
+    if (seg[s].active) {
+      double4 mn, mx;
+      aabb_of(p4[i], g4[i], seg[s].env, &mn, &mx);
+      amin[i] = mn;
+      amax[i] = mx;
+      lo[0] = ordered_bits(mn.x); lo[1] = ordered_bits(mn.y); lo[2] = ordered_bits(mn.z);
+      hi[0] = ordered_bits(mx.x); hi[1] = ordered_bits(mx.y); hi[2] = ordered_bits(mx.z);
+    } else {
+      s = -1;
     }
   }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    int d = threadIdx.x;
-    unsigned long long a = s_lo[d][0], b = s_hi[d][0];
-    for (int w = 1; w < kWarpsPerCta; ++w) {
-      a = s_lo[d][w] < a ? s_lo[d][w] : a;
-      b = s_hi[d][w] > b ? s_hi[d][w] : b;
+  const int s0 = __shfl_sync(0xffffffffu, s, 0);
+  const bool uniform = __all_sync(0xffffffffu, s == s0);
+  if (uniform) {
+    if (s0 < 0) return;
+    for (int d = 0; d < 3; ++d) {
+      unsigned long long a = lo[d], b = hi[d];
+      for (int off = 16; off >= 1; off >>= 1) {
+        unsigned long long oa = __shfl_down_sync(0xffffffffu, a, off);
+        unsigned long long ob = __shfl_down_sync(0xffffffffu, b, off);
+        a = oa < a ? oa : a;
+        b = ob > b ? ob : b;
+      }
+      if (lane == 0) {
+        atomicMin(&grid[s0].lo[d], a);
+        atomicMax(&grid[s0].hi[d], b);
+      }
     }
-    atomicMin(&grid->lo[d], a);
-    atomicMax(&grid->hi[d], b);
+  } else if (s >= 0) {
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&grid[s].lo[d], lo[d]);
+      atomicMax(&grid[s].hi[d], hi[d]);
+    }
   }
 }
 
 // CollisionDetector.cu:566-568: origin = union min - 0.01; grid sized for the
-// widest sphere AABB, capped at `cap` cells (a wider cell only adds candidates).
-__global__ void k_grid_setup(GridInfo* g, double W, int cap) {
+// widest sphere AABB of the segment, capped at its `cell_cap` cells (a wider
+// cell only adds candidates).
+__global__ void k_grid_setup(int nseg, const SegParams* __restrict__ seg,
+                             GridInfo* __restrict__ grid, const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
+  int s = blockIdx.x * kThreads + threadIdx.x;
+  if (s >= nseg || !seg[s].active) return;
+  GridInfo* g = grid + s;
   double lo[3], hi[3];
   for (int d = 0; d < 3; ++d) {
     lo[d] = from_ordered(g->lo[d]);
@@ -109,7 +144,8 @@ __global__ void k_grid_setup(GridInfo* g, double W, int cap) {
   g->oy = lo[1] - 0.01;
   g->oz = lo[2] - 0.01;
   double ext[3] = {hi[0] + 0.01 - g->ox, hi[1] + 0.01 - g->oy, hi[2] + 0.01 - g->oz};
-  double w = W * (1.0 + 1e-6) + 1e-300;
+  double w = seg[s].W * (1.0 + 1e-6) + 1e-300;
+  const int cap = seg[s].cell_cap;
   int dims[3];
   for (int it = 0; it < 64; ++it) {
     double total = 1.0;
@@ -137,38 +173,53 @@ __global__ void k_grid_setup(GridInfo* g, double W, int cap) {
 
 __device__ inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// CollisionDetector.cu:574: aabb -= origin.  Spheres also get their cell key.
+// CollisionDetector.cu:574: aabb -= origin.  Spheres also get their cell key;
+// spheres of inactive segments go to the parking cell `park`.
 __global__ void __launch_bounds__(kThreads) k_shift_and_bin(
-    int nb, const int* __restrict__ small_ids, int n_small, const double4* __restrict__ p4,
-    const double4* __restrict__ g4, double env, double4* __restrict__ amin,
-    double4* __restrict__ amax, const GridInfo* __restrict__ g, int4* __restrict__ cell,
-    uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    int nb, const int* __restrict__ small_ids, int n_small, const int* __restrict__ bseg,
+    const SegParams* __restrict__ seg, const double4* __restrict__ p4,
+    const double4* __restrict__ g4, double4* __restrict__ amin, double4* __restrict__ amax,
+    const GridInfo* __restrict__ grid, int4* __restrict__ cell, uint32_t* __restrict__ keys,
+    uint32_t* __restrict__ vals, int park, const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
   int i = blockIdx.x * kThreads + threadIdx.x;
-  double ox = g->ox, oy = g->oy, oz = g->oz;
   if (i < nb) {
-    double4 a = amin[i], b = amax[i];
-    amin[i] = make_double4(a.x - ox, a.y - oy, a.z - oz, 0.0);
-    amax[i] = make_double4(b.x - ox, b.y - oy, b.z - oz, 0.0);
+    int s = bseg[i];
+    if (seg[s].active) {
+      const GridInfo* g = grid + s;
+      double ox = g->ox, oy = g->oy, oz = g->oz;
+      double4 a = amin[i], b = amax[i];
+      amin[i] = make_double4(a.x - ox, a.y - oy, a.z - oz, 0.0);
+      amax[i] = make_double4(b.x - ox, b.y - oy, b.z - oz, 0.0);
+    }
   }
   if (i < n_small) {
     int body = small_ids[i];
-    double4 a, b;
-    aabb_of(p4[body], g4[body], env, &a, &b);
-    a = make_double4(a.x - ox, a.y - oy, a.z - oz, 0.0);
-    double iw = g->inv_w;
-    int cx = clampi((int)floor(a.x * iw), 0, g->dx - 1);
-    int cy = clampi((int)floor(a.y * iw), 0, g->dy - 1);
-    int cz = clampi((int)floor(a.z * iw), 0, g->dz - 1);
-    int id = cx + g->dx * (cy + g->dy * cz);
-    cell[body] = make_int4(cx, cy, cz, id);
-    keys[i] = (uint32_t)id;
+    int s = bseg[body];
+    uint32_t key = (uint32_t)park;
+    if (seg[s].active) {
+      const GridInfo* g = grid + s;
+      double4 a, b;
+      aabb_of(p4[body], g4[body], seg[s].env, &a, &b);
+      a = make_double4(a.x - g->ox, a.y - g->oy, a.z - g->oz, 0.0);
+      double iw = g->inv_w;
+      int cx = clampi((int)floor(a.x * iw), 0, g->dx - 1);
+      int cy = clampi((int)floor(a.y * iw), 0, g->dy - 1);
+      int cz = clampi((int)floor(a.z * iw), 0, g->dz - 1);
+      int id = seg[s].cell_base + cx + g->dx * (cy + g->dy * cz);
+      cell[body] = make_int4(cx, cy, cz, id);
+      key = (uint32_t)id;
+    }
+    keys[i] = key;
     vals[i] = (uint32_t)body;
   }
 }
 
 __global__ void __launch_bounds__(kThreads) k_cell_ranges(const uint32_t* __restrict__ keys,
                                                          int n, int* __restrict__ cstart,
-                                                         int* __restrict__ cend, int ncap) {
+                                                         int* __restrict__ cend, int ncap,
+                                                         const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
   int j = blockIdx.x * kThreads + threadIdx.x;
   if (j >= n) return;
   uint32_t k = keys[j];
@@ -246,10 +297,13 @@ __device__ inline bool narrowphase(const double4* __restrict__ p4, const double4
 }
 
 struct CollideArgs {
-  int nb, n_small, n_large;
+  int nb, n_small, n_large, max_seg_chunks;
   const double4* p4;
   const double4* g4;
   const int* fam;
+  const int* bseg;
+  const SegParams* seg;
+  SegState* sst;
   const double4* amin;
   const double4* amax;
   const int4* cell;
@@ -259,19 +313,18 @@ struct CollideArgs {
   const int* cstart;
   const int* cend;
   const GridInfo* grid;
-  double env;
   int* cnt_cont;
   int* cnt_cand;
-  int* counters;
   const int* cbase;
+  EngineWords* ew;
   // contact outputs
   size_t ccap;
   uint32_t* ida;
   uint32_t* idb;
   double* F;
+  float* nf;
   double* gap;
   double* loc;
-  unsigned* err;
 };
 
 __device__ inline void write_contact(const CollideArgs& a, size_t c, int ia, int ib,
@@ -284,6 +337,9 @@ __device__ inline void write_contact(const CollideArgs& a, size_t c, int ia, int
   a.F[0 * S + c] = o.n.x; a.F[1 * S + c] = o.n.y; a.F[2 * S + c] = o.n.z;
   a.F[3 * S + c] = u.x;   a.F[4 * S + c] = u.y;   a.F[5 * S + c] = u.z;
   a.F[6 * S + c] = v.x;   a.F[7 * S + c] = v.y;   a.F[8 * S + c] = v.z;
+  a.nf[0 * S + c] = (float)o.n.x;
+  a.nf[1 * S + c] = (float)o.n.y;
+  a.nf[2 * S + c] = (float)o.n.z;
   a.gap[c] = o.gap;
   a.loc[0 * S + c] = o.loc.x;
   a.loc[1 * S + c] = o.loc.y;
@@ -291,25 +347,30 @@ __device__ inline void write_contact(const CollideArgs& a, size_t c, int ia, int
 }
 
 // One warp per sphere A: partners B > A from the 27 neighbour cells (lane =
-// cell) and from the box list (lanes 27..31).  kWrite = false counts,
-// kWrite = true emits the sorted partner list at cbase[A].
+// cell) and from the segment's box list (lanes 27..31).  kWrite = false
+// counts, kWrite = true emits the sorted partner list at the body's slot.
 template <bool kWrite>
 __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
   __shared__ int s_buf[kWarpsPerCta][kMaxPerBody];
   __shared__ int s_cnt[kWarpsPerCta];
+  if (a.ew->err) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int j = blockIdx.x * kWarpsPerCta + warp;
   if (j >= a.n_small) return;
   const int A = a.small_ids[j];
+  const int sg = a.bseg[A];
+  const SegParams& P = a.seg[sg];
+  if (!P.active) return;
+  const double env = P.env;
   if (lane == 0) s_cnt[warp] = 0;
   __syncwarp();
   int ncand = 0, ncont = 0;
   if (lane < 27) {
     int4 cA = a.cell[A];
     int x = cA.x + (lane % 3) - 1, y = cA.y + ((lane / 3) % 3) - 1, z = cA.z + (lane / 9) - 1;
-    const GridInfo* g = a.grid;
+    const GridInfo* g = a.grid + sg;
     if (x >= 0 && y >= 0 && z >= 0 && x < g->dx && y < g->dy && z < g->dz) {
-      int id = x + g->dx * (y + g->dy * z);
+      int id = P.cell_base + x + g->dx * (y + g->dy * z);
       int s = a.cstart[id];
       if (s >= 0) {
         int e = a.cend[id];
@@ -319,7 +380,7 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
           if (!is_candidate(a.amin, a.amax, a.fam, A, B)) continue;
           ++ncand;
           NpOut o;
-          if (narrowphase(a.p4, a.g4, A, B, a.env, &o)) {
+          if (narrowphase(a.p4, a.g4, A, B, env, &o)) {
             ++ncont;
             if (kWrite) {
               int slot = atomicAdd(&s_cnt[warp], 1);
@@ -330,13 +391,13 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
       }
     }
   } else {
-    for (int m = lane - 27; m < a.n_large; m += 5) {
+    for (int m = P.l0 + lane - 27; m < P.l1; m += 5) {
       int B = a.large_ids[m];
       if (B <= A) continue;
       if (!is_candidate(a.amin, a.amax, a.fam, A, B)) continue;
       ++ncand;
       NpOut o;
-      if (narrowphase(a.p4, a.g4, A, B, a.env, &o)) {
+      if (narrowphase(a.p4, a.g4, A, B, env, &o)) {
         ++ncont;
         if (kWrite) {
           int slot = atomicAdd(&s_cnt[warp], 1);
@@ -353,8 +414,11 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
     if (lane == 0) {
       a.cnt_cand[A] = ncand;
       a.cnt_cont[A] = ncont;
-      if (ncont > kMaxPerBody) atomicOr(a.err, kErrCapacity);
-      if (ncand) atomicAdd(&a.counters[1], ncand);
+      if (ncont > kMaxPerBody) atomicOr(&a.ew->err, kErrPartners);
+      if (ncand) {
+        atomicAdd(&a.sst[sg].npossible, ncand);
+        atomicAdd(&a.ew->npossible, ncand);
+      }
     }
     return;
   }
@@ -376,34 +440,42 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
     for (int t = 0; t < kMaxPerBody / 32; ++t) rk[t] += (other < mine[t]) ? 1 : 0;
   }
   __syncwarp();
-  size_t base = (size_t)a.cbase[A];
+  size_t base = (size_t)(a.cbase[A] + a.sst[sg].delta);
 #pragma unroll
   for (int t = 0; t < kMaxPerBody / 32; ++t) {
     int e = lane + 32 * t;
     if (e < n) {
       NpOut o;
-      narrowphase(a.p4, a.g4, A, mine[t], a.env, &o);
+      narrowphase(a.p4, a.g4, A, mine[t], env, &o);
       write_contact(a, base + rk[t], A, mine[t], o);
     }
   }
 }
 
 // Boxes: body L = large_ids[blockIdx.y] against the 256 bodies of chunk
-// blockIdx.x, keeping B > L; ranks within the chunk by warp ballots.
+// blockIdx.x of its segment, keeping B > L; ranks within the chunk by warp
+// ballots.
 template <bool kWrite>
 __global__ void __launch_bounds__(kThreads) k_box_pairs(CollideArgs a, int* __restrict__ chunk_cnt,
-                                                        const int* __restrict__ chunk_off,
-                                                        int nchunks) {
+                                                        const int* __restrict__ chunk_off) {
   __shared__ int s_w[kWarpsPerCta];
+  if (a.ew->err) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int m = blockIdx.y;
   const int L = a.large_ids[m];
-  const int B = blockIdx.x * kThreads + threadIdx.x;
+  const int sg = a.bseg[L];
+  const SegParams& P = a.seg[sg];
+  const size_t crow = (size_t)m * a.max_seg_chunks;
+  if (!P.active || P.b0 + (int)blockIdx.x * kThreads >= P.b1) {
+    if (!kWrite && threadIdx.x == 0) chunk_cnt[crow + blockIdx.x] = 0;
+    return;
+  }
+  const int B = P.b0 + blockIdx.x * kThreads + threadIdx.x;
   bool cand = false, cont = false;
   NpOut o;
-  if (B < a.nb && B > L && is_candidate(a.amin, a.amax, a.fam, L, B)) {
+  if (B < P.b1 && B > L && is_candidate(a.amin, a.amax, a.fam, L, B)) {
     cand = true;
-    cont = narrowphase(a.p4, a.g4, L, B, a.env, &o);
+    cont = narrowphase(a.p4, a.g4, L, B, P.env, &o);
   }
   unsigned bal = __ballot_sync(0xffffffffu, cont);
   if (!kWrite) {
@@ -413,12 +485,13 @@ __global__ void __launch_bounds__(kThreads) k_box_pairs(CollideArgs a, int* __re
     if (threadIdx.x == 0) {
       int tot = 0;
       for (int w = 0; w < kWarpsPerCta; ++w) tot += s_w[w];
-      chunk_cnt[(size_t)m * nchunks + blockIdx.x] = tot;
+      chunk_cnt[crow + blockIdx.x] = tot;
       if (tot) atomicAdd(&a.cnt_cont[L], tot);
     }
     if (lane == 0 && balc) {
       atomicAdd(&a.cnt_cand[L], __popc(balc));
-      atomicAdd(&a.counters[1], __popc(balc));
+      atomicAdd(&a.sst[sg].npossible, __popc(balc));
+      atomicAdd(&a.ew->npossible, __popc(balc));
     }
     return;
   }
@@ -428,29 +501,135 @@ __global__ void __launch_bounds__(kThreads) k_box_pairs(CollideArgs a, int* __re
   int pre = 0;
   for (int w = 0; w < warp; ++w) pre += s_w[w];
   pre += __popc(bal & ((1u << lane) - 1u));
-  size_t pos = (size_t)a.cbase[L] + (size_t)(chunk_off[(size_t)m * nchunks + blockIdx.x] -
-                                             chunk_off[(size_t)m * nchunks]) + pre;
+  size_t pos = (size_t)(a.cbase[L] + a.sst[sg].delta) +
+               (size_t)(chunk_off[crow + blockIdx.x] - chunk_off[crow]) + pre;
   write_contact(a, pos, L, B, o);
 }
 
-__global__ void __launch_bounds__(kThreads) k_count_b(const uint32_t* __restrict__ idb, int nc,
+// Contact layout: segment s gets nc_s = contacts of its bodies, slots
+// [c0, c0 + nc_s) with c0 a multiple of kContactAlign, tiles [t0, t0 + nt).
+// One CTA scans the segments in order.
+__global__ void __launch_bounds__(1024) k_seg_layout(int nseg, int nb,
+                                                     const SegParams* __restrict__ seg,
+                                                     SegState* __restrict__ sst,
+                                                     const int* __restrict__ cbase,
+                                                     int* __restrict__ seg_tstart, size_t ccap,
+                                                     int tcap, EngineWords* __restrict__ ew) {
+  __shared__ long long s_c[32], s_t[32];
+  __shared__ long long s_carry_c, s_carry_t;
+  if (ew->err) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    s_carry_c = 0;
+    s_carry_t = 0;
+  }
+  __syncthreads();
+  for (int base = 0; base < nseg; base += 1024) {
+    int s = base + threadIdx.x;
+    long long nc = 0, pad = 0, nt = 0;
+    if (s < nseg && seg[s].active) {
+      nc = cbase[seg[s].b1] - cbase[seg[s].b0];
+      pad = (nc + kContactAlign - 1) / kContactAlign * kContactAlign;
+      nt = (nc + kTileItems - 1) / kTileItems;
+      if (nc > seg[s].wcap) atomicOr(&ew->err, kErrCapacity);  // warm-start region too small
+    }
+    long long xc = pad, xt = nt;
+    for (int off = 1; off < 32; off <<= 1) {
+      long long yc = __shfl_up_sync(0xffffffffu, xc, off);
+      long long yt = __shfl_up_sync(0xffffffffu, xt, off);
+      if (lane >= off) { xc += yc; xt += yt; }
+    }
+    if (lane == 31) { s_c[warp] = xc; s_t[warp] = xt; }
+    __syncthreads();
+    if (warp == 0) {
+      long long wc = s_c[lane], wt = s_t[lane];
+      for (int off = 1; off < 32; off <<= 1) {
+        long long yc = __shfl_up_sync(0xffffffffu, wc, off);
+        long long yt = __shfl_up_sync(0xffffffffu, wt, off);
+        if (lane >= off) { wc += yc; wt += yt; }
+      }
+      s_c[lane] = wc;
+      s_t[lane] = wt;
+    }
+    __syncthreads();
+    long long ec = s_carry_c + xc - pad + (warp ? s_c[warp - 1] : 0);
+    long long et = s_carry_t + xt - nt + (warp ? s_t[warp - 1] : 0);
+    if (s < nseg) {
+      SegState& S = sst[s];
+      S.nc = (int)nc;
+      S.c0 = (int)ec;
+      S.t0 = (int)et;
+      S.nt = (int)nt;
+      S.delta = (int)(ec - (seg[s].active ? cbase[seg[s].b0] : 0));
+      seg_tstart[s] = (int)et;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_carry_c += s_c[31];
+      s_carry_t += s_t[31];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    seg_tstart[nseg] = (int)s_carry_t;
+    ew->nc_total = cbase[nb];
+    ew->nc_pad = (int)s_carry_c;
+    ew->ntiles = (int)s_carry_t;
+    if (s_carry_c > (long long)ccap || s_carry_t > (long long)tcap) atomicOr(&ew->err, kErrCapacity);
+  }
+}
+
+// tile -> segment (binary search of the tile starts)
+__global__ void __launch_bounds__(kThreads) k_tile_table(int nseg, const int* __restrict__ seg_tstart,
+                                                        int* __restrict__ tseg, int tcap,
+                                                        const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
+  const int nt = ew->ntiles;
+  for (int t = blockIdx.x * kThreads + threadIdx.x; t < nt; t += gridDim.x * kThreads) {
+    int lo = 0, hi = nseg - 1;  // last segment with tstart <= t and tiles
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (seg_tstart[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    tseg[t] = lo;
+  }
+}
+
+// Contacts in (B, contact) key form for the B-side incidence; the radix input
+// index is the contact's unpadded position.
+__global__ void __launch_bounds__(kThreads) k_count_b(const uint32_t* __restrict__ idb,
+                                                     const int* __restrict__ tseg,
+                                                     const SegState* __restrict__ sst,
                                                      int* __restrict__ cnt, uint32_t* __restrict__ keys,
-                                                     uint32_t* __restrict__ vals) {
-  int c = blockIdx.x * kThreads + threadIdx.x;
-  if (c >= nc) return;
-  uint32_t b = idb[c];
-  atomicAdd(&cnt[b], 1);
-  keys[c] = b;
-  vals[c] = (uint32_t)c;
+                                                     uint32_t* __restrict__ vals,
+                                                     const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
+  const int nt = ew->ntiles;
+  for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+    const SegState& S = sst[tseg[t]];
+    const int k0 = (t - S.t0) * kTileItems;
+    for (int m = 0; m < kItemsPerThread; ++m) {
+      int k = k0 + m * kThreads + threadIdx.x;
+      if (k < S.nc) {
+        int c = S.c0 + k;
+        uint32_t b = idb[c];
+        atomicAdd(&cnt[b], 1);
+        keys[c - S.delta] = b;
+        vals[c - S.delta] = (uint32_t)c;
+      }
+    }
+  }
 }
 
 // Per-body incidence length: contacts where the body is B plus where it is A.
 __global__ void __launch_bounds__(kThreads) k_inc_count(int nb, const int* __restrict__ bstart,
-                                                       const int* __restrict__ abase,
-                                                       int* __restrict__ cnt) {
+                                                       const int* __restrict__ acnt,
+                                                       int* __restrict__ cnt,
+                                                       const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
   int b = blockIdx.x * kThreads + threadIdx.x;
   if (b >= nb) return;
-  cnt[b] = (bstart[b + 1] - bstart[b]) + (abase[b + 1] - abase[b]);
+  cnt[b] = (bstart[b + 1] - bstart[b]) + acnt[b];
 }
 
 // B-side contacts (flagged, ascending) then the A-side range: the ascending
@@ -458,23 +637,36 @@ __global__ void __launch_bounds__(kThreads) k_inc_count(int nb, const int* __res
 __global__ void __launch_bounds__(kThreads) k_inc_fill(int nb, const int* __restrict__ bstart,
                                                       const uint32_t* __restrict__ binc,
                                                       const int* __restrict__ abase,
+                                                      const int* __restrict__ acnt,
+                                                      const int* __restrict__ bseg,
+                                                      const SegState* __restrict__ sst,
                                                       const int* __restrict__ istart,
-                                                      uint32_t* __restrict__ inc) {
+                                                      uint32_t* __restrict__ inc,
+                                                      const EngineWords* __restrict__ ew) {
+  if (ew->err) return;
   int b = blockIdx.x * kThreads + threadIdx.x;
   if (b >= nb) return;
   int o = istart[b];
   for (int i = bstart[b]; i < bstart[b + 1]; ++i) inc[o++] = binc[i] | 0x80000000u;
-  for (int c = abase[b]; c < abase[b + 1]; ++c) inc[o++] = (uint32_t)c;
+  const int n = acnt[b];
+  if (n) {
+    const int c0 = abase[b] + sst[bseg[b]].delta;
+    for (int j = 0; j < n; ++j) inc[o++] = (uint32_t)(c0 + j);
+  }
 }
 
-CollideArgs make_args(SceneDev& sd, double env) {
+CollideArgs make_args(SceneDev& sd) {
   CollideArgs a;
   a.nb = sd.nb;
   a.n_small = sd.n_small;
   a.n_large = sd.n_large;
+  a.max_seg_chunks = sd.max_seg_chunks;
   a.p4 = sd.p4;
   a.g4 = sd.geom4;
   a.fam = sd.family;
+  a.bseg = sd.bseg;
+  a.seg = sd.seg;
+  a.sst = sd.sst;
   a.amin = sd.amin;
   a.amax = sd.amax;
   a.cell = sd.cell;
@@ -484,18 +676,17 @@ CollideArgs make_args(SceneDev& sd, double env) {
   a.cstart = sd.cell_start;
   a.cend = sd.cell_end;
   a.grid = sd.grid;
-  a.env = env;
   a.cnt_cont = sd.cnt_cont;
   a.cnt_cand = sd.cnt_cand;
-  a.counters = sd.counters;
   a.cbase = sd.cbase;
+  a.ew = sd.ew;
   a.ccap = sd.ccap;
   a.ida = sd.ida;
   a.idb = sd.idb;
   a.F = sd.F;
+  a.nf = sd.nf;
   a.gap = sd.gap;
   a.loc = sd.loc;
-  a.err = reinterpret_cast<unsigned*>(sd.counters + 2);
   return a;
 }
 
@@ -505,84 +696,76 @@ int bits_for(int n) {
   return b;
 }
 
+int blocks_for(long long n) { return (int)std::max(1LL, (n + kThreads - 1) / kThreads); }
+
 }  // namespace
 
-void collide_count(SceneDev& sd, double env, cudaStream_t st, int64_t* launches) {
-  int nb = sd.nb;
-  cudaMemsetAsync(sd.counters, 0, 4 * sizeof(int), st);
+void collide(SceneDev& sd, cudaStream_t st, int64_t* launches) {
+  const int nb = sd.nb;
+  if (nb == 0) return;
+  const int park = sd.ncell_cap - 1;  // cell of spheres in inactive segments
   cudaMemsetAsync(sd.cnt_cont, 0, sizeof(int) * (size_t)nb, st);
   cudaMemsetAsync(sd.cnt_cand, 0, sizeof(int) * (size_t)nb, st);
-  k_bounds_init<<<1, 1, 0, st>>>(sd.grid);
-  int gb = (nb + kThreads - 1) / kThreads;
-  k_aabb<<<gb, kThreads, 0, st>>>(sd.p4, sd.geom4, nb, env, sd.amin, sd.amax, sd.grid);
-  k_grid_setup<<<1, 1, 0, st>>>(sd.grid, sd.W, sd.ncell_cap);
-  int gs = (std::max(nb, sd.n_small) + kThreads - 1) / kThreads;
-  k_shift_and_bin<<<gs, kThreads, 0, st>>>(nb, sd.small_ids, sd.n_small, sd.p4, sd.geom4, env,
-                                           sd.amin, sd.amax, sd.grid, sd.cell, sd.keyA, sd.valA);
+  k_seg_reset<<<blocks_for(sd.nseg), kThreads, 0, st>>>(sd.nseg, sd.grid, sd.sst, sd.ew);
+  k_aabb<<<blocks_for(nb), kThreads, 0, st>>>(sd.p4, sd.geom4, sd.bseg, sd.seg, nb, sd.amin,
+                                              sd.amax, sd.grid, sd.ew);
+  k_grid_setup<<<blocks_for(sd.nseg), kThreads, 0, st>>>(sd.nseg, sd.seg, sd.grid, sd.ew);
+  k_shift_and_bin<<<blocks_for(std::max(nb, sd.n_small)), kThreads, 0, st>>>(
+      nb, sd.small_ids, sd.n_small, sd.bseg, sd.seg, sd.p4, sd.geom4, sd.amin, sd.amax, sd.grid,
+      sd.cell, sd.keyA, sd.valA, park, sd.ew);
   *launches += 4;
   if (sd.n_small > 0) {
-    radix_sort_pairs(sd.keyA, sd.valA, sd.keyB, sd.valB, sd.radix_hist, sd.n_small,
-                     bits_for(sd.ncell_cap), st, launches);
+    radix_sort_pairs(sd.keyA, sd.valA, sd.keyB, sd.valB, sd.radix_hist, &sd.ew->n_small,
+                     sd.n_small, bits_for(sd.ncell_cap), st, launches);
     cudaMemsetAsync(sd.cell_start, 0xff, sizeof(int) * (size_t)sd.ncell_cap, st);
-    k_cell_ranges<<<(sd.n_small + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-        sd.keyA, sd.n_small, sd.cell_start, sd.cell_end, sd.ncell_cap);
+    k_cell_ranges<<<blocks_for(sd.n_small), kThreads, 0, st>>>(sd.keyA, sd.n_small, sd.cell_start,
+                                                               sd.cell_end, park, sd.ew);
     ++*launches;
   }
-  CollideArgs a = make_args(sd, env);
+  CollideArgs a = make_args(sd);
+  const int pair_blocks = (sd.n_small + kWarpsPerCta - 1) / kWarpsPerCta;
+  dim3 box_grid(sd.max_seg_chunks, sd.n_large);
   if (sd.n_small > 0) {
-    k_sphere_pairs<false><<<(sd.n_small + kWarpsPerCta - 1) / kWarpsPerCta, kThreads, 0, st>>>(a);
+    k_sphere_pairs<false><<<pair_blocks, kThreads, 0, st>>>(a);
     ++*launches;
   }
   if (sd.n_large > 0) {
-    int nchunks = (nb + kThreads - 1) / kThreads;
-    dim3 grid(nchunks, sd.n_large);
-    k_box_pairs<false><<<grid, kThreads, 0, st>>>(a, sd.large_chunk, nullptr, nchunks);
+    k_box_pairs<false><<<box_grid, kThreads, 0, st>>>(a, sd.large_chunk, nullptr);
     ++*launches;
   }
   exclusive_scan_i32(sd.cnt_cont, sd.cbase, nb, sd.scan_tmp, st, launches);
-  cudaMemcpyAsync(sd.counters, sd.cbase + nb, sizeof(int), cudaMemcpyDeviceToDevice, st);
-  cudaMemcpyAsync(sd.h_counters, sd.counters, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
-}
-
-void collide_write(SceneDev& sd, double env, cudaStream_t st, int64_t* launches) {
-  int nb = sd.nb;
-  CollideArgs a = make_args(sd, env);
+  k_seg_layout<<<1, 1024, 0, st>>>(sd.nseg, nb, sd.seg, sd.sst, sd.cbase, sd.seg_tstart, sd.ccap,
+                                   sd.tcap, sd.ew);
+  k_tile_table<<<std::max(1, std::min(sd.tcap / kThreads + 1, 1184)), kThreads, 0, st>>>(
+      sd.nseg, sd.seg_tstart, sd.tseg, sd.tcap, sd.ew);
+  *launches += 2;
   if (sd.n_small > 0) {
-    k_sphere_pairs<true><<<(sd.n_small + kWarpsPerCta - 1) / kWarpsPerCta, kThreads, 0, st>>>(a);
+    k_sphere_pairs<true><<<pair_blocks, kThreads, 0, st>>>(a);
     ++*launches;
   }
   if (sd.n_large > 0) {
-    int nchunks = (nb + kThreads - 1) / kThreads;
-    exclusive_scan_i32(sd.large_chunk, sd.large_chunk_off, nchunks * sd.n_large, sd.scan_tmp, st,
-                       launches);
-    dim3 grid(nchunks, sd.n_large);
-    k_box_pairs<true><<<grid, kThreads, 0, st>>>(a, nullptr, sd.large_chunk_off, nchunks);
+    exclusive_scan_i32(sd.large_chunk, sd.large_chunk_off, sd.max_seg_chunks * sd.n_large,
+                       sd.scan_tmp, st, launches);
+    k_box_pairs<true><<<box_grid, kThreads, 0, st>>>(a, nullptr, sd.large_chunk_off);
     ++*launches;
   }
-  int nc = sd.nc;
   // B-side incidence: stable radix sort of (B, contact) keeps ascending contact order.
   cudaMemsetAsync(sd.cnt_cand, 0, sizeof(int) * (size_t)nb, st);
-  if (nc > 0) {
-    k_count_b<<<(nc + kThreads - 1) / kThreads, kThreads, 0, st>>>(sd.idb, nc, sd.cnt_cand,
-                                                                   sd.keyA, sd.valA);
-    ++*launches;
-    radix_sort_pairs(sd.keyA, sd.valA, sd.keyB, sd.valB, sd.radix_hist, nc, bits_for(nb), st,
-                     launches);
-  }
+  const int tile_blocks = std::max(1, std::min(sd.tcap, 4 * 148 * 4));
+  k_count_b<<<tile_blocks, kThreads, 0, st>>>(sd.idb, sd.tseg, sd.sst, sd.cnt_cand, sd.keyA,
+                                              sd.valA, sd.ew);
+  ++*launches;
+  radix_sort_pairs(sd.keyA, sd.valA, sd.keyB, sd.valB, sd.radix_hist, &sd.ew->nc_total,
+                   (int)sd.ccap, bits_for(nb), st, launches);
   exclusive_scan_i32(sd.cnt_cand, sd.binc_start, nb, sd.scan_tmp, st, launches);
-  if (nc > 0)
-    cudaMemcpyAsync(sd.binc, sd.valA, sizeof(uint32_t) * (size_t)nc, cudaMemcpyDeviceToDevice, st);
-  int gb = (nb + kThreads - 1) / kThreads;
-  if (nb > 0) {
-    k_inc_count<<<gb, kThreads, 0, st>>>(nb, sd.binc_start, sd.cbase, sd.cnt_cand);
-    ++*launches;
-  }
+  k_inc_count<<<blocks_for(nb), kThreads, 0, st>>>(nb, sd.binc_start, sd.cnt_cont, sd.cnt_cand,
+                                                   sd.ew);
+  ++*launches;
   exclusive_scan_i32(sd.cnt_cand, sd.inc_start, nb, sd.scan_tmp, st, launches);
-  if (nb > 0 && nc > 0) {
-    k_inc_fill<<<gb, kThreads, 0, st>>>(nb, sd.binc_start, sd.binc, sd.cbase, sd.inc_start,
-                                        sd.inc);
-    ++*launches;
-  }
+  k_inc_fill<<<blocks_for(nb), kThreads, 0, st>>>(nb, sd.binc_start, sd.valA, sd.cbase,
+                                                  sd.cnt_cont, sd.bseg, sd.sst, sd.inc_start,
+                                                  sd.inc, sd.ew);
+  ++*launches;
 }
 
 }  // namespace dv

@@ -205,6 +205,7 @@ enum : unsigned {
   kErrCapacity = 8u,
   kErrAborted = 16u,
   kErrCopyTimeout = 32u,
+  kErrPartners = 64u,     // a sphere has more contact partners than the pair kernel keeps
 };
 
 // Longest a CTA waits at a grid barrier before it records a timeout and

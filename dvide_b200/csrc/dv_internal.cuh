@@ -1,18 +1,32 @@
-// dv_internal.cuh -- device-side layout of one scene and the kernels' entry
-// points.  Data layout in HBM (all device-resident between calls):
+// dv_internal.cuh -- device-side layout of an engine (one or many scenes) and
+// the kernels' entry points.
 //
-//   bodies (nb):  p4, v4, k4, f4, w4, fc4 as double4 (x, y, z, unused) so a
-//                 body is one 32-byte sector for the random gathers of the
-//                 narrowphase and the Schur product; minv (double, 0 = fixed);
-//                 geom4 (gx, gy, gz, 1 if box); family (int).
-//   contacts:     sorted by (A, B) like the reference's thrust::unique of
-//                 64-bit pair keys (CollisionDetector.cu:319-325).  ids A/B
-//                 (uint32), frame n,u,v as 9 planes, gap, location (3 planes),
-//                 r (3 planes); every per-contact 3-vector is 3 planes of
-//                 stride `ccap` (structure of arrays, coalesced 8-byte loads).
-//   incidence:    contacts where a body is B, in ascending contact order
-//                 (stable radix sort by B); contacts where it is A are the
-//                 contiguous range [cbase[b], cbase[b+1]).
+// An engine steps S independent scenes ("segments") together.  A plain
+// System is an engine with one segment; a batch or a server holds many.
+// Every per-segment computation (collision grid, contact order, reductions,
+// APGD control) depends only on that segment's own data, so a scene's
+// results are bit-identical alone and in any mix.
+//
+// Data layout in HBM (all device-resident between calls):
+//
+//   bodies (nb, all segments concatenated, segment s owns [b0, b1)):
+//                 p4, v4, k4, f4, fc4 as double4 (x, y, z, unused) so a body is
+//                 one 32-byte sector for the random gathers of the narrowphase;
+//                 w4 (Schur body vector; float4 in the mixed-precision solve);
+//                 minv (double, 0 = fixed); geom4 (gx, gy, gz, 1 if box);
+//                 family (int); bseg (segment of the body).
+//   contacts:     per segment sorted by (A, B) like the reference's
+//                 thrust::unique of 64-bit pair keys (CollisionDetector.cu:
+//                 319-325); segment s owns [c0, c0 + nc), c0 a multiple of 256.
+//                 ids A/B (uint32, global body ids), normal n as 3 planes (plus
+//                 u, v for the frame accessors), gap, location (3 planes); every
+//                 per-contact 3-vector is 3 planes of stride `ccap` (structure
+//                 of arrays, coalesced loads).
+//   tiles:        512 contacts; segment s owns tiles [t0, t0 + nt); tile k of
+//                 a segment covers its contacts [512 k, 512 k + 512).  Per-tile
+//                 partial sums are folded per segment in a fixed order.
+//   incidence:    per body, its contacts in ascending contact order: those
+//                 where it is B (bit 31 set), then those where it is A.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,8 +38,10 @@
 
 namespace dv {
 
+constexpr int kContactAlign = 256;  // segment contact ranges start on this multiple
+
 struct GridInfo {
-  double ox, oy, oz;        // global origin (AABB union min - 0.01, CollisionDetector.cu:566-568)
+  double ox, oy, oz;        // origin (AABB union min - 0.01, CollisionDetector.cu:566-568)
   double inv_w;             // 1 / cell width
   int dx, dy, dz;           // cells per axis
   int ncells;
@@ -33,11 +49,24 @@ struct GridInfo {
   unsigned long long hi[3]; // ordered-bits AABB max accumulator
 };
 
-// Scalar state of one APGD solve, owned by the controller CTA of the
-// persistent kernel (APGD.cu:208-223, 266-332).  Iterates live in five
-// rotating buffers G[0..4] with their Schur products NG[0..4]: cur = gamma_k,
-// prev = gamma_{k-1}, nw = target of gamma_new, best = gamma_hat (-1 before the
-// first accepted iterate); the fifth holds the next iterate computed ahead.
+// Read-only description of one segment (host-written).
+struct SegParams {
+  double h, mu, tol, env;
+  double W;                 // grid cell lower bound: widest small AABB, 2 (r_max + env)
+  int max_iter, max_bt, warm;
+  int active;               // 0: the segment is skipped entirely (free server slot)
+  int b0, b1;               // bodies
+  int s0, s1;               // small (gridded) bodies in small_ids
+  int l0, l1;               // large bodies (boxes) in large_ids
+  int cell_base, cell_cap;  // global cell ids [cell_base, cell_base + cell_cap)
+  int wbase, wcap;          // warm-start region [wbase, wbase + wcap) of the gamma arena
+};
+
+// Scalar state of one APGD solve (APGD.cu:208-223, 266-332).  Iterates live in
+// five rotating buffers G[0..4] with their Schur products NG[0..4]: cur =
+// gamma_k, prev = gamma_{k-1}, nw = target of gamma_new, best = gamma_hat (-1
+// before the first accepted iterate); the fifth holds the next iterate computed
+// ahead.
 struct ApgdCtl {
   double L, t, theta, theta_new, beta;
   double obj1, obj2, obj2_base;
@@ -57,26 +86,64 @@ struct ApgdCtl {
   unsigned err;
   int iterations;
   int sweeps;           // iterations executed
-  // device time between consecutive grid-barrier releases, by the phase that
-  // ended at the barrier (globaltimer ns): see kPhase* in dv_apgd.cu
+};
+
+// Per-segment results of the current step (device-written).
+struct SegState {
+  int nc, npossible;
+  int c0;               // first contact slot (multiple of kContactAlign)
+  int t0, nt;           // tiles
+  int delta;            // c0 - (unpadded global offset of the segment's first contact)
+  int gsize;            // warm-start length (System::gamma_d / 3); kept when nc = 0
+  unsigned arrive;      // tile arrivals in the current pass
+  unsigned err;         // error bits of this segment's last step
+  int pad_;
+  ApgdCtl ctl;
+};
+
+// Engine-wide words (device).
+struct EngineWords {
+  int nc_total;         // unpadded contacts of all segments
+  int nc_pad;           // padded contact slots in use
+  int ntiles;           // tiles in use
+  int npossible;
+  int n_small;          // gridded bodies (constant)
+  int stop_on_seg_err;  // 1: a segment's solver error also sets err (plain System semantics)
+  unsigned err;         // error bits (kErr*); sticky: every kernel of a step skips its work while set
+  int steps_done;       // steps completed since creation
+  int active;           // segments still iterating (solve kernel)
+  int step_count;       // segments that request a step pass next iteration
+  int step_needed;      // latched step_count for the current iteration
+  unsigned bar[4];      // grid barrier: [0] arrivals, [1] generation, [2] error bits
   unsigned long long last_release;
   unsigned long long phase_ns[8];
   unsigned long long phase_count[8];
 };
 
 struct SceneDev {
-  int nb = 0;
+  int nb = 0, nseg = 0;
   int n_small = 0, n_large = 0;
+  int precision = DV_PREC_FP64;
+  // segments
+  SegParams* seg = nullptr;     // nseg
+  SegState* sst = nullptr;      // nseg
+  GridInfo* grid = nullptr;     // nseg
+  int* seg_tstart = nullptr;    // nseg + 1 tile starts (for tile -> segment lookup)
+  int* tseg = nullptr;          // tile -> segment
+  unsigned* donemask = nullptr; // (nseg + 31) / 32 words: segments not iterating
+  EngineWords* ew = nullptr;
   // bodies
   double4 *p4 = nullptr, *v4 = nullptr, *k4 = nullptr, *f4 = nullptr, *w4 = nullptr, *fc4 = nullptr;
   double4* geom4 = nullptr;
   double* minv = nullptr;
   int* family = nullptr;
-  int* small_ids = nullptr;   // sphere bodies binned in the grid
-  int* large_ids = nullptr;   // boxes, tested against all bodies
+  int* bseg = nullptr;
+  int* small_ids = nullptr;   // sphere bodies binned in the grid, grouped by segment
+  int* large_ids = nullptr;   // boxes, tested against all bodies of their segment
+  int max_seg_chunks = 0;     // largest ceil(segment bodies / 256)
   // collision scratch
   double4 *amin = nullptr, *amax = nullptr;   // shifted AABBs
-  int4* cell = nullptr;                       // cell coords + linear id (small bodies)
+  int4* cell = nullptr;                       // cell coords + global linear id
   uint32_t *keyA = nullptr, *valA = nullptr, *keyB = nullptr, *valB = nullptr;  // radix buffers
   size_t radix_cap = 0;
   uint32_t* radix_hist = nullptr;
@@ -86,70 +153,65 @@ struct SceneDev {
   int ncell_cap = 0;
   int* cnt_cont = nullptr;    // contacts with A = body
   int* cnt_cand = nullptr;    // candidate pairs with A = body
-  int* cbase = nullptr;       // exclusive scan of cnt_cont (nb + 1)
+  int* cbase = nullptr;       // exclusive scan of cnt_cont (nb + 1), unpadded
   int* scan_tmp = nullptr;
   size_t scan_tmp_cap = 0;
   int* large_chunk = nullptr; // per (large body, chunk) counts
   int* large_chunk_off = nullptr;
   int large_chunks = 0;
-  GridInfo* grid = nullptr;
-  int* counters = nullptr;    // [0] nc, [1] npossible (device)
-  int* h_counters = nullptr;  // pinned mirror
-  double W = 0;               // widest small AABB (2 (r_max + envelope))
   // contacts
-  size_t ccap = 0;
-  int nc = 0, npossible = 0;
+  size_t ccap = 0;            // contact slots
+  int tcap = 0;               // tiles
   uint32_t *ida = nullptr, *idb = nullptr;
-  double* F = nullptr;        // 9 planes
+  double* F = nullptr;        // 9 planes (n, u, v)
+  float* nf = nullptr;        // 3 planes: n rounded to float (mixed-precision solve)
   double* gap = nullptr;
   double* loc = nullptr;      // 3 planes
-  double* r = nullptr;        // 3 planes
+  double* r = nullptr;        // 3 planes (float planes in the mixed solve)
   int* binc_start = nullptr;  // nb + 1
   uint32_t* binc = nullptr;   // contact ids sorted by B
-  // flat incidence per body in ascending contact order: B-side contacts with
-  // bit 31 set (sign -1), then A-side contacts; body b owns [inc_start[b], inc_start[b+1])
   int* inc_start = nullptr;   // nb + 1
   uint32_t* inc = nullptr;    // 2 * ccap
   // APGD work: iterates and their Schur products, 3 planes each (stride ccap)
   double* G[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double* NG[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double4* q = nullptr;
-  double* part = nullptr;     // reduction partials
-  int part_tiles = 0;
-  // warm-start buffer (System::gamma_d): 3 planes, stride gcap
+  double* part = nullptr;     // reduction partials, 9 x tcap
+  // warm-start arena (System::gamma_d of every segment): 3 planes of stride
+  // wtotal; segment s owns [wbase, wbase + wcap), positional within it
   double* gamma = nullptr;
-  size_t gcap = 0;
-  int gsize = 0;
-  ApgdCtl* ctl = nullptr;
-  ApgdCtl* h_ctl = nullptr;   // pinned mirror
-  unsigned* bar = nullptr;    // grid barrier words
+  size_t wtotal = 0;
+  // host mirrors
+  EngineWords* h_ew = nullptr;    // pinned
+  SegState* h_sst = nullptr;      // pinned, nseg
 };
 
 // ---- sort / scan (dv_sort.cu) ----
 size_t radix_hist_size(size_t n);
-// Stable LSD radix sort of (key, value) by the low `bits` bits of key.
-// On return the sorted data is in (k0, v0); k1/v1 are scratch.
+// Stable LSD radix sort of (key, value) by the low `bits` bits of key.  The
+// item count is read on the device from *n_dev (at most n_cap).  On return the
+// sorted data is in (k0, v0); k1/v1 are scratch.
 void radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint32_t* hist,
-                      int n, int bits, cudaStream_t st, int64_t* launches);
+                      const int* n_dev, int n_cap, int bits, cudaStream_t st, int64_t* launches);
 size_t scan_tmp_size(size_t n);
 // out[i] = sum_{j<i} in[i]; out[n] = total.  n may be 0.
 void exclusive_scan_i32(const int* in, int* out, int n, int* tmp, cudaStream_t st,
                         int64_t* launches);
 
 // ---- collision (dv_collide.cu) ----
-// Counts candidates and contacts; leaves nc / npossible in sd.counters.
-void collide_count(SceneDev& sd, double envelope, cudaStream_t st, int64_t* launches);
-// Writes the sorted contact list, frames and the B-side incidence.
-void collide_write(SceneDev& sd, double envelope, cudaStream_t st, int64_t* launches);
+// The whole collision pipeline of one step: contacts of every active segment,
+// their tiles and the body incidence.  Sizes are read on the device; a
+// capacity overflow sets kErrCapacity in EngineWords::err and leaves the
+// contact arrays unwritten.
+void collide(SceneDev& sd, cudaStream_t st, int64_t* launches);
 
 // ---- step (dv_apgd.cu) ----
 struct SolveConfig {
-  double h, mu, tol;
-  int max_iter, max_bt, warm, precision;
-  int grid;   // CTAs of the persistent kernel
+  int grid;        // CTAs of the persistent kernel
+  int chunk;       // tiles a CTA takes at a time (1, 2, 4)
+  int contiguous;  // 1: CTA c takes a contiguous range of tiles; 0: round robin
 };
 int apgd_max_ctas(int precision);
 void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches);
-void launch_step_nocontact(SceneDev& sd, double h, cudaStream_t st, int64_t* launches);
 
 }  // namespace dv

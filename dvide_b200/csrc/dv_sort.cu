@@ -7,6 +7,8 @@
 // digits; a scan of the digit-major count table gives every (digit, tile) its
 // output base; the scatter recomputes each item's rank among equal digits in
 // index order with warp match masks, so equal keys keep their input order.
+#include <algorithm>
+
 #include "dv_internal.cuh"
 
 namespace dv {
@@ -17,10 +19,11 @@ constexpr int kRadixTile = 2048;
 constexpr int kRadixRounds = kRadixTile / kThreads;  // 8
 constexpr int kScanBlock = 1024;
 
-__global__ void __launch_bounds__(kThreads) k_radix_count(const uint32_t* __restrict__ keys, int n,
-                                                          int shift, uint32_t* __restrict__ hist,
-                                                          int ntiles) {
+__global__ void __launch_bounds__(kThreads) k_radix_count(const uint32_t* __restrict__ keys,
+                                                          const int* __restrict__ n_dev, int shift,
+                                                          uint32_t* __restrict__ hist, int ntiles) {
   __shared__ unsigned cnt[256];
+  const int n = *n_dev;
   cnt[threadIdx.x] = 0;
   __syncthreads();
   int base = blockIdx.x * kRadixTile;
@@ -34,8 +37,11 @@ __global__ void __launch_bounds__(kThreads) k_radix_count(const uint32_t* __rest
 
 __global__ void __launch_bounds__(kThreads) k_radix_scatter(
     const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    uint32_t* __restrict__ vout, int n, int shift, const int* __restrict__ offs, int ntiles) {
+    uint32_t* __restrict__ vout, const int* __restrict__ n_dev, int shift,
+    const int* __restrict__ offs, int ntiles) {
   __shared__ int run[256];
+  const int n = *n_dev;
+  if (blockIdx.x * kRadixTile >= n) return;
   __shared__ int wcnt[kThreads / 32][256];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   run[threadIdx.x] = offs[(size_t)threadIdx.x * ntiles + blockIdx.x];
@@ -132,6 +138,18 @@ __global__ void __launch_bounds__(kThreads) k_scan_add(int* __restrict__ out, in
 
 __global__ void k_set_zero_total(int* out) { out[0] = 0; }
 
+__global__ void __launch_bounds__(kThreads) k_copy_pairs(const uint32_t* __restrict__ ks,
+                                                         const uint32_t* __restrict__ vs,
+                                                         uint32_t* __restrict__ kd,
+                                                         uint32_t* __restrict__ vd,
+                                                         const int* __restrict__ n_dev) {
+  const int n = *n_dev;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+    kd[i] = ks[i];
+    vd[i] = vs[i];
+  }
+}
+
 }  // namespace
 
 size_t scan_tmp_size(size_t n);
@@ -177,9 +195,9 @@ void exclusive_scan_i32(const int* in, int* out, int n, int* tmp, cudaStream_t s
 }
 
 void radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint32_t* hist,
-                      int n, int bits, cudaStream_t st, int64_t* launches) {
-  if (n <= 1 || bits <= 0) return;
-  int ntiles = (n + kRadixTile - 1) / kRadixTile;
+                      const int* n_dev, int n_cap, int bits, cudaStream_t st, int64_t* launches) {
+  if (n_cap <= 1 || bits <= 0) return;
+  int ntiles = (n_cap + kRadixTile - 1) / kRadixTile;
   int passes = (bits + 7) / 8;
   uint32_t* cnt = hist;
   int* offs = reinterpret_cast<int*>(hist + 256 * (size_t)ntiles);
@@ -188,19 +206,20 @@ void radix_sort_pairs(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, ui
   uint32_t *ki = k0, *vi = v0, *ko = k1, *vo = v1;
   for (int p = 0; p < passes; ++p) {
     int shift = 8 * p;
-    k_radix_count<<<ntiles, kThreads, 0, st>>>(ki, n, shift, cnt, ntiles);
+    k_radix_count<<<ntiles, kThreads, 0, st>>>(ki, n_dev, shift, cnt, ntiles);
     ++*launches;
     exclusive_scan_i32(reinterpret_cast<const int*>(cnt), offs, 256 * ntiles, scan_tmp, st,
                        launches);
-    k_radix_scatter<<<ntiles, kThreads, 0, st>>>(ki, vi, ko, vo, n, shift, offs, ntiles);
+    k_radix_scatter<<<ntiles, kThreads, 0, st>>>(ki, vi, ko, vo, n_dev, shift, offs, ntiles);
     ++*launches;
     uint32_t* t;
     t = ki; ki = ko; ko = t;
     t = vi; vi = vo; vo = t;
   }
   if (passes & 1) {  // the sorted data is in (k1, v1): move it back
-    cudaMemcpyAsync(k0, k1, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(v0, v1, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    int g = std::min(ntiles * (kRadixTile / kThreads), 4 * 148 * 8);
+    k_copy_pairs<<<g, kThreads, 0, st>>>(k1, v1, k0, v0, n_dev);
+    ++*launches;
   }
 }
 

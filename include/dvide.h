@@ -176,6 +176,139 @@ DV_API int dv_ccp_violation_noalloc(int32_t nc, int32_t nb, const double* gamma,
                                     const uint32_t* ida, const uint32_t* idb, const double* v,
                                     double mu, double h, double* out4, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched scenes.  No counterpart in the reference (DVIDE steps one System
+ * per process).  A batch steps many independent scenes together: one
+ * collision pipeline and ONE persistent solve kernel per step for all of
+ * them, each scene with its own parameters, contact set, warm start and APGD
+ * convergence (a converged scene stops iterating while the others go on).
+ * Every reduction of a scene runs over that scene's own tiles in a fixed
+ * order, so each scene's results are bit-identical to the same scene stepped
+ * alone (dv_scene_* with the same precision) and independent of the launch
+ * shape.  Bodies of all scenes are passed concatenated: scene i owns
+ * counts[i] consecutive entries.  precision: DV_PREC_FP64 or DV_PREC_MIXED
+ * for every scene of the batch (each dv_params' own precision is ignored).
+ * ------------------------------------------------------------------------ */
+typedef struct dv_batch dv_batch;
+
+typedef struct dv_scene_stats {
+  int32_t num_contacts;
+  int32_t num_possible;
+  int32_t iterations;
+  int32_t backtracks;
+  double residual;
+  double objective;
+  int32_t status;            /* DV_OK, DV_ERR_NAN or DV_ERR_NOCONV for this scene */
+  int32_t sweeps;
+} dv_scene_stats;
+
+typedef struct dv_tune_candidate {
+  int32_t grid;              /* CTAs of the persistent solve kernel */
+  int32_t chunk;             /* consecutive 512-contact tiles a CTA takes at a time */
+  int32_t contiguous;        /* 1: each CTA owns one contiguous tile range (scenes per CTA) */
+  float ms_per_step;         /* measured device time per step */
+} dv_tune_candidate;
+
+typedef struct dv_tune_report {
+  int32_t num_candidates;
+  int32_t best;              /* index of the chosen candidate (now in effect) */
+  int32_t identical;         /* 1: every candidate produced bit-identical states */
+  int32_t steps_per_trial;
+  dv_tune_candidate cand[16];
+} dv_tune_report;
+
+DV_API int dv_batch_create(const dv_body_desc* bodies, const int32_t* counts, int32_t nscenes,
+                           const dv_params* params, int32_t precision, dv_batch** out);
+DV_API int dv_batch_destroy(dv_batch* b);
+DV_API int dv_batch_set_stream(dv_batch* b, void* cuda_stream);
+/* nsteps time steps of every scene; returns the first engine-level error
+ * (per-scene solver errors are reported in dv_batch_scene_stats). */
+DV_API int dv_batch_step(dv_batch* b, int32_t nsteps);
+DV_API int dv_batch_num_scenes(dv_batch* b, int32_t* nscenes, int32_t* nbodies);
+/* p, v: 3 doubles per body of `scene`, or of all scenes concatenated when scene < 0. */
+DV_API int dv_batch_get_state(dv_batch* b, int32_t scene, double* p, double* v);
+DV_API int dv_batch_set_state(dv_batch* b, int32_t scene, const double* p, const double* v);
+/* Per-scene report of the last step (nscenes entries). */
+DV_API int dv_batch_scene_stats(dv_batch* b, dv_scene_stats* out);
+/* Per-step, per-scene reports of the last dv_batch_step call: steps x nscenes
+ * entries (step-major) and the device time of each step. */
+DV_API int dv_batch_step_history(dv_batch* b, dv_scene_stats* out, float* step_ms, int32_t cap_steps,
+                                 int32_t* nsteps);
+DV_API int dv_batch_get_gamma(dv_batch* b, int32_t scene, double* gamma, int32_t cap, int32_t* n);
+DV_API int dv_batch_ccp_violation(dv_batch* b, int32_t scene, double* out4);
+/* Launch shape of the solve kernel (grid <= 0: default). */
+DV_API int dv_batch_set_launch(dv_batch* b, int32_t grid, int32_t chunk, int32_t contiguous);
+DV_API int dv_batch_get_launch(dv_batch* b, int32_t* grid, int32_t* chunk, int32_t* contiguous,
+                               int32_t* max_grid);
+/* Replay each step from a captured CUDA graph (collision + solve); returns
+ * DV_ERR_UNSUPPORTED and keeps stream launches if capture fails. */
+DV_API int dv_batch_set_graph(dv_batch* b, int32_t enable);
+/* Times candidate launch shapes on the batch's own scenes (steps_per_trial
+ * steps each, state restored after every trial and at the end), checks that
+ * all of them give bit-identical states, and keeps the fastest. */
+DV_API int dv_batch_autotune(dv_batch* b, int32_t steps_per_trial, dv_tune_report* out);
+DV_API int64_t dv_batch_launch_count(dv_batch* b);
+
+/* ------------------------------------------------------------------------
+ * Serving.  No counterpart in the reference.  A server keeps scenes (requests
+ * for nsteps time steps each) resident on the device and steps every resident
+ * scene together; requests that arrive while others run are admitted as
+ * soon as a slot and the HBM budget allow, and a scene leaves when its steps
+ * are done (continuous batching).  Membership changes move the resident
+ * scenes' state device-to-device; a scene's results are bit-identical to the
+ * same scene stepped alone with the same precision.  The caller drives it:
+ * dv_server_submit when a request arrives, dv_server_round repeatedly (one
+ * round = admissions, steps_per_round steps, retirements), dv_server_poll for
+ * finished requests.  Times are seconds on the server's steady clock.
+ * ------------------------------------------------------------------------ */
+typedef struct dv_server dv_server;
+
+typedef struct dv_server_config {
+  double hbm_budget_bytes;   /* admission budget for resident scenes (estimate per scene) */
+  int32_t max_active;        /* resident scenes at most */
+  int32_t steps_per_round;   /* steps between admission and retirement checks */
+  int32_t precision;         /* DV_PREC_FP64 or DV_PREC_MIXED for every scene */
+  int32_t use_graph;         /* replay steps from a CUDA graph between membership changes */
+  int32_t keep_states;       /* keep each finished scene's final p, v for dv_server_result_state */
+  int32_t pad_;
+} dv_server_config;
+
+typedef struct dv_request_result {
+  int64_t id;
+  int32_t nb;
+  int32_t nsteps;
+  int32_t status;            /* first solver error of the scene, DV_OK otherwise */
+  int32_t rounds;
+  double t_submit, t_admit, t_done;
+  double contact_steps;      /* contacts summed over its steps */
+  double step_ms_mean, step_ms_p50, step_ms_p99;  /* device time of the steps it took part in */
+  double bytes;              /* admission estimate */
+} dv_request_result;
+
+typedef struct dv_server_stats {
+  int64_t submitted, admitted, completed, pending, active, rounds, reconfigures, steps;
+  double bytes_in_use;
+  double contact_steps;      /* contacts summed over every scene and step */
+  double device_ms;          /* device time of all steps */
+} dv_server_stats;
+
+DV_API int dv_server_default_config(dv_server_config* cfg);
+DV_API int dv_server_create(const dv_server_config* cfg, dv_server** out);
+DV_API int dv_server_destroy(dv_server* s);
+DV_API int dv_server_set_stream(dv_server* s, void* cuda_stream);
+DV_API double dv_server_clock(dv_server* s);
+/* Queues a request; bodies are copied.  Returns DV_ERR_OOM if the scene alone
+ * exceeds the budget. */
+DV_API int dv_server_submit(dv_server* s, const dv_body_desc* bodies, int32_t nb,
+                            const dv_params* params, int32_t nsteps, int64_t* id);
+/* One round; *busy = 0 when nothing is resident or pending after it. */
+DV_API int dv_server_round(dv_server* s, int32_t* busy);
+/* Finished requests since the last poll (up to cap; *n = how many written). */
+DV_API int dv_server_poll(dv_server* s, dv_request_result* out, int32_t cap, int32_t* n);
+/* Final positions / velocities of a finished request (keep_states); releases them. */
+DV_API int dv_server_result_state(dv_server* s, int64_t id, double* p, double* v);
+DV_API int dv_server_get_stats(dv_server* s, dv_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,8 @@ def test_defaults_are_reference_defaults(native):
 
 def test_invalid_arguments_rejected_before_device_use(native):
     L = native.lib()
-    arr, nb = native.body_array(np.zeros((1, 3)), np.zeros((1, 3)), [1.0], [[0.1, 0, 0]], [0], [-1])
+    arr, nb, _rec = native.body_array(np.zeros((1, 3)), np.zeros((1, 3)), [1.0], [[0.1, 0, 0]], [0],
+                                      [-1])
     out = C.c_void_p()
     p = native.Params()
     L.dv_params_default(C.byref(p))

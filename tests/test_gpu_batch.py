@@ -1,0 +1,127 @@
+"""Batched scenes on the GPU: one collision pipeline and one persistent solve
+kernel step many scenes together, and every scene's results are bit-identical
+to the same scene stepped alone (plain path) and to the CPU oracle, whatever
+the launch shape, with or without CUDA-graph replay."""
+import numpy as np
+import pytest
+
+from dvide_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix():
+    """Scenes of different sizes, parameters and contact regimes: settling
+    boxes, clusters (with and without warm start / friction), a ball on the
+    ground, and a free-falling sphere with no contact at all."""
+    rng = np.random.default_rng(7)
+    out = [
+        scenes.random_cluster(0, n=40),
+        scenes.settling_box(n_side=4, max_iterations=200),
+        scenes.random_cluster(5, n=27, mu=0.0),
+        scenes.ball_on_ground(h=1e-3),
+        scenes.random_cluster(11, n=30, warm_start=0),
+        scenes.lattice_container(rng, 300, max_iterations=300),
+        scenes.random_cluster(3, n=60, mu=0.45),
+    ]
+    free = scenes.ball_on_ground(h=1e-3)
+    free.pos[1, 1] = 50.0  # far above the box: no contact for many steps
+    out.append(free)
+    return out
+
+
+def _states_alone(native, scs, steps, precision=0):
+    res = []
+    for sc in scs:
+        g = native.NativeScene.from_scene(sc, precision=precision)
+        g.step(steps)
+        p, v = g.state()
+        res.append((p, v, g.gamma(), g.stats()))
+        g.close()
+    return res
+
+
+def test_batch_bit_identical_to_scenes_alone(native):
+    scs = _mix()
+    steps = 25
+    alone = _states_alone(native, scs, steps)
+    b = native.NativeBatch(scs)
+    b.step(steps)
+    st = b.scene_stats()
+    for i, (p, v, g, s) in enumerate(alone):
+        pb, vb = b.state(i)
+        assert np.array_equal(pb, p) and np.array_equal(vb, v), i
+        assert np.array_equal(b.gamma(i), g), i
+        assert st[i]["num_contacts"] == s["num_contacts"], i
+        assert st[i]["iterations"] == s["iterations"], i
+        assert st[i]["residual"] == s["residual"], i
+    # the free-falling sphere never touched anything
+    assert st[-1]["num_contacts"] == 0
+
+
+def test_batch_matches_oracle(native, oracle_mod):
+    scs = _mix()[:4]
+    steps = 15
+    b = native.NativeBatch(scs)
+    b.step(steps)
+    for i, sc in enumerate(scs):
+        o = oracle_mod.OracleScene(sc)
+        o.step(steps)
+        po, vo = o.state()
+        pb, vb = b.state(i)
+        assert np.array_equal(pb, po) and np.array_equal(vb, vo), i
+        assert np.array_equal(b.gamma(i), o.gamma()), i
+
+
+def test_batch_launch_shapes_and_graph_identical(native):
+    scs = _mix()
+    steps = 12
+    ref = native.NativeBatch(scs)
+    ref.step(steps)
+    pr, vr = ref.state()
+    shapes = [dict(grid=0, chunk=1, contiguous=0), dict(grid=0, chunk=4, contiguous=0),
+              dict(grid=0, chunk=1, contiguous=1), dict(grid=7, chunk=2, contiguous=0),
+              dict(grid=1, chunk=1, contiguous=0)]
+    for shp in shapes:
+        b = native.NativeBatch(scs)
+        b.set_launch(**shp)
+        b.step(steps)
+        p, v = b.state()
+        assert np.array_equal(p, pr) and np.array_equal(v, vr), shp
+        b.close()
+    g = native.NativeBatch(scs)
+    assert g.set_graph(True) == 0
+    g.step(steps)
+    p, v = g.state()
+    assert np.array_equal(p, pr) and np.array_equal(v, vr)
+
+
+def test_batch_autotune_restores_state(native):
+    scs = _mix()
+    b = native.NativeBatch(scs)
+    b.step(3)
+    p0, v0 = b.state()
+    rep = b.autotune(steps_per_trial=2)
+    assert rep["status"] == 0 and rep["identical"], rep
+    assert len(rep["candidates"]) >= 4
+    p1, v1 = b.state()
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+    # stepping on after tuning equals stepping a fresh batch
+    b.step(4)
+    c = native.NativeBatch(scs)
+    c.step(7)
+    assert np.array_equal(b.state()[0], c.state()[0])
+
+
+def test_batch_history_and_convergence_masks(native):
+    scs = _mix()
+    b = native.NativeBatch(scs)
+    b.step(6)
+    hist, ms = b.history()
+    assert len(hist) == 6 and len(ms) == 6 and all(m > 0 for m in ms)
+    last = hist[-1]
+    iters = [s["iterations"] for s in last if s["num_contacts"] > 0]
+    # scenes converge independently: iteration counts differ across the mix
+    assert len(set(iters)) > 1
+    for s in last:
+        assert s["status"] == 0

@@ -1,0 +1,93 @@
+"""Serving on the GPU: requests that arrive while others run are admitted as
+slots and the HBM budget allow, their steps share the device with the
+resident scenes, and each result is bit-identical to the same scene stepped
+alone (same precision)."""
+import numpy as np
+import pytest
+
+from dvide_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    rng = np.random.default_rng(5)
+    return [
+        (scenes.random_cluster(0, n=40), 9),
+        (scenes.settling_box(n_side=4, max_iterations=200), 14),
+        (scenes.lattice_container(rng, 200, max_iterations=300), 11),
+        (scenes.random_cluster(3, n=27, mu=0.4), 6),
+        (scenes.ball_on_ground(h=1e-3), 12),
+        (scenes.lattice_container(rng, 120, max_iterations=300), 8),
+    ]
+
+
+def _alone(native, sc, nsteps, precision):
+    g = native.NativeScene.from_scene(sc, precision=precision)
+    g.step(nsteps)
+    p, v = g.state()
+    g.close()
+    return p, v
+
+
+def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_round=3):
+    srv = native.NativeServer(precision=precision, hbm_budget_bytes=budget, max_active=max_active,
+                              steps_per_round=steps_per_round)
+    ids = []
+    results = {}
+    max_resident = 0
+    # staggered arrivals: two at once, then one per round, then the rest together
+    arrivals = [[0, 1], [2], [], [3], [4, 5]]
+    busy = True
+    r = 0
+    while busy or r < len(arrivals):
+        if r < len(arrivals):
+            for i in arrivals[r]:
+                ids.append((i, srv.submit(reqs[i][0], reqs[i][1])))
+        busy = srv.round()
+        max_resident = max(max_resident, srv.stats()["active"])
+        for res in srv.poll():
+            results[res["id"]] = res
+        r += 1
+        assert r < 500
+    states = {i: srv.result_state(rid) for i, rid in ids}
+    st = srv.stats()
+    srv.close()
+    return ids, results, states, st, max_resident
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_served_results_equal_alone(native, precision):
+    reqs = _requests()
+    ids, results, states, st, _ = _serve(native, reqs, precision)
+    assert st["completed"] == len(reqs) and st["pending"] == 0 and st["active"] == 0
+    for i, rid in ids:
+        res = results[rid]
+        assert res["status"] == 0
+        assert res["nsteps"] == reqs[i][1]
+        assert res["t_admit"] >= res["t_submit"] and res["t_done"] >= res["t_admit"]
+        p, v = _alone(native, reqs[i][0], reqs[i][1], precision)
+        ps, vs = states[i]
+        assert np.array_equal(ps, p) and np.array_equal(vs, v), i
+
+
+def test_budget_limits_residency(native):
+    reqs = _requests()
+    nb_max = max(sc.nb for sc, _ in reqs)
+    # room for about two of the larger scenes at a time (about 2.5 kB per body)
+    budget = 2.2 * 2.5e3 * nb_max
+    ids, results, states, st, max_resident = _serve(native, reqs, 1, budget=budget)
+    assert st["completed"] == len(reqs)
+    assert max_resident <= 3
+    for i, rid in ids:
+        p, v = _alone(native, reqs[i][0], reqs[i][1], 1)
+        assert np.array_equal(states[i][0], p), i
+
+
+def test_max_active_one_is_sequential(native):
+    reqs = _requests()[:3]
+    ids, results, states, st, max_resident = _serve(native, reqs, 0, max_active=1)
+    assert max_resident == 1 and st["completed"] == 3
+    order = sorted(results.values(), key=lambda r: r["t_admit"])
+    for a, b in zip(order, order[1:]):
+        assert b["t_admit"] >= a["t_done"]
