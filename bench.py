@@ -157,7 +157,8 @@ def run_reference(args, sc, desc):
     return {"metric": "contact-steps/s", "value": value, "unit": "contact-steps/s",
             "impl": "reference", "n_gpus": 0, "steps": done, "warmup": warm,
             "ms_per_step": 1e3 * dt / max(done, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == N.DV_PREC_FP64 else "f32+f64", "data": "synthetic",
             "config": {"workload": desc},
             "cpu_baseline": {"value": value, "unit": "contact-steps/s", "cores": threads,
                              "kind": "port", "sample": sample},
@@ -341,6 +342,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iterations", type=int, default=None,
                     help="override the APGD iteration cap (profiling runs only)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="precision of the headline workload (fp64 is the plain drop-in)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes line")
     ap.add_argument("--batch-scenes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=100)
@@ -378,7 +381,10 @@ def main():
     if args.max_iterations is not None:
         sc.params["max_iterations"] = args.max_iterations
         desc += f" (maxIter overridden to {args.max_iterations})"
-    g = N.NativeScene.from_scene(sc)
+    prec = N.DV_PREC_MIXED if args.precision == "mixed" else N.DV_PREC_FP64
+    if prec == N.DV_PREC_MIXED:
+        desc = desc.replace("FP64", "mixed precision (FP32 iterates, FP64 sums and update)")
+    g = N.NativeScene.from_scene(sc, precision=prec)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     g.set_stream(stream.cuda_stream)
@@ -456,7 +462,8 @@ def main():
             "metric": "contact-steps/s", "value": contacts_all / t_all, "unit": "contact-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == N.DV_PREC_FP64 else "f32+f64",
             "data": "synthetic (seeded scene, see config)",
             "config": {"workload": desc, "contacts_per_step": float(ncs.mean()),
                        "bodies": nb, "parallelism": f"replicas{world}",

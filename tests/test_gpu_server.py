@@ -43,7 +43,8 @@ def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_rou
     while busy or r < len(arrivals):
         if r < len(arrivals):
             for i in arrivals[r]:
-                ids.append((i, srv.submit(reqs[i][0], reqs[i][1])))
+                if i < len(reqs):
+                    ids.append((i, srv.submit(reqs[i][0], reqs[i][1])))
         busy = srv.round()
         max_resident = max(max_resident, srv.stats()["active"])
         for res in srv.poll():
