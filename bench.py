@@ -12,8 +12,8 @@ collision detection, APGD solve, velocity/position update.
 Our arm: W untimed steps, then K steps timed with CUDA events on the stream
 the library launches on (barrier + synchronize on both sides, max over ranks);
 value = contacts summed over the K steps and all ranks / time.  e2e repeats
-K steps through the host-buffer API (state copied in from pinned memory and
-back out every step).  Under torchrun every rank runs its own replica of the
+the same K steps (same starting state and warm start) through the host-buffer
+API, the state copied in from pinned memory and back out every step.  Under torchrun every rank runs its own replica of the
 scene (no collective on the data path).
 Reference arm (--impl reference): the CPU restatement of the reference's
 algorithm (oracle/, OpenMP over all host cores) on the same state and
@@ -348,10 +348,10 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--batch-timed", type=int, default=40)
-    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--plain-sample", type=int, default=16)
     ap.add_argument("--no-served", action="store_true", help="skip the served line")
     ap.add_argument("--serve-rate", type=float, default=200.0)
-    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--serve-round", type=int, default=4)
     args = ap.parse_args()
@@ -400,6 +400,9 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    # the e2e leg repeats exactly these steps: keep their starting state
+    p_start, v_start = g.state()
+    gamma_start = g.gamma()
     sampler = ClockSampler(local_rank)
     sampler.start()
     barrier()
@@ -421,9 +424,9 @@ def main():
     # end-to-end through the host-buffer API: state in from pinned memory, out every step
     p_host = torch.empty((nb, 3), dtype=torch.float64, pin_memory=True).numpy()
     v_host = torch.empty((nb, 3), dtype=torch.float64, pin_memory=True).numpy()
-    p0, v0 = g.state()
-    p_host[:] = p0
-    v_host[:] = v0
+    p_host[:] = p_start
+    v_host[:] = v_start
+    g.set_gamma(gamma_start)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):

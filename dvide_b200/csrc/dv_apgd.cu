@@ -255,13 +255,64 @@ __device__ inline void write_partials(const K& a, int tile, const double (&v)[NQ
   }
 }
 
+// Deferred tile folds.  At the end of a tile each warp folds its partial sums
+// with shuffles (strides 16..1) and parks the eight warp results in shared
+// memory; fold_parked() later completes the 8-warp tree of every parked tile
+// ((w0+w4)+(w2+w6)) + ((w1+w5)+(w3+w7)) -- the order of block_fold_multi --
+// and writes the tile partials.  Warps thus run their copy pipelines across
+// tiles without a CTA barrier per tile.
+constexpr int kMaxDefer = 16;
+struct DeferBuf {
+  double w[kMaxDefer][kNQ + 1][kWarps];  // [slot][quantity][warp]
+  int tile[kMaxDefer];
+  int fail;                              // a warp's copy wait timed out
+};
+
+template <int NQ, bool kMax>
+__device__ inline void park_tile(DeferBuf& B, int slot, int tile, const double (&acc)[NQ], double mx) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const double v = warp_fold(acc[q]);
+    if (lane == 0) B.w[slot][q][warp] = v;
+  }
+  if (kMax) {
+    const double m = warp_max(mx);
+    if (lane == 0) B.w[slot][NQ][warp] = m;
+  }
+  if (threadIdx.x == 0) B.tile[slot] = tile;
+}
+
+// Completes the parked tiles (NQ sums into planes 0..NQ-1, the max into
+// plane kQMax); returns false if a warp's copy wait had timed out.
+template <int NQ, bool kMax, class K>
+__device__ inline bool fold_parked(const K& a, DeferBuf& B, int n) {
+  __syncthreads();
+  const int nq = NQ + (kMax ? 1 : 0);
+  for (int i = threadIdx.x; i < n * nq; i += kThreads) {
+    const int slot = i / nq, q = i - slot * nq;
+    const double* w = B.w[slot][q];
+    double r;
+    if (kMax && q == NQ)
+      r = fmax(fmax(fmax(w[0], w[4]), fmax(w[2], w[6])), fmax(fmax(w[1], w[5]), fmax(w[3], w[7])));
+    else
+      r = ((w[0] + w[4]) + (w[2] + w[6])) + ((w[1] + w[5]) + (w[3] + w[7]));
+    const int plane = (kMax && q == NQ) ? kQMax : q;
+    a.part[(size_t)plane * a.tcap + B.tile[slot]] = r;
+  }
+  __threadfence();
+  __syncthreads();
+  return B.fail == 0;
+}
+
 // Tile arrivals of one segment: a CTA delivers the count of its consecutive
 // tiles of segment s at once (after their partials are written).  True, in
 // every thread, in the CTA whose delivery completes the segment's tiles.
 template <class K>
 __device__ inline bool seg_arrive(const K& a, int s, int n) {
   __shared__ int s_flag;
-  // thread 0 wrote the tiles' partials itself: no CTA barrier needed before it
+  // the tiles' partials were written (and fenced) before the CTA barrier that
+  // ends fold_parked
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned nt = (unsigned)a.sst[s].nt;
@@ -720,6 +771,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   __shared__ unsigned s_mask[kMaskWords];
   __shared__ ProdScalars s_ps;
   __shared__ StepScalars s_st;
+  __shared__ DeferBuf s_def;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   const size_t S = a.S;
   V* wv = reinterpret_cast<V*>(a.wd);
@@ -743,6 +795,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   if (threadIdx.x == 0) {
     sc.s = -1;
     sc.t0 = sc.t1 = 0;
+    s_def.fail = 0;
   }
   __syncthreads();
   const CtlArgs ca{a.part, a.tcap, sizeof(T) != sizeof(double) ? 1 : 0, a.sst, a.seg, a.ew,
@@ -801,6 +854,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // ---- r = D (Minv k) + b; gamma_0 -> G[0]; e = gamma_0 - gamma_hat_0 (= gamma_0 - 1)
   {
     SegRun run;
+    int nslot = 0;
     auto ctl = [&](int s) { ctl_setup(ca, s, scratch); };
     for (int i = 0;; ++i) {
       const int t = cta_tile(a, NT, i);
@@ -808,6 +862,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       locate(a, sc, t);
       const int s = sc.s;
       if (s != run.s) {
+        if (run.n) {
+          fold_parked<1, false>(a, s_def, nslot);
+          nslot = 0;
+        }
         flush_run(a, run, ctl);
         run.s = s;
       }
@@ -844,10 +902,14 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           qv[c] = f_times<T, V>(f, e0, e1, e2);
         }
       }
-      block_fold_multi<1>(acc, scratch);
-      write_partials<1>(a, t, acc);
+      park_tile<1, false>(s_def, nslot, t, acc, 0.0);
       ++run.n;
+      if (++nslot == kMaxDefer) {
+        fold_parked<1, false>(a, s_def, nslot);
+        nslot = 0;
+      }
     }
+    fold_parked<1, false>(a, s_def, nslot);
     flush_run(a, run, ctl);
   }
   if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
@@ -858,6 +920,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // ---- L = ||N e|| / ||e||; q = F gamma_0 for the first N y
   {
     SegRun run;
+    int nslot = 0;
     auto ctl = [&](int s) { ctl_lipschitz(ca, s, scratch); };
     for (int i = 0;; ++i) {
       const int t = cta_tile(a, NT, i);
@@ -865,6 +928,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       locate(a, sc, t);
       const int s = sc.s;
       if (s != run.s) {
+        if (run.n) {
+          fold_parked<1, false>(a, s_def, nslot);
+          nslot = 0;
+        }
         flush_run(a, run, ctl);
         run.s = s;
       }
@@ -883,10 +950,14 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           qv[c] = f_times<T, V>(f, y0, y1, y2);
         }
       }
-      block_fold_multi<1>(acc, scratch);
-      write_partials<1>(a, t, acc);
+      park_tile<1, false>(s_def, nslot, t, acc, 0.0);
       ++run.n;
+      if (++nslot == kMaxDefer) {
+        fold_parked<1, false>(a, s_def, nslot);
+        nslot = 0;
+      }
     }
+    fold_parked<1, false>(a, s_def, nslot);
     flush_run(a, run, ctl);
   }
   // step_count is raised by atomics of other CTAs: read and clear it atomically
@@ -919,6 +990,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     load_mask(a, s_mask, mwords);
     if (__ldcg(&a.ew->step_needed) > 0) {
       SegRun run;
+      int nslot = 0;
       auto ctl = [&](int s) { ctl_step(ca, s, scratch); };
       int cs = -1;
       for (int i = 0;; ++i) {
@@ -953,6 +1025,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         const bool part = s_st.part != 0;
         if (!part) continue;
         if (s != run.s) {
+          if (run.n) {
+            fold_parked<5, false>(a, s_def, nslot);
+            nslot = 0;
+          }
           flush_run(a, run, ctl);
           run.s = s;
         }
@@ -1007,10 +1083,14 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             }
           }
         }
-        block_fold_multi<5>(acc, scratch);
-        write_partials<5>(a, t, acc);
+        park_tile<5, false>(s_def, nslot, t, acc, 0.0);
         ++run.n;
+        if (++nslot == kMaxDefer) {
+          fold_parked<5, false>(a, s_def, nslot);
+          nslot = 0;
+        }
       }
+      fold_parked<5, false>(a, s_def, nslot);
       flush_run(a, run, ctl);
       if (!grid_sync(a, kPhaseStep, NoCtl{})) return;
     }
@@ -1084,6 +1164,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         __syncthreads();
       };
       SegRun run;
+      int nslot = 0;
       auto ctl = [&](int s) { ctl_product(ca, s, scratch); };
 
       double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -1104,6 +1185,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       while (seq >= 0) {
         const int ti = tcur;
         if (sub == 0 && s != run.s) {
+          if (run.n) {
+            if (!fold_parked<7, true>(a, s_def, nslot)) return;
+            nslot = 0;
+          }
           flush_run(a, run, ctl);
           run.s = s;
         }
@@ -1192,16 +1277,17 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           acc[6] = acc[6] + dot3i(y0, y1, y2, r0, r1, r2);
         }
         if (sub == kItemsPerThread - 1) {
-          if (__syncthreads_or(failed)) return;
-          if (__syncthreads_or(bad) && threadIdx.x == 0) seg_error(a, s, kErrNaN);
-          block_fold_multi<7>(acc, scratch);
-          write_partials<7>(a, ti, acc);
-          double bm = block_max256(mx, scratch);
-          if (threadIdx.x == 0) a.part[(size_t)kQMax * a.tcap + ti] = bm;
+          if (__any_sync(0xffffffffu, bad) && lane == 0) seg_error(a, s, kErrNaN);
+          if (failed && lane == 0) s_def.fail = 1;
+          park_tile<7, true>(s_def, nslot, ti, acc, mx);
           for (int qq = 0; qq < 7; ++qq) acc[qq] = 0.0;
           mx = 0.0;
           bad = false;
           ++run.n;
+          if (++nslot == kMaxDefer) {
+            if (!fold_parked<7, true>(a, s_def, nslot)) return;
+            nslot = 0;
+          }
         }
         seq = nseq;
         tcur = ntile;
@@ -1213,6 +1299,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           sc0 = sc.c0; st0 = sc.t0; snc = sc.nc;
         }
       }
+      if (!fold_parked<7, true>(a, s_def, nslot)) return;
       flush_run(a, run, ctl);
     }
     if (!grid_sync(a, kPhaseProduct, latch)) return;
