@@ -438,17 +438,10 @@ def main():
     hist_e2e = g.history(clear=True)
     contacts_e2e = sum(h["num_contacts"] for h in hist_e2e)
 
-    tot = np.array([contacts, t_local, contacts_e2e, t_e2e], dtype=np.float64)
-    if dist is not None:
-        t = torch.tensor(tot, device="cuda")
-        sums = t.clone()
-        dist.all_reduce(sums, op=dist.ReduceOp.SUM)
-        maxs = t.clone()
-        dist.all_reduce(maxs, op=dist.ReduceOp.MAX)
-        contacts_all, t_all = sums[0].item(), maxs[1].item()
-        contacts_e2e_all, t_e2e_all = sums[2].item(), maxs[3].item()
-    else:
-        contacts_all, t_all, contacts_e2e_all, t_e2e_all = tot.tolist()
+    from dvide_b200 import replicas
+    contacts_all, t_all = replicas.combine_timed_region(dist, contacts, t_local, device="cuda")
+    contacts_e2e_all, t_e2e_all = replicas.combine_timed_region(dist, contacts_e2e, t_e2e,
+                                                                device="cuda")
 
     if rank == 0:
         peak, peak_kind = _peaks()
