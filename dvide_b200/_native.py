@@ -88,7 +88,7 @@ class SceneStats(C.Structure):
 
 class TuneCandidate(C.Structure):
     _fields_ = [("grid", C.c_int32), ("chunk", C.c_int32), ("contiguous", C.c_int32),
-                ("ms_per_step", C.c_float)]
+                ("blocks_per_sm", C.c_int32), ("ms_per_step", C.c_float)]
 
 
 class TuneReport(C.Structure):
@@ -99,7 +99,7 @@ class TuneReport(C.Structure):
         return {"best": self.best, "identical": bool(self.identical),
                 "steps_per_trial": self.steps_per_trial,
                 "candidates": [{"grid": c.grid, "chunk": c.chunk, "contiguous": c.contiguous,
-                                "ms_per_step": c.ms_per_step}
+                                "blocks_per_sm": c.blocks_per_sm, "ms_per_step": c.ms_per_step}
                                for c in self.cand[:self.num_candidates]]}
 
 
@@ -183,8 +183,8 @@ def lib():
         "dv_batch_step_history": [vp, C.POINTER(SceneStats), C.POINTER(C.c_float), C.c_int32, ip],
         "dv_batch_get_gamma": [vp, C.c_int32, dp, C.c_int32, ip],
         "dv_batch_ccp_violation": [vp, C.c_int32, dp],
-        "dv_batch_set_launch": [vp, C.c_int32, C.c_int32, C.c_int32],
-        "dv_batch_get_launch": [vp, ip, ip, ip, ip],
+        "dv_batch_set_launch": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
+        "dv_batch_get_launch": [vp, ip, ip, ip, ip, ip],
         "dv_batch_set_graph": [vp, C.c_int32],
         "dv_batch_autotune": [vp, C.c_int32, C.POINTER(TuneReport)],
         "dv_server_default_config": [C.POINTER(ServerConfig)],
@@ -520,13 +520,16 @@ class NativeBatch:
         check(lib().dv_batch_ccp_violation(self.h, int(scene), dptr(o)))
         return o
 
-    def set_launch(self, grid=0, chunk=1, contiguous=0):
-        check(lib().dv_batch_set_launch(self.h, int(grid), int(chunk), int(contiguous)))
+    def set_launch(self, grid=0, chunk=1, contiguous=0, blocks_per_sm=2):
+        check(lib().dv_batch_set_launch(self.h, int(grid), int(chunk), int(contiguous),
+                                        int(blocks_per_sm)))
 
     def launch(self):
-        g, c, k, m = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
-        check(lib().dv_batch_get_launch(self.h, C.byref(g), C.byref(c), C.byref(k), C.byref(m)))
-        return {"grid": g.value, "chunk": c.value, "contiguous": k.value, "max_grid": m.value}
+        g, c, k, bps, m = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().dv_batch_get_launch(self.h, C.byref(g), C.byref(c), C.byref(k), C.byref(bps),
+                                        C.byref(m)))
+        return {"grid": g.value, "chunk": c.value, "contiguous": k.value,
+                "blocks_per_sm": bps.value, "max_grid": m.value}
 
     def set_graph(self, on=True):
         return lib().dv_batch_set_graph(self.h, int(bool(on)))

@@ -1380,11 +1380,11 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   }
 }
 
-template <class T>
+template <class T, int MB>
 void prepare_kernel() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_step_solve<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_step_solve<T, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)dyn_smem_bytes<T>());
   done = true;
 }
@@ -1430,39 +1430,46 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   return a;
 }
 
-template <class T>
+template <class T, int MB>
 void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
-  prepare_kernel<T>();
+  prepare_kernel<T, MB>();
   KArgs<T> a = make_kargs<T>(sd, cfg);
   void* params[] = {&a};
-  cudaLaunchCooperativeKernel((const void*)k_step_solve<T, 2>, cfg.grid, kThreads, params,
+  cudaLaunchCooperativeKernel((const void*)k_step_solve<T, MB>, cfg.grid, kThreads, params,
                               dyn_smem_bytes<T>(), st);
+}
+
+template <class T, int MB>
+int max_ctas_of() {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  prepare_kernel<T, MB>();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<T, MB>, kThreads,
+                                                dyn_smem_bytes<T>());
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
 }
 
 }  // namespace
 
-int apgd_max_ctas(int precision) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (precision == DV_PREC_MIXED) {
-    prepare_kernel<float>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<float, 2>, kThreads,
-                                                  dyn_smem_bytes<float>());
-  } else {
-    prepare_kernel<double>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<double, 2>, kThreads,
-                                                  dyn_smem_bytes<double>());
-  }
-  if (per_sm < 1) per_sm = 1;
-  return sms * per_sm;
+// Co-resident CTAs of the solve kernel for a precision and a register budget
+// (blocks_per_sm 2: 128 registers per thread; 3: 80, FP32 iterates only).
+int apgd_max_ctas(int precision, int blocks_per_sm) {
+  if (precision == DV_PREC_MIXED)
+    return blocks_per_sm == 3 ? max_ctas_of<float, 3>() : max_ctas_of<float, 2>();
+  return max_ctas_of<double, 2>();
 }
 
 void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches) {
   cudaMemsetAsync(sd.ew->bar, 0, sizeof(sd.ew->bar), st);
   cudaMemsetAsync(&sd.ew->last_release, 0, sizeof(unsigned long long), st);
-  if (sd.precision == DV_PREC_MIXED) launch_typed<float>(sd, cfg, st);
-  else launch_typed<double>(sd, cfg, st);
+  if (sd.precision == DV_PREC_MIXED) {
+    if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st);
+    else launch_typed<float, 2>(sd, cfg, st);
+  } else {
+    launch_typed<double, 2>(sd, cfg, st);
+  }
   ++*launches;
 }
 

@@ -83,7 +83,7 @@ DV_API int dv_batch_create(const dv_body_desc* bodies, const int32_t* counts, in
   b->counts.assign(counts, counts + nscenes);
   int rc = b->E.init(in, precision);
   if (rc == DV_OK) {
-    b->E.set_launch(b->E.max_ctas(), 1, 0);
+    b->E.set_launch(b->E.max_ctas(), 1, 0, 2);
   } else {
     delete b;
     return rc;
@@ -164,21 +164,23 @@ DV_API int dv_batch_ccp_violation(dv_batch* b, int32_t scene, double* out4) {
   return b->E.ccp_violation(scene, out4);
 }
 
-DV_API int dv_batch_set_launch(dv_batch* b, int32_t grid, int32_t chunk, int32_t contiguous) {
+DV_API int dv_batch_set_launch(dv_batch* b, int32_t grid, int32_t chunk, int32_t contiguous,
+                               int32_t blocks_per_sm) {
   if (!b || chunk < 0) return DV_ERR_ARG;
-  b->E.set_launch(grid, chunk, contiguous);
+  b->E.set_launch(grid, chunk, contiguous, blocks_per_sm);
   if (b->E.graph_on()) return b->E.set_graph(true);
   return DV_OK;
 }
 
 DV_API int dv_batch_get_launch(dv_batch* b, int32_t* grid, int32_t* chunk, int32_t* contiguous,
-                               int32_t* max_grid) {
+                               int32_t* blocks_per_sm, int32_t* max_grid) {
   if (!b) return DV_ERR_ARG;
   SolveConfig c = b->E.launch();
   if (grid) *grid = c.grid;
   if (chunk) *chunk = c.chunk;
   if (contiguous) *contiguous = c.contiguous;
-  if (max_grid) *max_grid = b->E.max_ctas();
+  if (blocks_per_sm) *blocks_per_sm = c.blocks_per_sm;
+  if (max_grid) *max_grid = b->E.max_ctas_for(c.blocks_per_sm);
   return DV_OK;
 }
 
@@ -193,10 +195,17 @@ DV_API int dv_batch_autotune(dv_batch* b, int32_t steps_per_trial, dv_tune_repor
   const bool graph = E.graph_on();
   const int G = E.max_ctas();
   const int sms = std::max(1, G / 2);
-  struct Cand { int grid, chunk, contiguous; };
+  struct Cand { int grid, chunk, contiguous, bps; };
   std::vector<Cand> cands = {
-      {G, 1, 0}, {G, 2, 0}, {G, 4, 0}, {G, 1, 1}, {sms, 1, 0}, {sms, 2, 0}, {sms, 1, 1},
+      {G, 1, 0, 2}, {G, 2, 0, 2}, {G, 4, 0, 2}, {G, 1, 1, 2}, {sms, 1, 0, 2}, {sms, 2, 0, 2},
+      {sms, 1, 1, 2},
   };
+  if (E.precision() == DV_PREC_MIXED) {
+    const int G3 = E.max_ctas_for(3);
+    cands.push_back({G3, 1, 0, 3});
+    cands.push_back({G3, 2, 0, 3});
+    cands.push_back({G3, 1, 1, 3});
+  }
   dv_tune_report rep;
   memset(&rep, 0, sizeof(rep));
   rep.steps_per_trial = steps_per_trial;
@@ -207,7 +216,7 @@ DV_API int dv_batch_autotune(dv_batch* b, int32_t steps_per_trial, dv_tune_repor
   float best_ms = 1e30f;
   int best = 0;
   for (size_t i = 0; i < cands.size() && i < 16; ++i) {
-    E.set_launch(cands[i].grid, cands[i].chunk, cands[i].contiguous);
+    E.set_launch(cands[i].grid, cands[i].chunk, cands[i].contiguous, cands[i].bps);
     if (graph && E.set_graph(true) != DV_OK) E.set_graph(false);
     if ((rc = E.restore()) != DV_OK) return rc;
     if ((rc = E.step(steps_per_trial)) != DV_OK) return rc;
@@ -222,6 +231,7 @@ DV_API int dv_batch_autotune(dv_batch* b, int32_t steps_per_trial, dv_tune_repor
     c.grid = E.launch().grid;
     c.chunk = cands[i].chunk;
     c.contiguous = cands[i].contiguous;
+    c.blocks_per_sm = E.launch().blocks_per_sm;
     c.ms_per_step = ms;
     if (ms < best_ms) {
       best_ms = ms;
@@ -229,7 +239,7 @@ DV_API int dv_batch_autotune(dv_batch* b, int32_t steps_per_trial, dv_tune_repor
     }
   }
   rep.best = best;
-  E.set_launch(cands[best].grid, cands[best].chunk, cands[best].contiguous);
+  E.set_launch(cands[best].grid, cands[best].chunk, cands[best].contiguous, cands[best].bps);
   if (graph) E.set_graph(true);
   if ((rc = E.restore()) != DV_OK) return rc;
   if (out) *out = rep;

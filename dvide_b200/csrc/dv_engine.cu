@@ -195,11 +195,12 @@ int Engine::init(const std::vector<SceneInput>& scenes, int precision) {
   std::vector<SlotSpec> slots(scenes.size());
   for (size_t i = 0; i < scenes.size(); ++i) slots[i].in = scenes[i];
   TRY(reconfigure(slots));
-  max_ctas_ = apgd_max_ctas(precision);
+  max_ctas_ = apgd_max_ctas(precision, 2);
   DV_CUDA_TRY(cudaGetLastError());
   cfg_.grid = std::max(1, std::min(max_ctas_, (d.nb + kThreads - 1) / kThreads));
   cfg_.chunk = 1;
   cfg_.contiguous = 0;
+  cfg_.blocks_per_sm = 2;
   return DV_OK;
 }
 
@@ -523,16 +524,24 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
   return DV_OK;
 }
 
-void Engine::set_launch(int grid, int chunk, int contiguous) {
+int Engine::max_ctas_for(int blocks_per_sm) const {
+  if (blocks_per_sm == 3 && d.precision == DV_PREC_MIXED) return apgd_max_ctas(d.precision, 3);
+  return max_ctas_;
+}
+
+void Engine::set_launch(int grid, int chunk, int contiguous, int blocks_per_sm) {
+  const int bps = (blocks_per_sm == 3 && d.precision == DV_PREC_MIXED) ? 3 : 2;
+  const int mx = max_ctas_for(bps);
   if (grid <= 0) {
     cfg_user_ = false;
-    cfg_.grid = std::max(1, std::min(max_ctas_, (d.nb + kThreads - 1) / kThreads));
+    cfg_.grid = std::max(1, std::min(mx, (d.nb + kThreads - 1) / kThreads));
   } else {
     cfg_user_ = true;
-    cfg_.grid = std::min(grid, max_ctas_);
+    cfg_.grid = std::min(grid, mx);
   }
   cfg_.chunk = std::max(1, chunk);
   cfg_.contiguous = contiguous ? 1 : 0;
+  cfg_.blocks_per_sm = bps;
   drop_graph();
 }
 
@@ -573,7 +582,8 @@ int Engine::set_precision(int precision) {
   if (precision == d.precision) return DV_OK;
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   d.precision = precision;
-  max_ctas_ = apgd_max_ctas(precision);
+  max_ctas_ = apgd_max_ctas(precision, 2);
+  cfg_.blocks_per_sm = 2;
   if (cfg_.grid > max_ctas_) cfg_.grid = max_ctas_;
   drop_graph();
   return DV_OK;

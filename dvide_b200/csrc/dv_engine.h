@@ -67,8 +67,10 @@ class Engine {
   const SegState& seg_state(int s) const { return h_sst_[s]; }
   int sync_state();  // waits and refreshes words()/seg_state()
 
-  // Launch shape of the persistent solve kernel.
-  void set_launch(int grid, int chunk, int contiguous);
+  // Launch shape of the persistent solve kernel (blocks_per_sm 3 only with
+  // FP32 iterates; grid <= 0: one CTA per 256 bodies up to the co-resident maximum).
+  void set_launch(int grid, int chunk, int contiguous, int blocks_per_sm = 2);
+  int max_ctas_for(int blocks_per_sm) const;
   SolveConfig launch() const { return cfg_; }
   int max_ctas() const { return max_ctas_; }
   // CUDA-graph replay of the step (collision + solve); false if capture failed.
@@ -146,7 +148,7 @@ class Engine {
   std::vector<double> time_;
   std::vector<int> time_index_;
   int max_ctas_ = 1;
-  SolveConfig cfg_{1, 1, 0};
+  SolveConfig cfg_{1, 1, 0, 2};
   bool cfg_user_ = false;
   int64_t launches_ = 0;
   // graph

@@ -207,11 +207,12 @@ void collide(SceneDev& sd, cudaStream_t st, int64_t* launches);
 
 // ---- step (dv_apgd.cu) ----
 struct SolveConfig {
-  int grid;        // CTAs of the persistent kernel
-  int chunk;       // tiles a CTA takes at a time (1, 2, 4)
-  int contiguous;  // 1: CTA c takes a contiguous range of tiles; 0: round robin
+  int grid;           // CTAs of the persistent kernel
+  int chunk;          // tiles a CTA takes at a time (1, 2, 4)
+  int contiguous;     // 1: CTA c takes a contiguous range of tiles; 0: round robin
+  int blocks_per_sm;  // register budget: 2 (128 per thread) or 3 (80, FP32 iterates only)
 };
-int apgd_max_ctas(int precision);
+int apgd_max_ctas(int precision, int blocks_per_sm);
 void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches);
 
 }  // namespace dv

@@ -92,7 +92,7 @@ struct dv_server {
       E.reset(new Engine());
       rc = E->init(in, cfg.precision);
       if (rc == DV_OK && user_stream) rc = E->set_stream(user_stream);
-      if (rc == DV_OK) E->set_launch(E->max_ctas(), 1, 0);
+      if (rc == DV_OK) E->set_launch(E->max_ctas(), 1, 0, 2);
     } else {
       rc = E->reconfigure(slots);
     }

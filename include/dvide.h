@@ -206,6 +206,7 @@ typedef struct dv_tune_candidate {
   int32_t grid;              /* CTAs of the persistent solve kernel */
   int32_t chunk;             /* consecutive 512-contact tiles a CTA takes at a time */
   int32_t contiguous;        /* 1: each CTA owns one contiguous tile range (scenes per CTA) */
+  int32_t blocks_per_sm;     /* 2 (128 registers per thread) or 3 (80; DV_PREC_MIXED only) */
   float ms_per_step;         /* measured device time per step */
 } dv_tune_candidate;
 
@@ -236,10 +237,12 @@ DV_API int dv_batch_step_history(dv_batch* b, dv_scene_stats* out, float* step_m
                                  int32_t* nsteps);
 DV_API int dv_batch_get_gamma(dv_batch* b, int32_t scene, double* gamma, int32_t cap, int32_t* n);
 DV_API int dv_batch_ccp_violation(dv_batch* b, int32_t scene, double* out4);
-/* Launch shape of the solve kernel (grid <= 0: default). */
-DV_API int dv_batch_set_launch(dv_batch* b, int32_t grid, int32_t chunk, int32_t contiguous);
+/* Launch shape of the solve kernel (grid <= 0: default; blocks_per_sm 3 is
+ * taken only by DV_PREC_MIXED batches). */
+DV_API int dv_batch_set_launch(dv_batch* b, int32_t grid, int32_t chunk, int32_t contiguous,
+                               int32_t blocks_per_sm);
 DV_API int dv_batch_get_launch(dv_batch* b, int32_t* grid, int32_t* chunk, int32_t* contiguous,
-                               int32_t* max_grid);
+                               int32_t* blocks_per_sm, int32_t* max_grid);
 /* Replay each step from a captured CUDA graph (collision + solve); returns
  * DV_ERR_UNSUPPORTED and keeps stream launches if capture fails. */
 DV_API int dv_batch_set_graph(dv_batch* b, int32_t enable);

@@ -125,3 +125,17 @@ def test_batch_history_and_convergence_masks(native):
     assert len(set(iters)) > 1
     for s in last:
         assert s["status"] == 0
+
+
+def test_mixed_batch_register_budgets_identical(native):
+    """FP32 iterates: the 80-register variant (3 CTAs per SM) and the
+    128-register one give the same bits."""
+    scs = _mix()
+    ref = native.NativeBatch(scs, precision=1)
+    ref.step(10)
+    b = native.NativeBatch(scs, precision=1)
+    b.set_launch(grid=0, chunk=1, contiguous=0, blocks_per_sm=3)
+    assert b.launch()["blocks_per_sm"] == 3
+    b.step(10)
+    assert np.array_equal(b.state()[0], ref.state()[0])
+    assert np.array_equal(b.state()[1], ref.state()[1])
