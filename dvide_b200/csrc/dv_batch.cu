@@ -40,25 +40,7 @@ int copy_state(dv_batch* b, int32_t scene, double* p, double* v, bool upload) {
     b0 = E.seg_b0(scene);
     n = E.seg_nb(scene);
   }
-  if (n == 0) return DV_OK;
-  cudaStream_t st = E.stream();
-  if (upload) {
-    if (p)
-      DV_CUDA_TRY(cudaMemcpy2DAsync(E.d.p4 + b0, sizeof(double4), p, 3 * sizeof(double),
-                                    3 * sizeof(double), n, cudaMemcpyHostToDevice, st));
-    if (v)
-      DV_CUDA_TRY(cudaMemcpy2DAsync(E.d.v4 + b0, sizeof(double4), v, 3 * sizeof(double),
-                                    3 * sizeof(double), n, cudaMemcpyHostToDevice, st));
-  } else {
-    if (p)
-      DV_CUDA_TRY(cudaMemcpy2DAsync(p, 3 * sizeof(double), E.d.p4 + b0, sizeof(double4),
-                                    3 * sizeof(double), n, cudaMemcpyDeviceToHost, st));
-    if (v)
-      DV_CUDA_TRY(cudaMemcpy2DAsync(v, 3 * sizeof(double), E.d.v4 + b0, sizeof(double4),
-                                    3 * sizeof(double), n, cudaMemcpyDeviceToHost, st));
-  }
-  DV_CUDA_TRY(cudaStreamSynchronize(st));
-  return DV_OK;
+  return upload ? E.copy_state_in(b0, n, p, v) : E.copy_state_out(b0, n, p, v);
 }
 
 }  // namespace

@@ -868,6 +868,66 @@ int Engine::set_stop_on_segment_error(bool on) {
   return DV_OK;
 }
 
+namespace {
+__global__ void __launch_bounds__(kThreads) k_pack3(const double4* __restrict__ src, int n,
+                                                   double* __restrict__ dst) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  double4 x = src[i];
+  dst[3 * i] = x.x;
+  dst[3 * i + 1] = x.y;
+  dst[3 * i + 2] = x.z;
+}
+__global__ void __launch_bounds__(kThreads) k_unpack3(const double* __restrict__ src, int n,
+                                                     double4* __restrict__ dst) {
+  int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  dst[i] = make_double4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0);
+}
+}  // namespace
+
+int Engine::copy_state_out(int b0, int n, double* p, double* v) {
+  if (n <= 0) return DV_OK;
+  if (b0 < 0 || b0 + n > d.nb) return DV_ERR_ARG;
+  const size_t need = 3 * (size_t)n * ((p && v) ? 2 : 1);
+  if (need > stage3_cap_) {
+    dfree(stage3_);
+    TRY(dalloc(&stage3_, need));
+    stage3_cap_ = need;
+  }
+  const int g = (n + kThreads - 1) / kThreads;
+  double* sp = stage3_;
+  double* sv = stage3_ + ((p && v) ? 3 * (size_t)n : 0);
+  if (p) k_pack3<<<g, kThreads, 0, st_>>>(d.p4 + b0, n, sp);
+  if (v) k_pack3<<<g, kThreads, 0, st_>>>(d.v4 + b0, n, sv);
+  if (p) DV_CUDA_TRY(cudaMemcpyAsync(p, sp, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st_));
+  if (v) DV_CUDA_TRY(cudaMemcpyAsync(v, sv, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st_));
+  DV_CUDA_TRY(cudaStreamSynchronize(st_));
+  DV_CUDA_TRY(cudaGetLastError());
+  return DV_OK;
+}
+
+int Engine::copy_state_in(int b0, int n, const double* p, const double* v) {
+  if (n <= 0) return DV_OK;
+  if (b0 < 0 || b0 + n > d.nb) return DV_ERR_ARG;
+  const size_t need = 3 * (size_t)n * ((p && v) ? 2 : 1);
+  if (need > stage3_cap_) {
+    dfree(stage3_);
+    TRY(dalloc(&stage3_, need));
+    stage3_cap_ = need;
+  }
+  const int g = (n + kThreads - 1) / kThreads;
+  double* sp = stage3_;
+  double* sv = stage3_ + ((p && v) ? 3 * (size_t)n : 0);
+  if (p) DV_CUDA_TRY(cudaMemcpyAsync(sp, p, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st_));
+  if (v) DV_CUDA_TRY(cudaMemcpyAsync(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st_));
+  if (p) k_unpack3<<<g, kThreads, 0, st_>>>(sp, n, d.p4 + b0);
+  if (v) k_unpack3<<<g, kThreads, 0, st_>>>(sv, n, d.v4 + b0);
+  DV_CUDA_TRY(cudaStreamSynchronize(st_));
+  DV_CUDA_TRY(cudaGetLastError());
+  return DV_OK;
+}
+
 int Engine::snapshot() {
   TRY(sync_words());
   if (!snap_p_ || snap_nb_ != d.nb) {

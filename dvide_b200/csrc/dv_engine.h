@@ -95,6 +95,12 @@ class Engine {
   int set_stop_on_segment_error(bool on);
   int64_t launches() const { return launches_; }
 
+  // Positions / velocities of bodies [b0, b0 + n) as 3 doubles per body,
+  // between host arrays and the device's double4 layout: one contiguous copy
+  // plus a pack/unpack kernel (synchronous).  p or v may be null.
+  int copy_state_out(int b0, int n, double* p, double* v);
+  int copy_state_in(int b0, int n, const double* p, const double* v);
+
   // Download helpers (synchronous).
   int download(void* dst, const void* src, size_t bytes);
   int download_planes(const double* dev, size_t stride, int k, int first, int n,
@@ -177,6 +183,9 @@ class Engine {
   std::vector<int> snap_gsize_;
   std::vector<double> snap_time_;
   std::vector<int> snap_time_index_;
+  // state transfer staging (3 doubles per body)
+  double* stage3_ = nullptr;
+  size_t stage3_cap_ = 0;
   // diagnostics scratch
   double* d_red_ = nullptr;
   size_t d_red_cap_ = 0;

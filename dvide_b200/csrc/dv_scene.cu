@@ -160,32 +160,12 @@ DV_API int dv_collide(dv_scene* s) {
 
 DV_API int dv_get_state(dv_scene* s, double* p, double* v) {
   if (!s) return DV_ERR_ARG;
-  Engine& E = s->E;
-  int nb = E.d.nb;
-  cudaStream_t st = E.stream();
-  if (p)
-    DV_CUDA_TRY(cudaMemcpy2DAsync(p, 3 * sizeof(double), E.d.p4, sizeof(double4), 3 * sizeof(double),
-                                  nb, cudaMemcpyDeviceToHost, st));
-  if (v)
-    DV_CUDA_TRY(cudaMemcpy2DAsync(v, 3 * sizeof(double), E.d.v4, sizeof(double4), 3 * sizeof(double),
-                                  nb, cudaMemcpyDeviceToHost, st));
-  DV_CUDA_TRY(cudaStreamSynchronize(st));
-  return DV_OK;
+  return s->E.copy_state_out(0, s->E.d.nb, p, v);
 }
 
 DV_API int dv_set_state(dv_scene* s, const double* p, const double* v) {
   if (!s) return DV_ERR_ARG;
-  Engine& E = s->E;
-  int nb = E.d.nb;
-  cudaStream_t st = E.stream();
-  if (p)
-    DV_CUDA_TRY(cudaMemcpy2DAsync(E.d.p4, sizeof(double4), p, 3 * sizeof(double), 3 * sizeof(double),
-                                  nb, cudaMemcpyHostToDevice, st));
-  if (v)
-    DV_CUDA_TRY(cudaMemcpy2DAsync(E.d.v4, sizeof(double4), v, 3 * sizeof(double), 3 * sizeof(double),
-                                  nb, cudaMemcpyHostToDevice, st));
-  DV_CUDA_TRY(cudaStreamSynchronize(st));
-  return DV_OK;
+  return s->E.copy_state_in(0, s->E.d.nb, p, v);
 }
 
 DV_API int dv_get_contact_force(dv_scene* s, double* f) {

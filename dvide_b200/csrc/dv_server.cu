@@ -192,13 +192,8 @@ struct dv_server {
       if (cfg.keep_states) {
         const int n = o.nb;
         std::vector<double> p(3 * (size_t)n), v(3 * (size_t)n);
-        const int b0 = E->seg_b0(q.seg);
-        cudaStream_t stv = E->stream();
-        DV_CUDA_TRY(cudaMemcpy2DAsync(p.data(), 3 * sizeof(double), E->d.p4 + b0, sizeof(double4),
-                                      3 * sizeof(double), n, cudaMemcpyDeviceToHost, stv));
-        DV_CUDA_TRY(cudaMemcpy2DAsync(v.data(), 3 * sizeof(double), E->d.v4 + b0, sizeof(double4),
-                                      3 * sizeof(double), n, cudaMemcpyDeviceToHost, stv));
-        DV_CUDA_TRY(cudaStreamSynchronize(stv));
+        int rc3 = E->copy_state_out(E->seg_b0(q.seg), n, p.data(), v.data());
+        if (rc3 != DV_OK) return rc3;
         states[q.id] = {std::move(p), std::move(v)};
       }
       finished.push_back(o);
