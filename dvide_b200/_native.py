@@ -243,6 +243,7 @@ def make_params(p: dict, precision=DV_PREC_FP64) -> Params:
     o.tolerance = float(p.get("tolerance", o.tolerance))
     o.max_iterations = int(p.get("max_iterations", o.max_iterations))
     o.warm_start = int(p.get("warm_start", o.warm_start))
+    o.solver = int(p.get("solver", o.solver))
     o.max_backtracks = int(p.get("max_backtracks", o.max_backtracks))
     o.precision = int(p.get("precision", precision))
     o.verbose = int(p.get("verbose", 0))

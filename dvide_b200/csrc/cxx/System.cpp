@@ -61,9 +61,13 @@ System::System()
 }
 
 System::System(int type) : System() {
-  // System.cu:84-107: 1 = APGD (also the default); the interior-point,
-  // active-set and Jacobi/Gauss-Seidel solvers are not part of this build.
+  // System.cu:77-101: 1 = APGD (also the default), 5 = PGJ; the interior-point,
+  // active-set and Gauss-Seidel solvers are not part of this build.
   solverType = type;
+  if (type == 5) {
+    delete solver;
+    solver = new PGJ(this);
+  }
 }
 
 System::~System() {
@@ -92,6 +96,7 @@ int System::sync_params() {
   P.max_iterations = solver->maxIterations;
   APGD* apgd = dynamic_cast<APGD*>(solver);
   P.warm_start = apgd && apgd->useWarmStarting ? 1 : 0;
+  P.solver = solverType == 5 ? DV_SOLVER_PGJ : DV_SOLVER_APGD;
   P.verbose = solver->verbose ? 1 : 0;
   if (!scene) return DV_ERR_ARG;
   return dv_set_params(scene, &P);
@@ -99,7 +104,7 @@ int System::sync_params() {
 
 int System::initializeSystem() {
   if (solverType < 1 || solverType > 7) solverType = 1;
-  if (solverType != 1) return DV_ERR_UNSUPPORTED;
+  if (solverType != 1 && solverType != 5) return DV_ERR_UNSUPPORTED;
   APGD* apgd = dynamic_cast<APGD*>(solver);
   if (apgd && apgd->useAntiRelaxation) return DV_ERR_UNSUPPORTED;
   std::vector<dv_body_desc> desc(bodies.size());
@@ -127,6 +132,7 @@ int System::initializeSystem() {
   P.tolerance = solver->tolerance;
   P.max_iterations = solver->maxIterations;
   P.warm_start = apgd && apgd->useWarmStarting ? 1 : 0;
+  P.solver = solverType == 5 ? DV_SOLVER_PGJ : DV_SOLVER_APGD;
   if (scene) dv_scene_destroy(scene);
   scene = nullptr;
   int rc = dv_scene_create(desc.data(), (int32_t)desc.size(), &P, &scene);
@@ -260,6 +266,11 @@ int APGD::setup() { return 0; }
 // The APGD iterations run inside System::DoTimeStep's device step; a
 // separate solve() is not exposed by the B200 step and reports unsupported.
 int APGD::solve() { return DV_ERR_UNSUPPORTED; }
+
+// PGJ runs inside the GPU time step (dv_step); like APGD it has no separate
+// solve entry point in this build.
+int PGJ::setup() { return 0; }
+int PGJ::solve() { return DV_ERR_UNSUPPORTED; }
 
 int CollisionDetector::setEnvelope(double e) {
   envelope = e;

@@ -41,568 +41,12 @@
 //
 // Work is split in tiles of 512 contacts (2 per thread) and 256 bodies.
 // Every wait has a time limit.
-#include <stdio.h>
-#include <stdlib.h>
-
-#include "dv_internal.cuh"
+#include "dv_solve.cuh"
 
 namespace dv {
 
 namespace {
 
-constexpr int kNQ = 7;      // partial-sum slots per tile
-constexpr int kQMax = kNQ;  // slot of the per-tile maximum
-constexpr int kWarps = kThreads / 32;
-constexpr int kSub = kThreads;  // contacts per sub-tile
-
-// Phases timed between grid-barrier releases (EngineWords::phase_ns).
-enum Phase : int {
-  kPhaseSetup = 0,     // k, r, Lipschitz estimate
-  kPhaseStep = 1,      // gamma_new = P(y - t g): first iteration or backtrack
-  kPhaseBody = 3,      // body gather w = Minv D^T q
-  kPhaseProduct = 4,   // N gamma_new, objective, residual, look-ahead step
-  kPhaseFinal = 5,     // gamma = gamma_hat, update
-};
-
-template <class T> struct Vec4;
-template <> struct Vec4<double> { using type = double4; };
-template <> struct Vec4<float> { using type = float4; };
-
-template <class T>
-struct KArgs {
-  int nb, nseg;
-  int tcap;           // plane stride of the partials
-  int chunk, contiguous;
-  size_t S;           // plane stride of contact arrays
-  size_t WS;          // plane stride of the warm-start arena
-  double4* p4;
-  double4* v4;
-  double4* k4;
-  const double4* __restrict__ f4;
-  double4* fc4;
-  double4* wd;        // body vector, double4 (setup); reinterpreted as Vec4<T> in iterations
-  const double* __restrict__ minv;
-  const int* __restrict__ bseg;
-  const uint32_t* __restrict__ ida;
-  const uint32_t* __restrict__ idb;
-  const double* __restrict__ F;
-  const float* __restrict__ nf;
-  const double* __restrict__ gap;
-  T* r;
-  const int* __restrict__ inc_start;
-  const uint32_t* __restrict__ inc;
-  T* G[5];
-  T* NG[5];
-  double4* qd;        // contact vector q, double4 (final pass); Vec4<T> in iterations
-  double* gamma;
-  double* part;
-  const SegParams* __restrict__ seg;
-  SegState* sst;
-  const int* __restrict__ tseg;
-  unsigned* donemask;
-  EngineWords* ew;
-};
-
-template <class T>
-struct Frame {
-  T n0, n1, n2, u0, u1, u2, v0, v1, v2;
-};
-
-// System.cu:753-762 in float arithmetic (mixed path).
-__device__ inline void frame_from_normal_f(float n0, float n1, float n2, Frame<float>& f) {
-  float ux, uy, uz;
-  if (n2 != 0.0f) {
-    ux = 1.0f; uy = 0.0f; uz = __fdiv_rn(-n0, n2);
-  } else if (n0 != 0.0f) {
-    ux = __fdiv_rn(-n2, n0); uy = 0.0f; uz = 1.0f;
-  } else {
-    ux = 1.0f; uy = __fdiv_rn(-n0, n1); uz = 0.0f;
-  }
-  float iu = __fdiv_rn(1.0f, __fsqrt_rn(ux * ux + uy * uy + uz * uz));
-  ux *= iu; uy *= iu; uz *= iu;
-  float vx = n1 * uz - n2 * uy, vy = n2 * ux - n0 * uz, vz = n0 * uy - n1 * ux;
-  float iv = __fdiv_rn(1.0f, __fsqrt_rn(vx * vx + vy * vy + vz * vz));
-  f.n0 = n0; f.n1 = n1; f.n2 = n2;
-  f.u0 = ux; f.u1 = uy; f.u2 = uz;
-  f.v0 = vx * iv; f.v1 = vy * iv; f.v2 = vz * iv;
-}
-
-// The FP64 frame, recomputed from the stored normal with the narrowphase's own
-// function (same bits as the stored u, v planes).
-__device__ inline Frame<double> frame_d(double n0, double n1, double n2) {
-  d3 u, v;
-  frame_from_normal(mk3(n0, n1, n2), &u, &v);
-  Frame<double> f;
-  f.n0 = n0; f.n1 = n1; f.n2 = n2;
-  f.u0 = u.x; f.u1 = u.y; f.u2 = u.z;
-  f.v0 = v.x; f.v1 = v.y; f.v2 = v.z;
-  return f;
-}
-
-template <class T> __device__ inline Frame<T> make_frame(T n0, T n1, T n2);
-template <> __device__ inline Frame<double> make_frame<double>(double n0, double n1, double n2) {
-  return frame_d(n0, n1, n2);
-}
-template <> __device__ inline Frame<float> make_frame<float>(float n0, float n1, float n2) {
-  Frame<float> f;
-  frame_from_normal_f(n0, n1, n2, f);
-  return f;
-}
-
-// Normal planes in the solve's precision.
-template <class T> __device__ inline const T* normal_planes(const KArgs<T>& a);
-template <> __device__ inline const double* normal_planes<double>(const KArgs<double>& a) {
-  return a.F;
-}
-template <> __device__ inline const float* normal_planes<float>(const KArgs<float>& a) {
-  return a.nf;
-}
-
-template <class T>
-__device__ inline Frame<T> load_frame(const KArgs<T>& a, int c) {
-  const T* n = normal_planes<T>(a);
-  return make_frame<T>(n[c], n[a.S + c], n[2 * a.S + c]);
-}
-
-template <class T>
-__device__ inline Frame<double> load_frame_fp64(const KArgs<T>& a, int c) {
-  return frame_d(__ldg(a.F + c), __ldg(a.F + a.S + c), __ldg(a.F + 2 * a.S + c));
-}
-
-// q = F x : q_k = (n_k x0 + u_k x1) + v_k x2
-template <class T, class V>
-__device__ inline V f_times(const Frame<T>& f, T x0, T x1, T x2) {
-  V q;
-  q.x = (f.n0 * x0 + f.u0 * x1) + f.v0 * x2;
-  q.y = (f.n1 * x0 + f.u1 * x1) + f.v1 * x2;
-  q.z = (f.n2 * x0 + f.u2 * x1) + f.v2 * x2;
-  q.w = T(0);
-  return q;
-}
-
-// (F^T d)_row = (f_x d_x + f_y d_y) + f_z d_z with d = w_A - w_B
-template <class T, class V>
-__device__ inline void ft_times(const Frame<T>& f, V wa, V wb, T* o0, T* o1, T* o2) {
-  T d0 = wa.x - wb.x, d1 = wa.y - wb.y, d2 = wa.z - wb.z;
-  *o0 = (f.n0 * d0 + f.n1 * d1) + f.n2 * d2;
-  *o1 = (f.u0 * d0 + f.u1 * d1) + f.u2 * d2;
-  *o2 = (f.v0 * d0 + f.v1 * d1) + f.v2 * d2;
-}
-
-// Dot products of the reductions, always in FP64.
-template <class A, class B>
-__device__ inline double dot3i(A a0, A a1, A a2, B b0, B b1, B b2) {
-  return ((double)a0 * (double)b0 + (double)a1 * (double)b1) + (double)a2 * (double)b2;
-}
-
-// Folds NQ values of each thread; thread 0 gets the results.
-template <int NQ>
-__device__ inline void block_fold_multi(double (&v)[NQ], double* scratch) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int qi = 0; qi < NQ; ++qi) v[qi] = warp_fold(v[qi]);
-  __syncthreads();
-  if (lane == 0) {
-#pragma unroll
-    for (int qi = 0; qi < NQ; ++qi) scratch[qi * 8 + warp] = v[qi];
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int qi = 0; qi < NQ; ++qi) {
-      double w = (lane < 8) ? scratch[qi * 8 + lane] : 0.0;
-#pragma unroll
-      for (int off = 4; off >= 1; off >>= 1) w = w + __shfl_down_sync(0xffffffffu, w, off);
-      v[qi] = w;
-    }
-  }
-  __syncthreads();
-}
-
-// Segment controller side: folds the segment's per-tile partials of NQ
-// quantities in the fixed order (slot j sums the segment's tiles j, j+256,
-// ...; then the 256-slot tree).
-template <int NQ, class K>
-__device__ inline void fold_tiles(const K& a, int t0, int nt, double (&out)[NQ], double* scratch) {
-  double v[NQ];
-#pragma unroll
-  for (int qi = 0; qi < NQ; ++qi) {
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < nt; t += kThreads)
-      acc = acc + __ldcg(a.part + (size_t)qi * a.tcap + t0 + t);
-    v[qi] = acc;
-  }
-  block_fold_multi<NQ>(v, scratch);
-#pragma unroll
-  for (int qi = 0; qi < NQ; ++qi) out[qi] = v[qi];
-}
-
-template <class K>
-__device__ inline double fold_tiles_max(const K& a, int t0, int nt, double* scratch) {
-  double m = 0.0;
-  for (int t = threadIdx.x; t < nt; t += kThreads)
-    m = fmax(m, __ldcg(a.part + (size_t)kQMax * a.tcap + t0 + t));
-  double r = block_max256(m, scratch);
-  __syncthreads();
-  return r;
-}
-
-template <int NQ, class K>
-__device__ inline void write_partials(const K& a, int tile, const double (&v)[NQ]) {
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int qi = 0; qi < NQ; ++qi) a.part[(size_t)qi * a.tcap + tile] = v[qi];
-  }
-}
-
-// Deferred tile folds.  At the end of a tile each warp folds its partial sums
-// with shuffles (strides 16..1) and parks the eight warp results in shared
-// memory; fold_parked() later completes the 8-warp tree of every parked tile
-// ((w0+w4)+(w2+w6)) + ((w1+w5)+(w3+w7)) -- the order of block_fold_multi --
-// and writes the tile partials.  Warps thus run their copy pipelines across
-// tiles without a CTA barrier per tile.
-constexpr int kMaxDefer = 16;
-struct DeferBuf {
-  double w[kMaxDefer][kNQ + 1][kWarps];  // [slot][quantity][warp]
-  int tile[kMaxDefer];
-  int fail;                              // a warp's copy wait timed out
-};
-
-template <int NQ, bool kMax>
-__device__ inline void park_tile(DeferBuf& B, int slot, int tile, const double (&acc)[NQ], double mx) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    const double v = warp_fold(acc[q]);
-    if (lane == 0) B.w[slot][q][warp] = v;
-  }
-  if (kMax) {
-    const double m = warp_max(mx);
-    if (lane == 0) B.w[slot][NQ][warp] = m;
-  }
-  if (threadIdx.x == 0) B.tile[slot] = tile;
-}
-
-// Completes the parked tiles (NQ sums into planes 0..NQ-1, the max into
-// plane kQMax); returns false if a warp's copy wait had timed out.
-template <int NQ, bool kMax, class K>
-__device__ inline bool fold_parked(const K& a, DeferBuf& B, int n) {
-  __syncthreads();
-  const int nq = NQ + (kMax ? 1 : 0);
-  for (int i = threadIdx.x; i < n * nq; i += kThreads) {
-    const int slot = i / nq, q = i - slot * nq;
-    const double* w = B.w[slot][q];
-    double r;
-    if (kMax && q == NQ)
-      r = fmax(fmax(fmax(w[0], w[4]), fmax(w[2], w[6])), fmax(fmax(w[1], w[5]), fmax(w[3], w[7])));
-    else
-      r = ((w[0] + w[4]) + (w[2] + w[6])) + ((w[1] + w[5]) + (w[3] + w[7]));
-    const int plane = (kMax && q == NQ) ? kQMax : q;
-    a.part[(size_t)plane * a.tcap + B.tile[slot]] = r;
-  }
-  __threadfence();
-  __syncthreads();
-  return B.fail == 0;
-}
-
-// Tile arrivals of one segment: a CTA delivers the count of its consecutive
-// tiles of segment s at once (after their partials are written).  True, in
-// every thread, in the CTA whose delivery completes the segment's tiles.
-template <class K>
-__device__ inline bool seg_arrive(const K& a, int s, int n) {
-  __shared__ int s_flag;
-  // the tiles' partials were written (and fenced) before the CTA barrier that
-  // ends fold_parked
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const unsigned nt = (unsigned)a.sst[s].nt;
-    unsigned old = atom_add_acq_rel(&a.sst[s].arrive, (unsigned)n);
-    int last = (old + (unsigned)n == nt);
-    if (last) a.sst[s].arrive = 0u;  // the next pass starts after a grid barrier
-    s_flag = last;
-  }
-  __syncthreads();
-  const bool last = s_flag != 0;
-  if (last) __threadfence();
-  return last;
-}
-
-// The segment of a tile and its ranges, cached per CTA for the whole kernel
-// (they do not change during a step): tiles of the cached segment need no
-// loads to find their contacts.
-struct SegCache {
-  int s;
-  int t0, t1;   // tiles [t0, t1)
-  int c0, nc;   // contacts [c0, c0 + nc)
-  int gsize;
-};
-
-// c is in shared memory; every thread of the CTA calls this with the same t.
-template <class K>
-__device__ inline void locate(const K& a, SegCache& c, int t) {
-  if (t >= c.t0 && t < c.t1) return;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int s = a.tseg[t];
-    const SegState& X = a.sst[s];
-    c.s = s;
-    c.t0 = X.t0;
-    c.t1 = X.t0 + X.nt;
-    c.c0 = X.c0;
-    c.nc = X.nc;
-    c.gsize = X.gsize;
-  }
-  __syncthreads();
-}
-
-struct SegRun {
-  int s = -1;  // segment of the current run of tiles
-  int n = 0;   // tiles of it processed since the last delivery
-};
-
-// Delivers the run's arrivals; the CTA that completes the segment runs ctl(s).
-template <class K, class Fn>
-__device__ inline void flush_run(const K& a, SegRun& run, Fn ctl) {
-  if (run.n == 0) return;
-  const int s = run.s, n = run.n;
-  run.n = 0;
-  if (seg_arrive(a, s, n)) ctl(s);
-}
-
-// Grid barrier.  The last CTA to arrive runs `ctl_fn` (all its threads),
-// then releases the generation word.  Returns false after a timeout or an
-// error raised by another CTA; the caller then leaves the kernel.
-template <class K, class Fn>
-__device__ inline bool grid_sync(const K& a, int phase, Fn ctl_fn) {
-  __shared__ unsigned s_last, s_target;
-  __shared__ int s_fail;
-  unsigned* bar = a.ew->bar;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned ticket = atom_add_acq_rel(&bar[0], 1u);
-    s_target = ticket / gridDim.x + 1u;
-    s_last = (ticket % gridDim.x) == gridDim.x - 1u;
-    s_fail = 0;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    ctl_fn();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      // written by whichever CTA arrives last: no L1-cached copies
-      volatile EngineWords* E = a.ew;
-      unsigned long long now = global_ns();
-      if (E->last_release) {
-        E->phase_ns[phase] += now - E->last_release;
-        E->phase_count[phase] += 1;
-      }
-      E->last_release = now;
-      __threadfence();
-      st_release(&bar[1], s_target);
-    }
-  } else if (threadIdx.x == 0) {
-    uint64_t t0 = global_ns();
-    unsigned polls = 0;
-    while (ld_acquire(&bar[1]) < s_target) {
-      __nanosleep(20);
-      if ((++polls & 1023u) == 0u) {
-        if (ld_acquire(&a.ew->err) & (kErrBarrierTimeout | kErrCopyTimeout)) {
-          s_fail = 1;
-          break;
-        }
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
-          atomicOr(&a.ew->err, kErrBarrierTimeout);
-          s_fail = 1;
-          break;
-        }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return !s_fail;
-}
-
-struct NoCtl {
-  __device__ void operator()() const {}
-};
-
-// Tile i of this CTA's sequence (-1 past the end): round robin in chunks of
-// `chunk` consecutive tiles, or one contiguous range per CTA.
-template <class K>
-__device__ inline int cta_tile(const K& a, int nt, int i) {
-  if (a.contiguous) {
-    long long lo = (long long)nt * blockIdx.x / gridDim.x;
-    long long hi = (long long)nt * (blockIdx.x + 1) / gridDim.x;
-    long long t = lo + i;
-    return t < hi ? (int)t : -1;
-  }
-  const int k = a.chunk;
-  long long t = ((long long)blockIdx.x + (long long)(i / k) * gridDim.x) * k + (i % k);
-  return t < nt ? (int)t : -1;
-}
-
-// Sum of -q over B-side contacts, then +q over A-side contacts, ascending
-// contact order (the flat incidence list); loads are issued in groups of
-// eight, the additions stay in order.
-template <class T, class V, class K>
-__device__ inline V gather_q(const K& a, const V* q, int b) {
-  T ax = T(0), ay = T(0), az = T(0);
-  const int s = __ldg(a.inc_start + b), e = __ldg(a.inc_start + b + 1);
-  for (int i = s; i < e; i += 8) {
-    uint32_t c[8];
-    V qq[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) c[j] = (i + j < e) ? __ldg(a.inc + i + j) : 0u;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (i + j < e) {
-        qq[j] = q[c[j] & 0x7fffffffu];
-      } else {
-        qq[j].x = T(0); qq[j].y = T(0); qq[j].z = T(0); qq[j].w = T(0);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (i + j < e) {
-        if (c[j] & 0x80000000u) {
-          ax = ax - qq[j].x; ay = ay - qq[j].y; az = az - qq[j].z;
-        } else {
-          ax = ax + qq[j].x; ay = ay + qq[j].y; az = az + qq[j].z;
-        }
-      }
-    }
-  }
-  V r;
-  r.x = ax; r.y = ay; r.z = az; r.w = T(0);
-  return r;
-}
-
-// A solver error of segment s; with stop_on_seg_err it also stops the steps
-// that follow (every kernel checks EngineWords::err first).
-template <class K>
-__device__ inline void seg_error(const K& a, int s, unsigned bit) {
-  atomicOr(&a.sst[s].err, bit);
-  if (a.ew->stop_on_seg_err) atomicOr(&a.ew->err, bit);
-}
-
-// Done mask: bit s set when segment s is not iterating.  Each pass starts
-// with a copy in shared memory (segments beyond kMaskWords * 32 read it from
-// global memory).
-constexpr int kMaskWords = 256;
-
-template <class K>
-__device__ inline void load_mask(const K& a, unsigned* s_mask, int mwords) {
-  if (a.nseg == 1) return;  // a single segment iterates while the loop runs
-  __syncthreads();
-  for (int i = threadIdx.x; i < mwords && i < kMaskWords; i += kThreads)
-    s_mask[i] = __ldcg(a.donemask + i);
-  __syncthreads();
-}
-
-template <class K>
-__device__ inline bool mask_done(const K& a, const unsigned* s_mask, int mwords, int s) {
-  if (a.nseg == 1) return false;
-  const int w = s >> 5;
-  const unsigned m = (w < kMaskWords) ? s_mask[w] : __ldcg(a.donemask + w);
-  return (m >> (s & 31)) & 1u;
-}
-
-// Segment s stops iterating (controller thread).
-template <class K>
-__device__ inline void mark_done(const K& a, int s) {
-  volatile ApgdCtl* C = &a.sst[s].ctl;
-  C->done = 1;
-  atomicOr(a.donemask + (s >> 5), 1u << (s & 31));
-}
-
-// Schur body pass: w_b = minv_b * (D^T x)_b for bodies of iterating
-// segments; fixed bodies keep w = 0.
-template <class T>
-__device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask) {
-  using V = typename Vec4<T>::type;
-  V* w = reinterpret_cast<V*>(a.wd);
-  const V* q = reinterpret_cast<const V*>(a.qd);
-  const int nbt = (a.nb + kThreads - 1) / kThreads;
-  const int mwords = (a.nseg + 31) >> 5;
-  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
-    int b = bt * kThreads + threadIdx.x;
-    if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b)))) {
-      double mi = __ldg(a.minv + b);
-      if (mi != 0.0) {
-        V s = gather_q<T, V>(a, q, b);
-        T m = (T)mi;
-        V o;
-        o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
-        w[b] = o;
-      } else if (sizeof(T) != sizeof(double)) {
-        // the FP32 view of w overlays the FP64 setup values: store the zero
-        V o;
-        o.x = T(0); o.y = T(0); o.z = T(0); o.w = T(0);
-        w[b] = o;
-      }
-    }
-  }
-}
-
-// A buffer holding none of the iterates in use (5 buffers, at most 4 in use).
-__device__ inline int free_slot(int a, int b, int c, int d) {
-  for (int i = 0; i < 5; ++i)
-    if (i != a && i != b && i != c && i != d) return i;
-  return 0;
-}
-
-// ---------------------------------------------------------------------------
-// Shared-memory staging of the look-ahead pass, per warp.  A CTA walks its
-// sub-tiles (256 consecutive contacts, kItemsPerThread per reduction tile) in
-// order; warp w owns contacts [32w, 32w+32) of each sub-tile and two stages of
-// its own.  While the warp computes sub-tile i from one stage, its lane 0 has
-// already issued the bulk copies of sub-tile i+1's plane segments (32 values
-// per plane) into the other stage, completed on the warp's own mbarrier, so
-// warps never wait for each other except at the per-tile reduction.
-// Planes: n (3), gamma_new (3), r (3), gamma_k (3), N gamma_k (3); ids A, B.
-// A segment's contacts start on a multiple of 256, so every copy starts on a
-// 128-byte boundary.
-// ---------------------------------------------------------------------------
-constexpr int kStagePlanes = 15;
-template <class T>
-__host__ __device__ constexpr unsigned warp_stage_bytes() {
-  return (unsigned)kStagePlanes * 32u * (unsigned)sizeof(T) + 2u * 32u * 4u;
-}
-template <class T>
-__host__ __device__ constexpr size_t dyn_smem_bytes() {
-  return (size_t)kWarps * 2 * warp_stage_bytes<T>() + (size_t)kWarps * 2 * 8;
-}
-
-struct Staging {
-  unsigned char* base;  // warp w, stage s at base + (2w + s) * stage_bytes
-  unsigned stage_bytes;
-  uint64_t* bar;        // mbarrier of warp w, stage s: bar[2w + s]
-  unsigned phase;       // bit s: parity the next wait on this warp's stage s expects
-};
-
-// Bounded wait for this warp's stage s; false after a timeout (error recorded).
-template <class K>
-__device__ inline bool wait_warp_stage(const K& a, Staging& st, int s) {
-  const int w = threadIdx.x >> 5;
-  unsigned par = (st.phase >> s) & 1u;
-  uint64_t* bar = st.bar + 2 * w + s;
-  bool ok = mbar_try_wait(bar, par);
-  if (!ok) {
-    uint64_t t0 = global_ns();
-    while (!(ok = mbar_try_wait(bar, par))) {
-      if (global_ns() - t0 > kBarrierTimeoutNs) break;
-    }
-  }
-  st.phase ^= (1u << s);
-  if (!ok) atomicOr(&a.ew->err, kErrCopyTimeout);
-  __syncwarp();
-  return ok;
-}
-
-// Scalars of a segment's product pass.
 // Per-segment scalars of the step and product passes, kept in shared memory
 // (written by thread 0 when the CTA moves to another segment) so that they
 // take no registers in the contact loops.
@@ -1464,7 +908,9 @@ int apgd_max_ctas(int precision, int blocks_per_sm) {
 void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches) {
   cudaMemsetAsync(sd.ew->bar, 0, sizeof(sd.ew->bar), st);
   cudaMemsetAsync(&sd.ew->last_release, 0, sizeof(unsigned long long), st);
-  if (sd.precision == DV_PREC_MIXED) {
+  if (sd.solver == DV_SOLVER_PGJ) {
+    launch_pgj_solve(sd, cfg, st);
+  } else if (sd.precision == DV_PREC_MIXED) {
     if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st);
     else launch_typed<float, 2>(sd, cfg, st);
   } else {

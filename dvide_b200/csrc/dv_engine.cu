@@ -74,7 +74,7 @@ Engine::~Engine() {
 static int check_params(const dv_params& p) {
   if (!(p.h > 0) || !(p.envelope >= 0) || !(p.mu >= 0) || !(p.tolerance >= 0)) return DV_ERR_ARG;
   if (p.max_iterations < 0 || p.max_backtracks < 0) return DV_ERR_ARG;
-  if (p.solver != DV_SOLVER_APGD) return DV_ERR_UNSUPPORTED;
+  if (p.solver != DV_SOLVER_APGD && p.solver != DV_SOLVER_PGJ) return DV_ERR_UNSUPPORTED;
   if (p.precision != DV_PREC_FP64 && p.precision != DV_PREC_MIXED) return DV_ERR_UNSUPPORTED;
   return DV_OK;
 }
@@ -220,6 +220,16 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
   for (const SlotSpec& sl : slots) {
     if (sl.keep >= d.nseg) return DV_ERR_ARG;
     if (sl.keep < 0) TRY(validate_scene(sl.in));
+  }
+  // one solver for every segment of an engine
+  int solver = -1;
+  for (const SlotSpec& sl : slots) {
+    const int sv = sl.keep >= 0 ? P_[sl.keep].solver : sl.in.P.solver;
+    if (solver < 0) solver = sv;
+    if (sv != solver) {
+      dv_set_error_text("the scenes of one batch must use the same solver");
+      return DV_ERR_UNSUPPORTED;
+    }
   }
   if (d.nseg > 0) TRY(sync_words());
 
@@ -490,6 +500,7 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
   // ---- engine dimensions, then the contact buffers (their tile count depends on nseg)
   d.nb = nb2;
   d.nseg = nseg2;
+  d.solver = solver;
   d.n_small = n_small2;
   d.n_large = n_large2;
   d.max_seg_chunks = max_chunks;
@@ -571,6 +582,11 @@ int Engine::set_segment_params(int s, const dv_params& P) {
   G.max_iter = P.max_iterations;
   G.max_bt = P.max_backtracks;
   G.warm = P.warm_start;
+  if (P.solver != P_[s].solver) {
+    if (d.nseg != 1) return DV_ERR_UNSUPPORTED;
+    d.solver = P.solver;
+    drop_graph();
+  }
   P_[s] = P;
   TRY(upload_segments());
   DV_CUDA_TRY(cudaStreamSynchronize(st_));

@@ -74,6 +74,7 @@ struct ApgdCtl {
   double objective;     // objective of the best iterate (APGD.cu:353-354)
   double gdiff, ginv;   // 1 / nc^2 and its reciprocal (APGD.cu:92, 98)
   double L0;
+  double fx;            // PGJ: primal feasibility of the iterate computed last
   double yb;            // beta used for y_k = (1+yb) gamma_k - yb gamma_{k-1}
   int k;                // iteration index
   int mode;             // next contact pass: 0 full iteration, 1 backtrack
@@ -124,6 +125,7 @@ struct SceneDev {
   int nb = 0, nseg = 0;
   int n_small = 0, n_large = 0;
   int precision = DV_PREC_FP64;
+  int solver = DV_SOLVER_APGD;  // every segment of an engine uses the same solver
   // segments
   SegParams* seg = nullptr;     // nseg
   SegState* sst = nullptr;      // nseg
@@ -214,5 +216,8 @@ struct SolveConfig {
 };
 int apgd_max_ctas(int precision, int blocks_per_sm);
 void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches);
+// ---- PGJ (dv_pgj.cu) ----
+int pgj_max_ctas(int precision);
+void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st);
 
 }  // namespace dv

@@ -41,7 +41,8 @@ enum {
 };
 
 enum { DV_PREC_FP64 = 0, DV_PREC_MIXED = 1 };
-enum { DV_SOLVER_APGD = 1 };
+/* System(int solverType) numbering (System.cu:77-101): 1 APGD, 5 PGJ. */
+enum { DV_SOLVER_APGD = 1, DV_SOLVER_PGJ = 5 };
 
 /* One rigid body, as System::initializeSystem flattens it (System.cu:344-424). */
 typedef struct dv_body_desc {

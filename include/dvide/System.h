@@ -10,6 +10,7 @@
 
 #include "../dvide.h"
 #include "APGD.h"
+#include "PGJ.h"
 #include "Body.h"
 #include "CollisionDetector.h"
 #include "Solver.h"
@@ -30,6 +31,7 @@ class DeviceArray {
 
 class System {
   friend class APGD;
+  friend class PGJ;
   friend class CollisionDetector;
   friend class DeviceArray;
 

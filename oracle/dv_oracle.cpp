@@ -763,6 +763,77 @@ void apgd_solve(Scene& S) {
   S.st.status = status;
 }
 
+/* PGJ.cu:152-224 (System(5)): projected Gauss-Jacobi with relaxation
+ * omega = 0.3, lambda = 2/3 (PGJ.cu:14-15).  gamma starts at (1, 0, 0) per
+ * contact (:170, no warm start); B_c = 3 / ((minv_A + minv_B) |F_c|^2) with the
+ * nine frame entries squared and summed n, u, v in order (buildB, :73-89);
+ * each iteration
+ *   gamma_hat = P(gamma - omega B (N gamma + r)),
+ *   gamma = lambda gamma_hat + (1 - lambda) gamma                  (:176-186)
+ * and the residual of the new gamma is max(feasibleX, feasibleY, res3)
+ * (:188-211): feasibleX = max -min(0, mu gamma_n - |gamma_t|), feasibleY =
+ * max -min(0, g_n / mu - |g_t|) with g = N gamma + r (a NaN term counts 0),
+ * res3 = max |g_c . gamma_c|.  The reference computes N gamma of the new
+ * iterate twice for the residual and again at the next iteration; it is one
+ * product here, reused. */
+double pgj_feasible(const double* x, double mu_scale, int nc) {
+  double m = -10e30;
+  for (int c = 0; c < nc; ++c) {
+    const double* g = x + 3 * c;
+    double xn = mu_scale * g[0] - sqrt(g[1] * g[1] + g[2] * g[2]);
+    if (xn != xn) xn = 0.0;
+    m = fmax(m, -fmin(0.0, xn));
+  }
+  return m;
+}
+
+void pgj_solve(Scene& S) {
+  const int nc = S.nc;
+  const int64_t n3 = 3 * (int64_t)nc;
+  const double omega = 0.3, lambda = 2.0 / 3.0, mu = S.P.mu;
+  std::vector<double> g(n3), Ng(n3), gh(n3), T(n3), Bc(nc), bt;
+  for (int c = 0; c < nc; ++c) {
+    g[3 * c] = 1.0;
+    g[3 * c + 1] = 0.0;
+    g[3 * c + 2] = 0.0;
+    const double* F = &S.F[9 * (size_t)c];
+    double sum = F[0] * F[0];
+    for (int k = 1; k < 9; ++k) sum = sum + F[k] * F[k];
+    const double ma = S.minv[3 * (size_t)S.A[c]], mb = S.minv[3 * (size_t)S.B[c]];
+    Bc[c] = 3.0 / ((ma + mb) * sum);
+  }
+  schur(S, g.data(), Ng.data(), bt);
+  double residual = 0.0;
+  int k;
+  for (k = 0; k < S.P.max_iterations; ++k) {
+    for (int64_t i = 0; i < n3; ++i) gh[i] = Ng[i] + S.r[i];
+    for (int64_t i = 0; i < n3; ++i) T[i] = Bc[i / 3] * gh[i];
+    for (int64_t i = 0; i < n3; ++i) gh[i] = g[i] + (-omega) * T[i];
+    for (int c = 0; c < nc; ++c) project3(&gh[3 * c], mu);
+    const double oml = 1.0 - lambda;
+    for (int64_t i = 0; i < n3; ++i) g[i] = lambda * gh[i] + oml * g[i];
+    const double fx = pgj_feasible(g.data(), mu, nc);
+    schur(S, g.data(), Ng.data(), bt);
+    for (int64_t i = 0; i < n3; ++i) T[i] = Ng[i] + S.r[i];
+    double res3 = 0.0;
+    for (int c = 0; c < nc; ++c) {
+      const double d = (T[3 * c] * g[3 * c] + T[3 * c + 1] * g[3 * c + 1]) + T[3 * c + 2] * g[3 * c + 2];
+      res3 = fmax(res3, fabs(d));
+    }
+    const double fy = pgj_feasible(T.data(), 1.0 / mu, nc);
+    residual = fmax(fmax(fx, fy), res3);
+    if (residual < S.P.tolerance) break;
+  }
+  if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
+  for (int64_t i = 0; i < n3; ++i) S.gamma[i] = g[i];
+  S.gsize = nc;
+  S.st.iterations = k;
+  S.st.backtracks = 0;
+  S.st.residual = residual;
+  S.st.objective = 0.0;
+  S.st.status = 0;
+}
+
 void build_k(Scene& S) {
   int n = 3 * S.nb;
   double h = S.P.h;
@@ -796,7 +867,8 @@ int do_step(Scene& S) {
   if (S.nc) {
     build_frames(S);
     build_r(S);
-    if (S.P.apgd_mode == 1) apgd_solve(S);
+    if (S.P.solver == 5) pgj_solve(S);
+    else if (S.P.apgd_mode == 1) apgd_solve(S);
     else apgd_solve_fused(S);
     std::vector<double> fc(n);
     apply_DT(S, S.gamma.data(), fc.data());

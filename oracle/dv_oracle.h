@@ -36,6 +36,7 @@ typedef struct or_params {
   int max_backtracks;     /* cap on Lipschitz doublings per iteration (unbounded in the reference) */
   int threads;            /* OpenMP threads, 0 = runtime default */
   int apgd_mode;          /* 0 = fused sequence shared with the GPU, 1 = literal reference sequence */
+  int solver;             /* System(solverType): 1 = APGD (APGD.cu), 5 = PGJ (PGJ.cu) */
 } or_params;
 
 typedef struct or_stats {

@@ -36,7 +36,8 @@ class OrParams(C.Structure):
                 ("envelope", C.c_double), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int), ("warm_start", C.c_int),
                 ("reduce_mode", C.c_int), ("spmv_mode", C.c_int),
-                ("max_backtracks", C.c_int), ("threads", C.c_int), ("apgd_mode", C.c_int)]
+                ("max_backtracks", C.c_int), ("threads", C.c_int), ("apgd_mode", C.c_int),
+                ("solver", C.c_int)]
 
 
 class OrStats(C.Structure):
@@ -116,6 +117,7 @@ def make_params(p: dict, reduce_mode=0, spmv_mode=0, threads=0, apgd_mode=0) -> 
     o.max_backtracks = int(p.get("max_backtracks", 4096))
     o.threads = threads
     o.apgd_mode = apgd_mode
+    o.solver = int(p.get("solver", 1))
     return o
 
 
