@@ -330,7 +330,26 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           a.r[1 * S + c] = (T)(0.0 + d1);
           a.r[2 * S + c] = (T)(0.0 + d2);
           double g0, g1, g2;
-          if (P.warm) {
+          if (P.warm == 2) {
+            // matched: the impulse the same (A, B) pair had at the last solve;
+            // A's earlier contacts are sorted by B, so a binary search finds it
+            const uint32_t ia = __ldg(a.ida + c);
+            const uint32_t bl = __ldg(a.idb + c) - (uint32_t)P.b0;
+            int lo = a.ws[ia], hi = lo + a.wc[ia];
+            if (hi > gsize) hi = gsize;
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (a.wid[(size_t)P.wbase + mid] < bl) lo = mid + 1;
+              else hi = mid;
+            }
+            g0 = 0.0; g1 = 0.0; g2 = 0.0;
+            if (lo < gsize && lo < a.ws[ia] + a.wc[ia] && a.wid[(size_t)P.wbase + lo] == bl) {
+              const size_t wj = (size_t)P.wbase + lo;
+              g0 = a.gamma[0 * a.WS + wj];
+              g1 = a.gamma[1 * a.WS + wj];
+              g2 = a.gamma[2 * a.WS + wj];
+            }
+          } else if (P.warm) {
             const size_t wi = (size_t)P.wbase + k;
             g0 = k < gsize ? a.gamma[0 * a.WS + wi] : 0.0;
             g1 = k < gsize ? a.gamma[1 * a.WS + wi] : 0.0;
@@ -777,6 +796,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           a.gamma[0 * a.WS + wi] = x0;
           a.gamma[1 * a.WS + wi] = x1;
           a.gamma[2 * a.WS + wi] = x2;
+          a.wid[wi] = __ldg(a.idb + c) - (uint32_t)P.b0;
           Frame<double> f = load_frame_fp64(a, c);
           a.qd[c] = f_times<double, double4>(f, x0, x1, x2);
         }
@@ -822,6 +842,15 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     SegState& X = a.sst[s];
     if (a.seg[s].active && X.nc > 0) X.gsize = X.nc;
   }
+  // matched warm start: where each body's A-contacts went in the warm region
+  for (int b = blockIdx.x * kThreads + threadIdx.x; b < a.nb; b += gridDim.x * kThreads) {
+    const int s = __ldg(a.bseg + b);
+    const SegState& X = a.sst[s];
+    if (a.seg[s].active && X.nc > 0) {
+      a.ws[b] = a.cbase[b] + X.delta - X.c0;
+      a.wc[b] = a.cnt_cont[b];
+    }
+  }
 }
 
 template <class T, int MB>
@@ -865,6 +894,11 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   }
   a.qd = sd.q;
   a.gamma = sd.gamma;
+  a.wid = sd.wid;
+  a.ws = sd.ws;
+  a.wc = sd.wc;
+  a.cbase = sd.cbase;
+  a.cnt_cont = sd.cnt_cont;
   a.part = sd.part;
   a.seg = sd.seg;
   a.sst = sd.sst;

@@ -135,19 +135,22 @@ namespace {
 __global__ void __launch_bounds__(kThreads) k_gather_bodies(
     int nb, const int* __restrict__ map, const double4* __restrict__ op, const double4* __restrict__ ov,
     const double4* __restrict__ of, const double4* __restrict__ og, const double* __restrict__ om,
-    const int* __restrict__ ofam, const double4* __restrict__ sp, const double4* __restrict__ sv,
+    const int* __restrict__ ofam, const int* __restrict__ ows, const int* __restrict__ owc,
+    const double4* __restrict__ sp, const double4* __restrict__ sv,
     const double4* __restrict__ sf, const double4* __restrict__ sg, const double* __restrict__ sm,
     const int* __restrict__ sfam, double4* __restrict__ np, double4* __restrict__ nv,
     double4* __restrict__ nf, double4* __restrict__ ng, double* __restrict__ nm,
-    int* __restrict__ nfam) {
+    int* __restrict__ nfam, int* __restrict__ nws, int* __restrict__ nwc) {
   int b = blockIdx.x * kThreads + threadIdx.x;
   if (b >= nb) return;
   int m = map[b];
   if (m >= 0) {
     np[b] = op[m]; nv[b] = ov[m]; nf[b] = of[m]; ng[b] = og[m]; nm[b] = om[m]; nfam[b] = ofam[m];
+    nws[b] = ows[m]; nwc[b] = owc[m];
   } else {
     int k = -(m + 1);
     np[b] = sp[k]; nv[b] = sv[k]; nf[b] = sf[k]; ng[b] = sg[k]; nm[b] = sm[k]; nfam[b] = sfam[k];
+    nws[b] = 0; nwc[b] = 0;
   }
 }
 
@@ -157,12 +160,16 @@ __global__ void __launch_bounds__(kThreads) k_gather_warm(const int* __restrict_
                                                          const int* __restrict__ dst,
                                                          const int* __restrict__ n,
                                                          const double* __restrict__ og, size_t ows,
-                                                         double* __restrict__ ng, size_t nws) {
+                                                         const uint32_t* __restrict__ oid,
+                                                         double* __restrict__ ng, size_t nws,
+                                                         uint32_t* __restrict__ nid) {
   const int s = blockIdx.y;
   const int cnt = n[s];
   if (src[s] < 0) return;
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads)
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads) {
     for (int k = 0; k < 3; ++k) ng[k * nws + dst[s] + i] = og[k * ows + src[s] + i];
+    nid[dst[s] + i] = oid[src[s] + i];
+  }
 }
 
 }  // namespace
@@ -362,6 +369,9 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
   TRY(dalloc(&ng4, nbz));
   TRY(dalloc(&nminv, nbz));
   TRY(dalloc(&nfam, nbz));
+  int *nws = nullptr, *nwc = nullptr;
+  TRY(dalloc(&nws, nbz));
+  TRY(dalloc(&nwc, nbz));
   {
     const size_t ns = std::max<size_t>(sp4.size(), 1);
     double4 *tp = nullptr, *tv = nullptr, *tf = nullptr, *tg = nullptr;
@@ -385,14 +395,17 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
     }
     DV_CUDA_TRY(cudaMemcpyAsync(tmap, map2.data(), sizeof(int) * nbz, cudaMemcpyHostToDevice, st));
     k_gather_bodies<<<(nb2 + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-        nb2, tmap, d.p4, d.v4, d.f4, d.geom4, d.minv, d.family, tp, tv, tf, tg, tm, tfam, np4, nv4,
-        nf4, ng4, nminv, nfam);
+        nb2, tmap, d.p4, d.v4, d.f4, d.geom4, d.minv, d.family, d.ws, d.wc, tp, tv, tf, tg, tm,
+        tfam, np4, nv4, nf4, ng4, nminv, nfam, nws, nwc);
     ++launches_;
     DV_CUDA_TRY(cudaGetLastError());
     // warm-start arena
     double* ng = nullptr;
+    uint32_t* nid = nullptr;
     TRY(dalloc(&ng, 3 * std::max<size_t>(wtotal2, 1)));
+    TRY(dalloc(&nid, std::max<size_t>(wtotal2, 1)));
     DV_CUDA_TRY(cudaMemsetAsync(ng, 0, sizeof(double) * 3 * std::max<size_t>(wtotal2, 1), st));
+    DV_CUDA_TRY(cudaMemsetAsync(nid, 0, sizeof(uint32_t) * std::max<size_t>(wtotal2, 1), st));
     bool any_keep = false;
     for (int s2 = 0; s2 < nseg2; ++s2) any_keep |= (wsrc[s2] >= 0 && gsize2[s2] > 0);
     if (any_keep) {
@@ -410,7 +423,8 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
       DV_CUDA_TRY(cudaMemcpyAsync(tdst, wdst.data(), sizeof(int) * nseg2, cudaMemcpyHostToDevice, st));
       DV_CUDA_TRY(cudaMemcpyAsync(tn, nn.data(), sizeof(int) * nseg2, cudaMemcpyHostToDevice, st));
       dim3 g(std::min((mx + kThreads - 1) / kThreads, 64), nseg2);
-      k_gather_warm<<<g, kThreads, 0, st>>>(tsrc, tdst, tn, d.gamma, d.wtotal, ng, wtotal2);
+      k_gather_warm<<<g, kThreads, 0, st>>>(tsrc, tdst, tn, d.gamma, d.wtotal, d.wid, ng, wtotal2,
+                                             nid);
       ++launches_;
       DV_CUDA_TRY(cudaGetLastError());
       DV_CUDA_TRY(cudaStreamSynchronize(st));
@@ -421,9 +435,12 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
     DV_CUDA_TRY(cudaStreamSynchronize(st));
     dfree(tp); dfree(tv); dfree(tf); dfree(tg); dfree(tm); dfree(tfam); dfree(tmap);
     dfree(d.p4); dfree(d.v4); dfree(d.f4); dfree(d.geom4); dfree(d.minv); dfree(d.family);
-    dfree(d.gamma);
+    dfree(d.gamma); dfree(d.wid); dfree(d.ws); dfree(d.wc);
     d.p4 = np4; d.v4 = nv4; d.f4 = nf4; d.geom4 = ng4; d.minv = nminv; d.family = nfam;
     d.gamma = ng;
+    d.wid = nid;
+    d.ws = nws;
+    d.wc = nwc;
     d.wtotal = wtotal2;
   }
 
@@ -713,18 +730,25 @@ int Engine::grow_warm(double factor, int min_seg_cap, int which) {
   }
   if ((long long)total > 0x7fffffffLL) return DV_ERR_OOM;
   double* g = nullptr;
+  uint32_t* id = nullptr;
   TRY(dalloc(&g, 3 * total));
+  TRY(dalloc(&id, total));
   DV_CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(double) * 3 * total, st_));
+  DV_CUDA_TRY(cudaMemsetAsync(id, 0, sizeof(uint32_t) * total, st_));
   for (int s = 0; s < d.nseg; ++s) {
     int n = std::min(h_sst_[s].gsize, hseg_[s].wcap);
     if (n <= 0) continue;
     for (int k = 0; k < 3; ++k)
       DV_CUDA_TRY(cudaMemcpyAsync(g + k * total + ns[s].wbase, d.gamma + k * d.wtotal + hseg_[s].wbase,
                                   sizeof(double) * n, cudaMemcpyDeviceToDevice, st_));
+    DV_CUDA_TRY(cudaMemcpyAsync(id + ns[s].wbase, d.wid + hseg_[s].wbase, sizeof(uint32_t) * n,
+                                cudaMemcpyDeviceToDevice, st_));
   }
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   dfree(d.gamma);
+  dfree(d.wid);
   d.gamma = g;
+  d.wid = id;
   d.wtotal = total;
   hseg_ = ns;
   TRY(upload_segments());
@@ -869,6 +893,8 @@ int Engine::set_gamma(int s, const double* g, int n) {
       DV_CUDA_TRY(cudaMemcpyAsync(d.gamma + k * d.wtotal + hseg_[s].wbase, h.data() + k * (size_t)n,
                                   sizeof(double) * n, cudaMemcpyHostToDevice, st_));
   DV_CUDA_TRY(cudaMemcpyAsync(&d.sst[s].gsize, &n, sizeof(int), cudaMemcpyHostToDevice, st_));
+  // a positional warm start carries no pairs: the matched lookup finds none
+  DV_CUDA_TRY(cudaMemsetAsync(d.wc + hseg_[s].b0, 0, sizeof(int) * (hseg_[s].b1 - hseg_[s].b0), st_));
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   h_sst_[s].gsize = n;
   return DV_OK;
@@ -949,19 +975,29 @@ int Engine::snapshot() {
   if (!snap_p_ || snap_nb_ != d.nb) {
     dfree(snap_p_);
     dfree(snap_v_);
+    dfree(snap_ws_);
+    dfree(snap_wc_);
     TRY(dalloc(&snap_p_, (size_t)d.nb));
     TRY(dalloc(&snap_v_, (size_t)d.nb));
+    TRY(dalloc(&snap_ws_, (size_t)d.nb));
+    TRY(dalloc(&snap_wc_, (size_t)d.nb));
     snap_nb_ = d.nb;
   }
   if (snap_wtotal_ != d.wtotal) {
     dfree(snap_g_);
+    dfree(snap_id_);
     TRY(dalloc(&snap_g_, 3 * d.wtotal));
+    TRY(dalloc(&snap_id_, d.wtotal));
     snap_wtotal_ = d.wtotal;
   }
   DV_CUDA_TRY(cudaMemcpyAsync(snap_p_, d.p4, sizeof(double4) * d.nb, cudaMemcpyDeviceToDevice, st_));
   DV_CUDA_TRY(cudaMemcpyAsync(snap_v_, d.v4, sizeof(double4) * d.nb, cudaMemcpyDeviceToDevice, st_));
   DV_CUDA_TRY(cudaMemcpyAsync(snap_g_, d.gamma, sizeof(double) * 3 * d.wtotal,
                               cudaMemcpyDeviceToDevice, st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(snap_id_, d.wid, sizeof(uint32_t) * d.wtotal, cudaMemcpyDeviceToDevice,
+                              st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(snap_ws_, d.ws, sizeof(int) * d.nb, cudaMemcpyDeviceToDevice, st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(snap_wc_, d.wc, sizeof(int) * d.nb, cudaMemcpyDeviceToDevice, st_));
   snap_gsize_.resize(d.nseg);
   for (int s = 0; s < d.nseg; ++s) snap_gsize_[s] = h_sst_[s].gsize;
   snap_time_ = time_;
@@ -976,6 +1012,10 @@ int Engine::restore() {
   DV_CUDA_TRY(cudaMemcpyAsync(d.v4, snap_v_, sizeof(double4) * d.nb, cudaMemcpyDeviceToDevice, st_));
   DV_CUDA_TRY(cudaMemcpyAsync(d.gamma, snap_g_, sizeof(double) * 3 * d.wtotal,
                               cudaMemcpyDeviceToDevice, st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(d.wid, snap_id_, sizeof(uint32_t) * d.wtotal, cudaMemcpyDeviceToDevice,
+                              st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(d.ws, snap_ws_, sizeof(int) * d.nb, cudaMemcpyDeviceToDevice, st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(d.wc, snap_wc_, sizeof(int) * d.nb, cudaMemcpyDeviceToDevice, st_));
   DV_CUDA_TRY(cudaMemcpy2DAsync(&d.sst[0].gsize, sizeof(SegState), snap_gsize_.data(), sizeof(int),
                                 sizeof(int), d.nseg, cudaMemcpyHostToDevice, st_));
   time_ = snap_time_;

@@ -178,6 +178,9 @@ class Engine {
   double4* snap_p_ = nullptr;
   double4* snap_v_ = nullptr;
   double* snap_g_ = nullptr;
+  uint32_t* snap_id_ = nullptr;
+  int* snap_ws_ = nullptr;
+  int* snap_wc_ = nullptr;
   size_t snap_wtotal_ = 0;
   int snap_nb_ = 0;
   std::vector<int> snap_gsize_;

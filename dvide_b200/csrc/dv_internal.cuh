@@ -183,6 +183,12 @@ struct SceneDev {
   // wtotal; segment s owns [wbase, wbase + wcap), positional within it
   double* gamma = nullptr;
   size_t wtotal = 0;
+  // matched warm start (warm_start 2): per warm slot the B body of its pair
+  // (segment-relative); per body the segment-relative range of the contacts
+  // where it was A at the last solve
+  uint32_t* wid = nullptr;    // wtotal
+  int* ws = nullptr;          // nb
+  int* wc = nullptr;          // nb
   // host mirrors
   EngineWords* h_ew = nullptr;    // pinned
   SegState* h_sst = nullptr;      // pinned, nseg

@@ -411,6 +411,11 @@ KArgs<T> make_pgj_args(SceneDev& sd, const SolveConfig& cfg) {
   }
   a.qd = sd.q;
   a.gamma = sd.gamma;
+  a.wid = sd.wid;
+  a.ws = sd.ws;
+  a.wc = sd.wc;
+  a.cbase = sd.cbase;
+  a.cnt_cont = sd.cnt_cont;
   a.part = sd.part;
   a.seg = sd.seg;
   a.sst = sd.sst;

@@ -61,6 +61,11 @@ struct KArgs {
   T* NG[5];
   double4* qd;        // contact vector q, double4 (final pass); Vec4<T> in iterations
   double* gamma;
+  uint32_t* wid;      // matched warm start: B of the pair per warm slot (segment-relative)
+  int* ws;            // matched warm start: per body, first warm slot of its A-contacts
+  int* wc;            // ... and their count
+  const int* __restrict__ cbase;     // this step's contact offsets (unpadded) per body
+  const int* __restrict__ cnt_cont;  // this step's contacts with A = body
   double* part;
   const SegParams* __restrict__ seg;
   SegState* sst;

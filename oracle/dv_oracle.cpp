@@ -168,6 +168,8 @@ struct Scene {
   std::vector<double> nP, loc, F, r, bst;
   std::vector<double> gamma;  // warm-start buffer, 3 * capacity
   int gsize = 0;              // contacts currently held (System.cu:185 starts at nb)
+  /* warm_start 2: the (A, B) pairs the held gamma belongs to (sorted) */
+  std::vector<uint32_t> wA, wB;
   /* body incidence, ascending contact order, sign +1 = body A */
   std::vector<int> incStart, incC;
   std::vector<signed char> incS;
@@ -562,9 +564,45 @@ double residual_from(const Scene& S, const double* src, const double* Nsrc, std:
   return nrmmaxv(T.data(), nc, nan_flag);
 }
 
+/* warm_start 2 (an opt-in improvement over the reference, not parity
+ * mode): every contact starts from the impulse the same (A, B) pair had at the
+ * last solve, a new pair from zero. */
+void match_gamma(Scene& S) {
+  const int nc = S.nc;
+  const int64_t n3 = 3 * (int64_t)nc;
+  std::vector<double> g(n3, 0.0);
+  const size_t m = S.wA.size();
+  for (int c = 0; c < nc; ++c) {
+    size_t lo = 0, hi = m;
+    const uint32_t a = S.A[c], b = S.B[c];
+    while (lo < hi) {  // first held pair >= (a, b)
+      const size_t mid = (lo + hi) / 2;
+      if (S.wA[mid] < a || (S.wA[mid] == a && S.wB[mid] < b)) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < m && S.wA[lo] == a && S.wB[lo] == b && (int64_t)lo < S.gsize)
+      for (int k = 0; k < 3; ++k) g[3 * c + k] = S.gamma[3 * lo + k];
+  }
+  if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
+  for (int64_t i = 0; i < n3; ++i) S.gamma[i] = g[i];
+  S.gsize = nc;
+}
+
+// the pairs the solved gamma belongs to
+void keep_pairs(Scene& S) {
+  S.wA = S.A;
+  S.wB = S.B;
+  S.wA.resize(S.nc);
+  S.wB.resize(S.nc);
+}
+
 void resize_gamma(Scene& S) {
   int nc = S.nc;
   int64_t n3 = 3 * (int64_t)nc;
+  if (S.P.warm_start == 2) {
+    match_gamma(S);
+    return;
+  }
   /* thrust resize keeps the prefix and zero-fills growth (APGD.cu:166). */
   if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
   if (S.gsize < nc)
@@ -678,11 +716,7 @@ void apgd_solve_fused(Scene& S) {
 void apgd_solve(Scene& S) {
   int nc = S.nc;
   int64_t n3 = 3 * (int64_t)nc;
-  /* thrust resize keeps the prefix and zero-fills growth (APGD.cu:166). */
-  if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
-  if (S.gsize < nc)
-    for (int64_t i = 3 * (int64_t)S.gsize; i < n3; ++i) S.gamma[i] = 0.0;
-  S.gsize = nc;
+  resize_gamma(S);
   double* gamma = S.gamma.data();
   std::vector<double> gHat(n3, 1.0), gNew(n3), g(n3), y(n3), yNew(n3), T(n3), bt;
   if (!S.P.warm_start)
@@ -870,6 +904,7 @@ int do_step(Scene& S) {
     if (S.P.solver == 5) pgj_solve(S);
     else if (S.P.apgd_mode == 1) apgd_solve(S);
     else apgd_solve_fused(S);
+    keep_pairs(S);
     std::vector<double> fc(n);
     apply_DT(S, S.gamma.data(), fc.data());
     for (int i = 0; i < n; ++i) {
@@ -999,6 +1034,8 @@ int or_set_gamma(void* s, const double* gamma, int ncont) {
   if ((int64_t)S->gamma.size() < 3 * (int64_t)ncont) S->gamma.resize(3 * (size_t)ncont, 0.0);
   if (ncont > 0) memcpy(S->gamma.data(), gamma, sizeof(double) * 3 * (size_t)ncont);
   S->gsize = ncont;
+  S->wA.clear();  // a positional warm start carries no pairs
+  S->wB.clear();
   return 0;
 }
 

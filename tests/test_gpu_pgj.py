@@ -15,7 +15,7 @@ def _pgj(sc, **kw):
 
 
 @pytest.mark.parametrize("make", [lambda: scenes.random_cluster(0, n=40),
-                                  lambda: scenes.settling_box(n_side=4)])
+                                  lambda: scenes.random_cluster(3, n=60, mu=0.45)])
 def test_pgj_teacher_forced_bitexact(native, oracle_mod, make):
     sc = _pgj(make(), max_iterations=3000)
     g = native.NativeScene.from_scene(sc)
