@@ -139,3 +139,20 @@ def test_mixed_batch_register_budgets_identical(native):
     b.step(10)
     assert np.array_equal(b.state()[0], ref.state()[0])
     assert np.array_equal(b.state()[1], ref.state()[1])
+
+
+def test_matched_warm_start_bit_identical_to_oracle_and_alone(native, oracle_mod):
+    scs = _mix()[:5]
+    for sc in scs:
+        sc.params["warm_start"] = 2
+    steps = 20
+    b = native.NativeBatch(scs)
+    b.step(steps)
+    for i, sc in enumerate(scs):
+        o = oracle_mod.OracleScene(sc)
+        o.step(steps)
+        assert np.array_equal(b.state(i)[0], o.state()[0]), i
+        assert np.array_equal(b.state(i)[1], o.state()[1]), i
+        g = native.NativeScene.from_scene(sc)
+        g.step(steps)
+        assert np.array_equal(g.state()[0], o.state()[0]), i
