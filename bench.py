@@ -158,7 +158,7 @@ def run_reference(args, sc, desc):
             "impl": "reference", "n_gpus": 0, "steps": done, "warmup": warm,
             "ms_per_step": 1e3 * dt / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if prec == N.DV_PREC_FP64 else "f32+f64", "data": "synthetic",
+            "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc},
             "cpu_baseline": {"value": value, "unit": "contact-steps/s", "cores": threads,
                              "kind": "port", "sample": sample},
