@@ -287,8 +287,11 @@ class NativeScene:
     def from_scene(cls, scene, precision=DV_PREC_FP64, **overrides):
         p = dict(scene.params)
         p.update(overrides)
-        return cls(scene.pos, scene.vel, scene.mass, scene.geom, scene.fixed, scene.family, p,
-                   precision)
+        g = cls(scene.pos, scene.vel, scene.mass, scene.geom, scene.fixed, scene.family, p,
+                precision)
+        if getattr(scene, "gamma", None) is not None:
+            g.set_gamma(scene.gamma)
+        return g
 
     def close(self):
         if getattr(self, "h", None):

@@ -43,6 +43,9 @@ class Scene:
     family: np.ndarray
     params: dict
     name: str = "scene"
+    # impulses of the previous solve (nc x 3, in that solve's contact order),
+    # the warm start the first step reads: System::gamma_d carried over
+    gamma: np.ndarray | None = None
 
     @property
     def nb(self) -> int:
@@ -50,7 +53,8 @@ class Scene:
 
     def copy(self) -> "Scene":
         return Scene(self.pos.copy(), self.vel.copy(), self.mass.copy(), self.geom.copy(),
-                     self.fixed.copy(), self.family.copy(), dict(self.params), self.name)
+                     self.fixed.copy(), self.family.copy(), dict(self.params), self.name,
+                     None if self.gamma is None else self.gamma.copy())
 
 
 def default_params(**kw) -> dict:

@@ -137,6 +137,8 @@ class OracleScene:
         self.params = make_params(scene.params, reduce_mode, spmv_mode, threads, apgd_mode)
         self.h = L.or_create(self.nb, _dp(a[0]), _dp(a[1]), _dp(a[2]), _dp(a[3]), _ip(a[4]),
                              _ip(a[5]), C.byref(self.params))
+        if getattr(scene, "gamma", None) is not None:
+            self.set_gamma(scene.gamma)
 
     def __del__(self):
         if getattr(self, "h", None):
