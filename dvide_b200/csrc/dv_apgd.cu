@@ -76,10 +76,7 @@ struct CtlArgs {
 __device__ __noinline__ void ctl_setup(CtlArgs a, int s, double* scratch) {
   double sm[1];
   fold_tiles<1>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
-  if (threadIdx.x == 0) {
-    volatile ApgdCtl* C = &a.sst[s].ctl;
-    C->L0 = sqrt(sm[0]);
-  }
+  if (threadIdx.x == 0) a.sst[s].ctl.L0 = sqrt(sm[0]);
 }
 
 __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
@@ -87,19 +84,21 @@ __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
   fold_tiles<1>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
   if (threadIdx.x == 0) {
     const SegParams& P = a.seg[s];
-    volatile ApgdCtl* C = &a.sst[s].ctl;
-    double L = sqrt(sm[0]) / C->L0;
+    ApgdCtl* C = &a.sst[s].ctl;
+    const double L = sqrt(sm[0]) / __ldcg(&C->L0);
     C->L = L;
     C->t = 1.0 / L;
     C->theta = 1.0;
-    double th = 1.0;
-    C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
-    C->beta = th * (1.0 - th) / (th * th + C->theta_new);
+    const double th = 1.0;
+    const double tn = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
+    C->theta_new = tn;
+    C->beta = th * (1.0 - th) / (th * th + tn);
     C->residual = 10e30;
     C->objective = 0.0;
-    double ncd = (double)a.sst[s].nc;
-    C->gdiff = 1.0 / (ncd * ncd);
-    C->ginv = 1.0 / C->gdiff;
+    const double ncd = (double)a.sst[s].nc;
+    const double gd = 1.0 / (ncd * ncd);
+    C->gdiff = gd;
+    C->ginv = 1.0 / gd;
     C->k = 0;
     C->mode = 0;
     C->iterations = 0;
@@ -113,7 +112,9 @@ __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
     C->yb = 0.0;
     C->first = 1;
     C->backtracks = 0;
-    C->obj1 = C->obj2 = C->obj2_base = 0.0;
+    C->obj1 = 0.0;
+    C->obj2 = 0.0;
+    C->obj2_base = 0.0;
     if (P.max_iter <= 0) {
       mark_done(a, s);
     } else {
@@ -128,80 +129,92 @@ __device__ __noinline__ void ctl_step(CtlArgs a, int s, double* scratch) {
   double sm[5];
   fold_tiles<5>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
   if (threadIdx.x == 0) {
-    volatile ApgdCtl* W = &a.sst[s].ctl;
-    if (W->first) W->obj2_base = 0.5 * sm[3] + sm[4];
-    double nr = sqrt(sm[1]);
-    W->obj2 = W->obj2_base + (sm[0] + 0.5 * W->L * (nr * nr));
+    ApgdCtl* W = &a.sst[s].ctl;
+    const int first = __ldcg(&W->first);
+    const double L = __ldcg(&W->L);
+    double ob = __ldcg(&W->obj2_base);
+    if (first) {
+      ob = 0.5 * sm[3] + sm[4];
+      W->obj2_base = ob;
+    }
+    const double nr = sqrt(sm[1]);
+    W->obj2 = ob + (sm[0] + 0.5 * L * (nr * nr));
     W->restart = (sm[2] > 0) ? 1 : 0;
     W->first = 0;
   }
 }
 
 __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
-  double sm[7];
-  fold_tiles<7>(a, a.sst[s].t0, a.sst[s].nt, sm, scratch);
-  double res = fold_tiles_max(a, a.sst[s].t0, a.sst[s].nt, scratch);
+  double sm[7], res;
+  fold_tiles_sm<7, 1>(a, a.sst[s].t0, a.sst[s].nt, sm, &res, kQMax, scratch);
   if (threadIdx.x == 0) {
     const SegParams& P = a.seg[s];
-    volatile ApgdCtl* C = &a.sst[s].ctl;
-    double obj1 = 0.5 * sm[0] + sm[1];
+    ApgdCtl* C = &a.sst[s].ctl;
+    const ApgdCtl c = ctl_read(C);
+    const double obj1 = 0.5 * sm[0] + sm[1];
     C->obj1 = obj1;
     bool finished = false;
+    int k = c.k;
     // APGD.cu:240: obj1 >= obj2 means the step was too long.  With FP32
     // iterates both objectives carry rounding of order 1e-7 |f|; a difference
     // within that noise is not a failed test (else L doubles on noise alone).
-    const double obj2 = C->obj2;
+    const double obj2 = c.obj2;
     const bool fail = a.mixed ? (obj1 - obj2 >= 1e-6 * (fabs(obj1) + fabs(obj2))) : (obj1 >= obj2);
     if (fail) {
       // (10)-(14): double L and retry the projection
-      if (C->backtracks >= P.max_bt) {
+      if (c.backtracks >= P.max_bt) {
         seg_error(a, s, kErrBacktrackCap);
         finished = true;
       } else {
-        C->backtracks += 1;
-        C->L = 2.0 * C->L;
-        C->t = 1.0 / C->L;
+        C->backtracks = c.backtracks + 1;
+        const double L = 2.0 * c.L;
+        C->L = L;
+        C->t = 1.0 / L;
         C->mode = 1;
         atomicAdd(&a.ew->step_count, 1);
       }
     } else {
       C->mode = 0;
-      C->sweeps += 1;
-      int old_best = C->best;
-      if (res < C->residual) {
+      C->sweeps = c.sweeps + 1;
+      double residual = c.residual;
+      if (res < residual) {
+        residual = res;
         C->residual = res;
         C->objective = obj1;
-        C->best = C->nw;
+        C->best = c.nw;
       }
-      if (C->residual < P.tol) {
+      if (residual < P.tol) {
         finished = true;
       } else {
-        double th = C->restart ? 1.0 : C->theta_new;
-        C->yb = C->beta;
-        C->yr = C->restart;
-        C->L = 0.9 * C->L;
-        C->t = 1.0 / C->L;
+        const double th = c.restart ? 1.0 : c.theta_new;
+        C->yb = c.beta;
+        C->yr = c.restart;
+        const double L = 0.9 * c.L;
+        C->L = L;
+        C->t = 1.0 / L;
         C->theta = th;
-        int nw2 = free_slot(C->nw, C->cur, C->prev, old_best);
-        C->prev = C->cur;
-        C->cur = C->nw;
-        C->nw = nw2;
-        C->k += 1;
-        if (C->k >= P.max_iter) {
+        C->prev = c.cur;
+        C->cur = c.nw;
+        C->nw = free_slot(c.nw, c.cur, c.prev, c.best);
+        k += 1;
+        C->k = k;
+        if (k >= P.max_iter) {
           finished = true;
         } else {
-          C->theta_new = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
-          C->beta = th * (1.0 - th) / (th * th + C->theta_new);
+          const double tn = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
+          C->theta_new = tn;
+          C->beta = th * (1.0 - th) / (th * th + tn);
           // the look-ahead step is now iteration k's step
-          C->obj2_base = 0.5 * sm[5] + sm[6];
-          double nr = sqrt(sm[3]);
-          C->obj2 = C->obj2_base + (sm[2] + 0.5 * C->L * (nr * nr));
+          const double ob = 0.5 * sm[5] + sm[6];
+          C->obj2_base = ob;
+          const double nr = sqrt(sm[3]);
+          C->obj2 = ob + (sm[2] + 0.5 * L * (nr * nr));
           C->restart = (sm[4] > 0) ? 1 : 0;
         }
       }
     }
     if (finished) {
-      C->iterations = C->k;
+      C->iterations = k;
       mark_done(a, s);
       atomicSub(&a.ew->active, 1);
     }

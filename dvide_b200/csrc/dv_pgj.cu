@@ -68,21 +68,16 @@ struct PgjCtlArgs {
 // Scene controller after a PGJ contact pass: planes 0..2 hold the tile maxima
 // of feasibleX (of the new iterate), feasibleY and res3 (of the current one).
 __device__ __noinline__ void pgj_ctl(PgjCtlArgs a, int s, double* scratch) {
-  const int t0 = a.sst[s].t0, nt = a.sst[s].nt;
   double m[3];
-  for (int q = 0; q < 3; ++q) {
-    double v = 0.0;
-    for (int t = threadIdx.x; t < nt; t += kThreads) v = fmax(v, __ldcg(a.part + (size_t)q * a.tcap + t0 + t));
-    m[q] = block_max256(v, scratch);
-    __syncthreads();
-  }
+  fold_tiles_sm<0, 3>(a, a.sst[s].t0, a.sst[s].nt, nullptr, m, 0, scratch);
   if (threadIdx.x != 0) return;
-  volatile ApgdCtl* C = &a.sst[s].ctl;
+  ApgdCtl* C = &a.sst[s].ctl;
+  const ApgdCtl c = ctl_read(C);
   const SegParams& P = a.seg[s];
-  const int k = C->k;
+  const int k = c.k;
   bool finished = false;
   if (k >= 1) {
-    const double residual = fmax(fmax(C->fx, m[1]), m[2]);
+    const double residual = fmax(fmax(c.fx, m[1]), m[2]);
     C->residual = residual;
     if (residual < P.tol) {
       finished = true;
@@ -93,15 +88,15 @@ __device__ __noinline__ void pgj_ctl(PgjCtlArgs a, int s, double* scratch) {
     }
   }
   if (finished) {
-    C->best = C->cur;  // gamma_k
+    C->best = c.cur;  // gamma_k
     C->done = 1;
     atomicOr(a.donemask + (s >> 5), 1u << (s & 31));
     atomicSub(&a.ew->active, 1);
   } else {
     C->fx = m[0];
-    C->cur = C->cur ^ 1;
+    C->cur = c.cur ^ 1;
     C->k = k + 1;
-    C->sweeps = C->sweeps + 1;
+    C->sweeps = c.sweeps + 1;
   }
 }
 

@@ -190,32 +190,95 @@ __device__ inline void block_fold_multi(double (&v)[NQ], double* scratch) {
   __syncthreads();
 }
 
-// Segment controller side: folds the segment's per-tile partials of NQ
-// quantities in the fixed order (slot j sums the segment's tiles j, j+256,
-// ...; then the 256-slot tree).
-template <int NQ, class K>
-__device__ inline void fold_tiles(const K& a, int t0, int nt, double (&out)[NQ], double* scratch) {
-  double v[NQ];
+// Folds NS sums (the order of block_fold_multi) and NM maxima of each thread
+// with one exchange through shared memory (NS + NM <= 8); thread 0 gets the
+// results.
+template <int NS, int NM>
+__device__ inline void block_fold_sums_maxes(double* v, double* m, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int qi = 0; qi < NQ; ++qi) {
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < nt; t += kThreads)
-      acc = acc + __ldcg(a.part + (size_t)qi * a.tcap + t0 + t);
-    v[qi] = acc;
+  for (int qi = 0; qi < NS; ++qi) v[qi] = warp_fold(v[qi]);
+#pragma unroll
+  for (int qi = 0; qi < NM; ++qi) m[qi] = warp_max(m[qi]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int qi = 0; qi < NS; ++qi) scratch[qi * 8 + warp] = v[qi];
+#pragma unroll
+    for (int qi = 0; qi < NM; ++qi) scratch[(NS + qi) * 8 + warp] = m[qi];
   }
-  block_fold_multi<NQ>(v, scratch);
+  __syncthreads();
+  if (warp == 0) {
 #pragma unroll
-  for (int qi = 0; qi < NQ; ++qi) out[qi] = v[qi];
+    for (int qi = 0; qi < NS; ++qi) {
+      double w = (lane < 8) ? scratch[qi * 8 + lane] : 0.0;
+#pragma unroll
+      for (int off = 4; off >= 1; off >>= 1) w = w + __shfl_down_sync(0xffffffffu, w, off);
+      v[qi] = w;
+    }
+#pragma unroll
+    for (int qi = 0; qi < NM; ++qi) {
+      double w = (lane < 8) ? scratch[(NS + qi) * 8 + lane] : 0.0;
+#pragma unroll
+      for (int off = 4; off >= 1; off >>= 1) w = fmax(w, __shfl_down_sync(0xffffffffu, w, off));
+      m[qi] = w;
+    }
+  }
+  __syncthreads();
 }
 
-template <class K>
-__device__ inline double fold_tiles_max(const K& a, int t0, int nt, double* scratch) {
-  double m = 0.0;
-  for (int t = threadIdx.x; t < nt; t += kThreads)
-    m = fmax(m, __ldcg(a.part + (size_t)kQMax * a.tcap + t0 + t));
-  double r = block_max256(m, scratch);
-  __syncthreads();
-  return r;
+// Segment controller side: folds the segment's per-tile partials, NS sums
+// (planes 0..NS-1) in the fixed order -- slot j sums the segment's tiles j,
+// j+256, ... in turn, then the 256-slot tree -- and NM maxima (planes
+// mplane0, mplane0+1, ...).  All loads of a chunk of U tiles are in flight
+// before its sums, which keep the slot order: one L2 round trip per chunk.
+template <int NS, int NM, class K>
+__device__ inline void fold_tiles_sm(const K& a, int t0, int nt, double* sum_out, double* max_out,
+                                     int mplane0, double* scratch) {
+  constexpr int U = (NS + NM) <= 2 ? 8 : 4;
+  constexpr int AS = NS > 0 ? NS : 1, AM = NM > 0 ? NM : 1;
+  const double* p = a.part + t0;
+  const size_t tc = (size_t)a.tcap;
+  double sum[AS], mx[AM];
+#pragma unroll
+  for (int qi = 0; qi < AS; ++qi) sum[qi] = 0.0;
+#pragma unroll
+  for (int qi = 0; qi < AM; ++qi) mx[qi] = 0.0;
+  int t = threadIdx.x;
+  for (; t + (U - 1) * kThreads < nt; t += U * kThreads) {
+    double xs[AS][U], xm[AM][U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+#pragma unroll
+      for (int qi = 0; qi < NS; ++qi) xs[qi][u] = __ldcg(p + qi * tc + t + u * kThreads);
+#pragma unroll
+      for (int qi = 0; qi < NM; ++qi)
+        xm[qi][u] = __ldcg(p + (size_t)(mplane0 + qi) * tc + t + u * kThreads);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+#pragma unroll
+      for (int qi = 0; qi < NS; ++qi) sum[qi] = sum[qi] + xs[qi][u];
+#pragma unroll
+      for (int qi = 0; qi < NM; ++qi) mx[qi] = fmax(mx[qi], xm[qi][u]);
+    }
+  }
+  for (; t < nt; t += kThreads) {
+#pragma unroll
+    for (int qi = 0; qi < NS; ++qi) sum[qi] = sum[qi] + __ldcg(p + qi * tc + t);
+#pragma unroll
+    for (int qi = 0; qi < NM; ++qi) mx[qi] = fmax(mx[qi], __ldcg(p + (size_t)(mplane0 + qi) * tc + t));
+  }
+  block_fold_sums_maxes<NS, NM>(sum, mx, scratch);
+#pragma unroll
+  for (int qi = 0; qi < NS; ++qi) sum_out[qi] = sum[qi];
+#pragma unroll
+  for (int qi = 0; qi < NM; ++qi) max_out[qi] = mx[qi];
+}
+
+template <int NQ, class K>
+__device__ inline void fold_tiles(const K& a, int t0, int nt, double (&out)[NQ], double* scratch) {
+  fold_tiles_sm<NQ, 0>(a, t0, nt, out, nullptr, 0, scratch);
 }
 
 template <int NQ, class K>
@@ -362,16 +425,20 @@ __device__ inline bool grid_sync(const K& a, int phase, Fn ctl_fn) {
     ctl_fn();
     __syncthreads();
     if (threadIdx.x == 0) {
-      // written by whichever CTA arrives last: no L1-cached copies
+      const unsigned long long now = global_ns();
+      __threadfence();
+      st_release(&bar[1], s_target);
+      // Phase timers, after the release so that their round trips to L2 are
+      // off the barrier's critical path.  Written by whichever CTA arrives
+      // last (no L1-cached copies); the next barrier's last CTA reads them
+      // only after this CTA's next arrival, which follows in program order.
       volatile EngineWords* E = a.ew;
-      unsigned long long now = global_ns();
-      if (E->last_release) {
-        E->phase_ns[phase] += now - E->last_release;
+      const unsigned long long prev = E->last_release;
+      if (prev) {
+        E->phase_ns[phase] += now - prev;
         E->phase_count[phase] += 1;
       }
       E->last_release = now;
-      __threadfence();
-      st_release(&bar[1], s_target);
     }
   } else if (threadIdx.x == 0) {
     uint64_t t0 = global_ns();
@@ -453,6 +520,25 @@ __device__ inline V gather_q(const K& a, const V* q, int b) {
 
 // A solver error of segment s; with stop_on_seg_err it also stops the steps
 // that follow (every kernel checks EngineWords::err first).
+// A segment's APGD words as its controller finds them: controllers of earlier
+// passes ran on other CTAs, so every field is read through L2, with all the
+// loads in flight together (one round trip instead of one per field).
+__device__ inline ApgdCtl ctl_read(const ApgdCtl* C) {
+  ApgdCtl c;
+  c.L = __ldcg(&C->L); c.t = __ldcg(&C->t); c.theta = __ldcg(&C->theta);
+  c.theta_new = __ldcg(&C->theta_new); c.beta = __ldcg(&C->beta);
+  c.obj1 = __ldcg(&C->obj1); c.obj2 = __ldcg(&C->obj2); c.obj2_base = __ldcg(&C->obj2_base);
+  c.residual = __ldcg(&C->residual); c.objective = __ldcg(&C->objective);
+  c.gdiff = __ldcg(&C->gdiff); c.ginv = __ldcg(&C->ginv); c.L0 = __ldcg(&C->L0);
+  c.fx = __ldcg(&C->fx); c.yb = __ldcg(&C->yb);
+  c.k = __ldcg(&C->k); c.mode = __ldcg(&C->mode); c.done = __ldcg(&C->done);
+  c.restart = __ldcg(&C->restart); c.cur = __ldcg(&C->cur); c.prev = __ldcg(&C->prev);
+  c.nw = __ldcg(&C->nw); c.best = __ldcg(&C->best); c.yr = __ldcg(&C->yr);
+  c.first = __ldcg(&C->first); c.backtracks = __ldcg(&C->backtracks); c.err = __ldcg(&C->err);
+  c.iterations = __ldcg(&C->iterations); c.sweeps = __ldcg(&C->sweeps);
+  return c;
+}
+
 template <class K>
 __device__ inline void seg_error(const K& a, int s, unsigned bit) {
   atomicOr(&a.sst[s].err, bit);
