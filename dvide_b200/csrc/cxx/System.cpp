@@ -95,7 +95,7 @@ int System::sync_params() {
   P.tolerance = solver->tolerance;
   P.max_iterations = solver->maxIterations;
   APGD* apgd = dynamic_cast<APGD*>(solver);
-  P.warm_start = apgd && apgd->useWarmStarting ? 1 : 0;
+  P.warm_start = apgd ? apgd->warmStartMode : 0;
   P.solver = solverType == 5 ? DV_SOLVER_PGJ : DV_SOLVER_APGD;
   P.verbose = solver->verbose ? 1 : 0;
   if (!scene) return DV_ERR_ARG;
@@ -131,7 +131,7 @@ int System::initializeSystem() {
   P.envelope = collisionDetector->envelope;
   P.tolerance = solver->tolerance;
   P.max_iterations = solver->maxIterations;
-  P.warm_start = apgd && apgd->useWarmStarting ? 1 : 0;
+  P.warm_start = apgd ? apgd->warmStartMode : 0;
   P.solver = solverType == 5 ? DV_SOLVER_PGJ : DV_SOLVER_APGD;
   if (scene) dv_scene_destroy(scene);
   scene = nullptr;

@@ -2,7 +2,7 @@
 // (System, Body, APGD; compare models/test_compaction.cu:184-431): 1,000
 // spheres (r = 0.05 m, rho = 2600) on a 10x10x10 lattice in an open box of
 // five fixed boxes, mu = 0.25, h = 1e-3, APGD with warm start.
-// Usage: settle <steps> <solverType> <tolerance> [maxIterations]
+// Usage: settle <steps> <solverType> <tolerance> [maxIterations] [warmStartMode]
 // Prints one line per step: time, contacts, iterations, weight carried by
 // the fixed boxes, and the four CCP violations.
 #include <math.h>
@@ -26,6 +26,7 @@ int main(int argc, char** argv) {
   int solverType = argc > 2 ? atoi(argv[2]) : 1;
   double tolerance = argc > 3 ? atof(argv[3]) : 1e-4;
   int maxIterations = argc > 4 ? atoi(argv[4]) : 1000;
+  int warmStartMode = argc > 5 ? atoi(argv[5]) : 1;
 
   System* sys = new System(solverType);
   sys->setTimeStep(1e-3);
@@ -33,7 +34,7 @@ int main(int argc, char** argv) {
   sys->solver->tolerance = tolerance;
   sys->solver->maxIterations = maxIterations;
   sys->collisionDetector->setBinsPerAxis(make_uint3(10, 10, 10));
-  if (solverType == 1) dynamic_cast<APGD*>(sys->solver)->setWarmStarting(true);
+  if (solverType == 1) dynamic_cast<APGD*>(sys->solver)->setWarmStarting(warmStartMode);
 
   const double t = 0.05, inner = 0.6, H = 0.75;
   double3 c[5] = {make_double3(0, 0, -t), make_double3(-inner - t, 0, H), make_double3(inner + t, 0, H),

@@ -10,18 +10,23 @@ class APGD : public Solver {
   friend class System;
 
  private:
-  bool useWarmStarting;
+  int warmStartMode;  // 0 off, 1 positional (the reference's), 2 matched by contact pair
   bool useAntiRelaxation;
 
  public:
-  explicit APGD(System* sys) : Solver(sys), useWarmStarting(false), useAntiRelaxation(false) {
+  explicit APGD(System* sys) : Solver(sys), warmStartMode(0), useAntiRelaxation(false) {
     tolerance = 1e-4;
     maxIterations = 100000;
     iterations = 0;
   }
-  void setWarmStarting(bool w) { useWarmStarting = w; }
+  // APGD.cuh:62: positional warm start on or off
+  void setWarmStarting(bool w) { warmStartMode = w ? 1 : 0; }
+  // extension: 2 starts each contact from the impulse its (A, B) pair had at
+  // the last solve (a new pair from zero); 0 and 1 as above
+  void setWarmStarting(int mode) { warmStartMode = mode; }
   void setAntiRelaxation(bool a) { useAntiRelaxation = a; }
-  bool getWarmStarting() const { return useWarmStarting; }
+  bool getWarmStarting() const { return warmStartMode != 0; }
+  int getWarmStartMode() const { return warmStartMode; }
   int setup();
   int solve();
 };

@@ -30,3 +30,17 @@ def test_unsupported_solver_type_reports(tmp_path):
                          timeout=120)
     assert out.returncode == 1
     assert "unsupported" in out.stderr
+
+
+@pytest.mark.parametrize("args", [["5", "1e-3", "2000"], ["1", "1e-4", "1000", "2"]],
+                         ids=["pgj", "apgd_matched_warm_start"])
+def test_settle_driver_other_solver_forms(tmp_path, args):
+    out = subprocess.run([DRIVER, "120", *args], cwd=tmp_path, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [l for l in out.stdout.splitlines() if l and l[0].isdigit()]
+    assert len(lines) == 120
+    last = [float(x) for x in lines[-1].split(",")]
+    assert last[1] > 100
+    assert all(np.isfinite(float(x)) for x in lines[-1].split(","))
+
