@@ -63,7 +63,8 @@ class Params(C.Structure):
     _fields_ = [("h", C.c_double), ("mu", C.c_double), ("gravity", C.c_double * 3),
                 ("envelope", C.c_double), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int32), ("warm_start", C.c_int32), ("solver", C.c_int32),
-                ("precision", C.c_int32), ("max_backtracks", C.c_int32), ("verbose", C.c_int32)]
+                ("precision", C.c_int32), ("max_backtracks", C.c_int32), ("verbose", C.c_int32),
+                ("fp64_narrowphase", C.c_int32)]
 
 
 class StepStats(C.Structure):
@@ -247,6 +248,7 @@ def make_params(p: dict, precision=DV_PREC_FP64) -> Params:
     o.max_backtracks = int(p.get("max_backtracks", o.max_backtracks))
     o.precision = int(p.get("precision", precision))
     o.verbose = int(p.get("verbose", 0))
+    o.fp64_narrowphase = int(p.get("fp64_narrowphase", 0))
     return o
 
 

@@ -51,11 +51,11 @@ namespace {
 // (written by thread 0 when the CTA moves to another segment) so that they
 // take no registers in the contact loops.
 struct ProdScalars {
-  int cur, nw, nw2, restart;
+  int cur, nw, nw2, restart, exact;
   double ya, ym, nt2, gd, gA, gB, mu;
 };
 struct StepScalars {
-  int part, first, cur, prev, nw, yr;
+  int part, first, cur, prev, nw, yr, exact;
   double ya, ym, nt, mu;
 };
 
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         int k = k0 + m * kThreads + threadIdx.x;
         if (k < nc) {
           const int c = c0 + k;
-          Frame<double> fd = load_frame_fp64(a, c);
+          Frame<double> fd = load_frame_fp64(a, c, P.exact != 0);
           double4 wa = a.wd[__ldg(a.ida + c)], wb = a.wd[__ldg(a.idb + c)];
           double d0, d1, d2;
           ft_times<double, double4>(fd, wa, wb, &d0, &d1, &d2);
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           a.G[0][0 * S + c] = x0; a.G[0][1 * S + c] = x1; a.G[0][2 * S + c] = x2;
           const T e0 = x0 + T(-1), e1 = x1 + T(-1), e2 = x2 + T(-1);
           acc[0] = acc[0] + dot3i(e0, e1, e2, e0, e1, e2);
-          Frame<T> f = load_frame<T>(a, c);
+          Frame<T> f = load_frame<T>(a, c, P.exact != 0);
           qv[c] = f_times<T, V>(f, e0, e1, e2);
         }
       }
@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         int k = k0 + m * kThreads + threadIdx.x;
         if (k < nc) {
           const int c = c0 + k;
-          Frame<T> f = load_frame<T>(a, c);
+          Frame<T> f = load_frame<T>(a, c, a.seg[s].exact != 0);
           V wa = wv[__ldg(a.ida + c)], wb = wv[__ldg(a.idb + c)];
           T n0, n1, n2;
           ft_times<T, V>(f, wa, wb, &n0, &n1, &n2);
@@ -493,6 +493,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
               s_st.ym = -yb;
               s_st.nt = -__ldcg(&C->t);
               s_st.mu = a.seg[s].mu;
+              s_st.exact = a.seg[s].exact;
             }
             s_st.part = part;
           }
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           int k = k0 + m * kThreads + threadIdx.x;
           if (k < nc) {
             const int c = c0 + k;
-            Frame<T> f = load_frame<T>(a, c);
+            Frame<T> f = load_frame<T>(a, c, s_st.exact != 0);
             T c0v = Gc[0 * S + c], c1v = Gc[1 * S + c], c2v = Gc[2 * S + c];
             T y0, y1, y2, N0, N1, N2;
             if (yr) {
@@ -636,6 +637,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           s_ps.gA = __ldcg(&C->ginv);
           s_ps.gB = -1.0 / gd;
           s_ps.mu = a.seg[s].mu;
+          s_ps.exact = a.seg[s].exact;
         }
         __syncthreads();
       };
@@ -697,7 +699,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
               reinterpret_cast<const T*>(stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes);
           const uint32_t* su = reinterpret_cast<const uint32_t*>(sd + (size_t)kStagePlanes * 32);
           const int j = lane;
-          Frame<T> f = make_frame<T>(sd[0 * 32 + j], sd[1 * 32 + j], sd[2 * 32 + j]);
+          Frame<T> f =
+              make_frame<T>(sd[0 * 32 + j], sd[1 * 32 + j], sd[2 * 32 + j], ps.exact != 0);
           V wa = wv[su[j]], wb = wv[su[32 + j]];
           T N0, N1, N2;
           ft_times<T, V>(f, wa, wb, &N0, &N1, &N2);
@@ -810,7 +813,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           a.gamma[1 * a.WS + wi] = x1;
           a.gamma[2 * a.WS + wi] = x2;
           a.wid[wi] = __ldg(a.idb + c) - (uint32_t)P.b0;
-          Frame<double> f = load_frame_fp64(a, c);
+          Frame<double> f = load_frame_fp64(a, c, P.exact != 0);
           a.qd[c] = f_times<double, double4>(f, x0, x1, x2);
         }
       }

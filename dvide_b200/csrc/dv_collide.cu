@@ -249,7 +249,7 @@ struct NpOut {
 
 // CollisionDetector.cu:187-331 (test) and 333-501 (store), rigid bodies only.
 __device__ inline bool narrowphase(const double4* __restrict__ p4, const double4* __restrict__ g4,
-                                   int ia, int ib, double env, NpOut* o) {
+                                   int ia, int ib, double env, bool exact, NpOut* o) {
   double4 pa = p4[ia], pb = p4[ib], ga = g4[ia], gb = g4[ib];
   d3 posA = mk3(pa.x, pa.y, pa.z), posB = mk3(pb.x, pb.y, pb.z);
   d3 gA = mk3(ga.x, ga.y, ga.z), gB = mk3(gb.x, gb.y, gb.z);
@@ -257,9 +257,9 @@ __device__ inline bool narrowphase(const double4* __restrict__ p4, const double4
   d3 normal, location;
   if (gA.y == 0 && gB.y == 0) {
     d3 d = sub3(posB, posA);
-    pen = (gA.x + gB.x) - length3(d);
+    pen = (gA.x + gB.x) - length3x(d, exact);
     if (!(pen >= -env)) return false;
-    normal = normalize3(d);
+    normal = normalize3x(d, exact);
     location = add3(posA, scale3(normal, gA.x));
   } else if ((gA.y != 0 && gB.y == 0) || (gA.y == 0 && gB.y != 0)) {
     double dmin = 0;
@@ -284,7 +284,7 @@ __device__ inline bool narrowphase(const double4* __restrict__ p4, const double4
     else if (center.z > bmax.z) { t = center.z - bmax.z; dmin += t * t; nrm.z = nrm.z + t; }
     pen = r - sqrt(dmin);
     if (!(pen >= -env)) return false;
-    normal = normalize3(nrm);
+    normal = normalize3x(nrm, exact);
     location = sub3(center, scale3(normal, r));
     if (sphereA) normal = neg3(normal);
   } else {
@@ -328,11 +328,11 @@ struct CollideArgs {
 };
 
 __device__ inline void write_contact(const CollideArgs& a, size_t c, int ia, int ib,
-                                     const NpOut& o) {
+                                     const NpOut& o, bool exact) {
   a.ida[c] = (uint32_t)ia;
   a.idb[c] = (uint32_t)ib;
   d3 u, v;
-  frame_from_normal(o.n, &u, &v);
+  frame_from_normal(o.n, &u, &v, exact);
   size_t S = a.ccap;
   a.F[0 * S + c] = o.n.x; a.F[1 * S + c] = o.n.y; a.F[2 * S + c] = o.n.z;
   a.F[3 * S + c] = u.x;   a.F[4 * S + c] = u.y;   a.F[5 * S + c] = u.z;
@@ -362,6 +362,7 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
   const SegParams& P = a.seg[sg];
   if (!P.active) return;
   const double env = P.env;
+  const bool exact = P.exact != 0;
   if (lane == 0) s_cnt[warp] = 0;
   __syncwarp();
   int ncand = 0, ncont = 0;
@@ -380,7 +381,7 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
           if (!is_candidate(a.amin, a.amax, a.fam, A, B)) continue;
           ++ncand;
           NpOut o;
-          if (narrowphase(a.p4, a.g4, A, B, env, &o)) {
+          if (narrowphase(a.p4, a.g4, A, B, env, exact, &o)) {
             ++ncont;
             if (kWrite) {
               int slot = atomicAdd(&s_cnt[warp], 1);
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
       if (!is_candidate(a.amin, a.amax, a.fam, A, B)) continue;
       ++ncand;
       NpOut o;
-      if (narrowphase(a.p4, a.g4, A, B, env, &o)) {
+      if (narrowphase(a.p4, a.g4, A, B, env, exact, &o)) {
         ++ncont;
         if (kWrite) {
           int slot = atomicAdd(&s_cnt[warp], 1);
@@ -446,8 +447,8 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
     int e = lane + 32 * t;
     if (e < n) {
       NpOut o;
-      narrowphase(a.p4, a.g4, A, mine[t], env, &o);
-      write_contact(a, base + rk[t], A, mine[t], o);
+      narrowphase(a.p4, a.g4, A, mine[t], env, exact, &o);
+      write_contact(a, base + rk[t], A, mine[t], o, exact);
     }
   }
 }
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(kThreads) k_box_pairs(CollideArgs a, int* __re
   NpOut o;
   if (B < P.b1 && B > L && is_candidate(a.amin, a.amax, a.fam, L, B)) {
     cand = true;
-    cont = narrowphase(a.p4, a.g4, L, B, P.env, &o);
+    cont = narrowphase(a.p4, a.g4, L, B, P.env, P.exact != 0, &o);
   }
   unsigned bal = __ballot_sync(0xffffffffu, cont);
   if (!kWrite) {
@@ -503,7 +504,7 @@ __global__ void __launch_bounds__(kThreads) k_box_pairs(CollideArgs a, int* __re
   pre += __popc(bal & ((1u << lane) - 1u));
   size_t pos = (size_t)(a.cbase[L] + a.sst[sg].delta) +
                (size_t)(chunk_off[crow + blockIdx.x] - chunk_off[crow]) + pre;
-  write_contact(a, pos, L, B, o);
+  write_contact(a, pos, L, B, o, P.exact != 0);
 }
 
 // Contact layout: segment s gets nc_s = contacts of its bodies, slots

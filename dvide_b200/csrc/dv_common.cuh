@@ -40,22 +40,32 @@ __device__ inline d3 normalize3(d3 a) {
   double inv = (double)__fdiv_rn(1.0f, s);
   return scale3(a, inv);
 }
+// The opt-in FP64 forms (not the reference's semantics): double sqrt, then
+// 1 / length and a scale, as normalize3 does in float.
+__device__ inline double length3x(d3 a, bool exact) {
+  return exact ? sqrt(dot3(a, a)) : length3(a);
+}
+__device__ inline d3 normalize3x(d3 a, bool exact) {
+  if (!exact) return normalize3(a);
+  const double inv = 1.0 / sqrt(dot3(a, a));
+  return scale3(a, inv);
+}
 __device__ inline d3 cross3(d3 a, d3 b) {
   return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
 // System.cu:753-762: tangent frame from the stored (B -> A) normal.
-__device__ inline void frame_from_normal(d3 n, d3* u, d3* v) {
+__device__ inline void frame_from_normal(d3 n, d3* u, d3* v, bool exact = false) {
   d3 uu;
   if (n.z != 0) {
-    uu = normalize3(mk3(1, 0, -n.x / n.z));
+    uu = normalize3x(mk3(1, 0, -n.x / n.z), exact);
   } else if (n.x != 0) {
-    uu = normalize3(mk3(-n.z / n.x, 0, 1));
+    uu = normalize3x(mk3(-n.z / n.x, 0, 1), exact);
   } else {
-    uu = normalize3(mk3(1, -n.x / n.y, 0));
+    uu = normalize3x(mk3(1, -n.x / n.y, 0), exact);
   }
   *u = uu;
-  *v = normalize3(cross3(n, uu));
+  *v = normalize3x(cross3(n, uu), exact);
 }
 
 // APGD.cu:47-78: projection of one contact impulse onto the friction cone.

@@ -76,6 +76,8 @@ static int check_params(const dv_params& p) {
   if (p.max_iterations < 0 || p.max_backtracks < 0) return DV_ERR_ARG;
   if (p.solver != DV_SOLVER_APGD && p.solver != DV_SOLVER_PGJ) return DV_ERR_UNSUPPORTED;
   if (p.precision != DV_PREC_FP64 && p.precision != DV_PREC_MIXED) return DV_ERR_UNSUPPORTED;
+  if (p.warm_start < 0 || p.warm_start > 2) return DV_ERR_ARG;
+  if (p.fp64_narrowphase != 0 && p.fp64_narrowphase != 1) return DV_ERR_ARG;
   return DV_OK;
 }
 
@@ -287,6 +289,7 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
       G.max_iter = P.max_iterations;
       G.max_bt = P.max_backtracks;
       G.warm = P.warm_start;
+      G.exact = P.fp64_narrowphase;
       G.active = 1;
       G.b0 = nb2;
       G.b1 = nb2 + n;
@@ -599,6 +602,7 @@ int Engine::set_segment_params(int s, const dv_params& P) {
   G.max_iter = P.max_iterations;
   G.max_bt = P.max_backtracks;
   G.warm = P.warm_start;
+  G.exact = P.fp64_narrowphase;
   if (P.solver != P_[s].solver) {
     if (d.nseg != 1) return DV_ERR_UNSUPPORTED;
     d.solver = P.solver;

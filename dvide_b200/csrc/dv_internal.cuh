@@ -54,6 +54,7 @@ struct SegParams {
   double h, mu, tol, env;
   double W;                 // grid cell lower bound: widest small AABB, 2 (r_max + env)
   int max_iter, max_bt, warm;
+  int exact;                // 1: FP64 length/normalize in narrowphase and frame (opt-in)
   int active;               // 0: the segment is skipped entirely (free server slot)
   int b0, b1;               // bodies
   int s0, s1;               // small (gridded) bodies in small_ids

@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
       int k = k0 + m * kThreads + threadIdx.x;
       if (k < nc) {
         const int c = c0 + k;
-        Frame<double> fd = load_frame_fp64(a, c);
+        Frame<double> fd = load_frame_fp64(a, c, P.exact != 0);
         const uint32_t ia = __ldg(a.ida + c), ib = __ldg(a.idb + c);
         double4 wa = a.wd[ia], wb = a.wd[ib];
         double d0, d1, d2;
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
         sum = sum + fd.v2 * fd.v2;
         const double mia = __ldg(a.minv + ia), mib = __ldg(a.minv + ib);
         Bc[c] = (T)(3.0 / ((mia + mib) * sum));
-        Frame<T> f = load_frame<T>(a, c);
+        Frame<T> f = load_frame<T>(a, c, P.exact != 0);
         qv[c] = f_times<T, V>(f, T(1), T(0), T(0));
       }
     }
@@ -237,6 +237,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
       int cs = -1, cur = 0, kk = 0;
       T mu = T(0);
       double mud = 0.0;
+      bool ex = false;
       for (int i = 0;; ++i) {
         const int t = cta_tile(a, NT, i);
         if (t < 0) break;
@@ -249,6 +250,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
           kk = __ldcg(&a.sst[s].ctl.k);
           mud = a.seg[s].mu;
           mu = (T)mud;
+          ex = a.seg[s].exact != 0;
         }
         if (s != run.s) {
           if (run.n) {
@@ -266,7 +268,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
           int k = k0 + m * kThreads + threadIdx.x;
           if (k < nc) {
             const int c = c0 + k;
-            Frame<T> f = load_frame<T>(a, c);
+            Frame<T> f = load_frame<T>(a, c, ex);
             V wa = wv[__ldg(a.ida + c)], wb = wv[__ldg(a.idb + c)];
             T N0, N1, N2;
             ft_times<T, V>(f, wa, wb, &N0, &N1, &N2);
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
           a.gamma[0 * a.WS + wi] = x0;
           a.gamma[1 * a.WS + wi] = x1;
           a.gamma[2 * a.WS + wi] = x2;
-          Frame<double> f = load_frame_fp64(a, c);
+          Frame<double> f = load_frame_fp64(a, c, P.exact != 0);
           a.qd[c] = f_times<double, double4>(f, x0, x1, x2);
         }
       }

@@ -99,10 +99,10 @@ __device__ inline void frame_from_normal_f(float n0, float n1, float n2, Frame<f
 }
 
 // The FP64 frame, recomputed from the stored normal with the narrowphase's own
-// function (same bits as the stored u, v planes).
-__device__ inline Frame<double> frame_d(double n0, double n1, double n2) {
+// function and the scene's mode (same bits as the stored u, v planes).
+__device__ inline Frame<double> frame_d(double n0, double n1, double n2, bool exact) {
   d3 u, v;
-  frame_from_normal(mk3(n0, n1, n2), &u, &v);
+  frame_from_normal(mk3(n0, n1, n2), &u, &v, exact);
   Frame<double> f;
   f.n0 = n0; f.n1 = n1; f.n2 = n2;
   f.u0 = u.x; f.u1 = u.y; f.u2 = u.z;
@@ -110,11 +110,13 @@ __device__ inline Frame<double> frame_d(double n0, double n1, double n2) {
   return f;
 }
 
-template <class T> __device__ inline Frame<T> make_frame(T n0, T n1, T n2);
-template <> __device__ inline Frame<double> make_frame<double>(double n0, double n1, double n2) {
-  return frame_d(n0, n1, n2);
+// `exact`: the scene's FP64 narrowphase mode (the FP32 frame ignores it).
+template <class T> __device__ inline Frame<T> make_frame(T n0, T n1, T n2, bool exact);
+template <>
+__device__ inline Frame<double> make_frame<double>(double n0, double n1, double n2, bool exact) {
+  return frame_d(n0, n1, n2, exact);
 }
-template <> __device__ inline Frame<float> make_frame<float>(float n0, float n1, float n2) {
+template <> __device__ inline Frame<float> make_frame<float>(float n0, float n1, float n2, bool) {
   Frame<float> f;
   frame_from_normal_f(n0, n1, n2, f);
   return f;
@@ -130,14 +132,14 @@ template <> __device__ inline const float* normal_planes<float>(const KArgs<floa
 }
 
 template <class T>
-__device__ inline Frame<T> load_frame(const KArgs<T>& a, int c) {
+__device__ inline Frame<T> load_frame(const KArgs<T>& a, int c, bool exact) {
   const T* n = normal_planes<T>(a);
-  return make_frame<T>(n[c], n[a.S + c], n[2 * a.S + c]);
+  return make_frame<T>(n[c], n[a.S + c], n[2 * a.S + c], exact);
 }
 
 template <class T>
-__device__ inline Frame<double> load_frame_fp64(const KArgs<T>& a, int c) {
-  return frame_d(__ldg(a.F + c), __ldg(a.F + a.S + c), __ldg(a.F + 2 * a.S + c));
+__device__ inline Frame<double> load_frame_fp64(const KArgs<T>& a, int c, bool exact) {
+  return frame_d(__ldg(a.F + c), __ldg(a.F + a.S + c), __ldg(a.F + 2 * a.S + c), exact);
 }
 
 // q = F x : q_k = (n_k x0 + u_k x1) + v_k x2

@@ -66,6 +66,10 @@ typedef struct dv_params {
   int32_t precision;     /* DV_PREC_FP64 (drop-in) or DV_PREC_MIXED */
   int32_t max_backtracks;/* cap on Lipschitz doublings per solve (reference: unbounded) */
   int32_t verbose;       /* print the per-step line of System.cu:592 */
+  int32_t fp64_narrowphase; /* extension, default 0: 1 computes length/normalize of the
+                               narrowphase and the tangent frame with FP64 square roots
+                               (the reference's are float, helper_math_double.h:576-597);
+                               not the reference's results, so never with parity checks */
 } dv_params;
 
 /* Per-step report (System.cu:586-599 and APGD.cu:351-357). */

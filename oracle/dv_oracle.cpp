@@ -70,6 +70,14 @@ inline V3 normalize3(V3 a) {
   double inv = (double)(1.0f / sqrtf((float)dot3(a, a)));
   return scale(a, inv);
 }
+/* The opt-in FP64 forms (not the reference's semantics): double sqrt, then
+ * 1 / length and a scale, as normalize3 does in float. */
+inline double length3x(V3 a, bool exact) { return exact ? std::sqrt(dot3(a, a)) : length3(a); }
+inline V3 normalize3x(V3 a, bool exact) {
+  if (!exact) return normalize3(a);
+  double inv = 1.0 / std::sqrt(dot3(a, a));
+  return scale(a, inv);
+}
 /* helper_math_double.h:692-695 */
 inline V3 cross3(V3 a, V3 b) {
   return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
@@ -144,17 +152,17 @@ inline void project3(double* g, double mu) {
 }
 
 /* System.cu:753-762, tangent frame from the stored normal. */
-inline void frame_from_normal(V3 n, V3* u, V3* v) {
+inline void frame_from_normal(V3 n, V3* u, V3* v, bool exact = false) {
   V3 uu;
   if (n.z != 0) {
-    uu = normalize3(mk(1, 0, -n.x / n.z));
+    uu = normalize3x(mk(1, 0, -n.x / n.z), exact);
   } else if (n.x != 0) {
-    uu = normalize3(mk(-n.z / n.x, 0, 1));
+    uu = normalize3x(mk(-n.z / n.x, 0, 1), exact);
   } else {
-    uu = normalize3(mk(1, -n.x / n.y, 0));
+    uu = normalize3x(mk(1, -n.x / n.y, 0), exact);
   }
   *u = uu;
-  *v = normalize3(cross3(n, uu));
+  *v = normalize3x(cross3(n, uu), exact);
 }
 
 struct Scene {
@@ -268,13 +276,14 @@ bool narrowphase(const Scene& S, int ia, int ib, double env, ContactOut* out) {
   V3 posB = mk(S.p[3 * ib], S.p[3 * ib + 1], S.p[3 * ib + 2]);
   V3 gA = mk(S.geom[3 * ia], S.geom[3 * ia + 1], S.geom[3 * ia + 2]);
   V3 gB = mk(S.geom[3 * ib], S.geom[3 * ib + 1], S.geom[3 * ib + 2]);
+  const bool exact = S.P.fp64_narrowphase != 0;
   double pen;
   V3 normal, location;
   if (gA.y == 0 && gB.y == 0) {
     V3 d = sub(posB, posA);
-    pen = (gA.x + gB.x) - length3(d);
+    pen = (gA.x + gB.x) - length3x(d, exact);
     if (!(pen >= -env)) return false;
-    normal = normalize3(d);
+    normal = normalize3x(d, exact);
     location = add(posA, scale(normal, gA.x));
   } else if ((gA.y != 0 && gB.y == 0) || (gA.y == 0 && gB.y != 0)) {
     double dmin = 0;
@@ -299,7 +308,7 @@ bool narrowphase(const Scene& S, int ia, int ib, double env, ContactOut* out) {
     else if (center.z > bmax.z) { t = center.z - bmax.z; dmin += t * t; nrm.z = nrm.z + t; }
     pen = r - sqrt(dmin);
     if (!(pen >= -env)) return false;
-    normal = normalize3(nrm);
+    normal = normalize3x(nrm, exact);
     location = sub(center, scale(normal, r));
     if (sphereA) normal = neg(normal);
   } else {
@@ -424,7 +433,7 @@ void build_frames(Scene& S) {
   for (int c = 0; c < nc; ++c) {
     V3 n = mk(S.nP[4 * c], S.nP[4 * c + 1], S.nP[4 * c + 2]);
     V3 u, v;
-    frame_from_normal(n, &u, &v);
+    frame_from_normal(n, &u, &v, S.P.fp64_narrowphase != 0);
     double* F = &S.F[9 * (size_t)c];
     F[0] = n.x; F[1] = n.y; F[2] = n.z;
     F[3] = u.x; F[4] = u.y; F[5] = u.z;

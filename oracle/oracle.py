@@ -37,7 +37,7 @@ class OrParams(C.Structure):
                 ("max_iterations", C.c_int), ("warm_start", C.c_int),
                 ("reduce_mode", C.c_int), ("spmv_mode", C.c_int),
                 ("max_backtracks", C.c_int), ("threads", C.c_int), ("apgd_mode", C.c_int),
-                ("solver", C.c_int)]
+                ("solver", C.c_int), ("fp64_narrowphase", C.c_int)]
 
 
 class OrStats(C.Structure):
@@ -118,6 +118,7 @@ def make_params(p: dict, reduce_mode=0, spmv_mode=0, threads=0, apgd_mode=0) -> 
     o.threads = threads
     o.apgd_mode = apgd_mode
     o.solver = int(p.get("solver", 1))
+    o.fp64_narrowphase = int(p.get("fp64_narrowphase", 0))
     return o
 
 
