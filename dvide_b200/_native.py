@@ -16,6 +16,9 @@ LIB_PATH = os.path.join(HERE, "libdvide_b200.so")
 DV_OK = 0
 DV_PREC_FP64 = 0
 DV_PREC_MIXED = 1
+DV_SOLVER_APGD = 1
+DV_SOLVER_PGJ = 5
+DV_SOLVER_PGS = 6
 STATUS = {0: "DV_OK", 1: "DV_ERR_ARG", 2: "DV_ERR_CUDA", 3: "DV_ERR_NAN", 4: "DV_ERR_NOCONV",
           5: "DV_ERR_OOM", 6: "DV_ERR_TIMEOUT", 7: "DV_ERR_UNSUPPORTED", 8: "DV_ERR_ABORTED"}
 

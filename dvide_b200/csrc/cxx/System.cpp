@@ -61,12 +61,15 @@ System::System()
 }
 
 System::System(int type) : System() {
-  // System.cu:77-101: 1 = APGD (also the default), 5 = PGJ; the interior-point,
-  // active-set and Gauss-Seidel solvers are not part of this build.
+  // System.cu:77-101: 1 = APGD (also the default), 5 = PGJ, 6 = PGS; the
+  // interior-point and active-set solvers are not part of this build.
   solverType = type;
   if (type == 5) {
     delete solver;
     solver = new PGJ(this);
+  } else if (type == 6) {
+    delete solver;
+    solver = new PGS(this);
   }
 }
 
@@ -96,7 +99,7 @@ int System::sync_params() {
   P.max_iterations = solver->maxIterations;
   APGD* apgd = dynamic_cast<APGD*>(solver);
   P.warm_start = apgd ? apgd->warmStartMode : 0;
-  P.solver = solverType == 5 ? DV_SOLVER_PGJ : DV_SOLVER_APGD;
+  P.solver = solverType == 5 ? DV_SOLVER_PGJ : solverType == 6 ? DV_SOLVER_PGS : DV_SOLVER_APGD;
   P.verbose = solver->verbose ? 1 : 0;
   if (!scene) return DV_ERR_ARG;
   return dv_set_params(scene, &P);
@@ -104,7 +107,7 @@ int System::sync_params() {
 
 int System::initializeSystem() {
   if (solverType < 1 || solverType > 7) solverType = 1;
-  if (solverType != 1 && solverType != 5) return DV_ERR_UNSUPPORTED;
+  if (solverType != 1 && solverType != 5 && solverType != 6) return DV_ERR_UNSUPPORTED;
   APGD* apgd = dynamic_cast<APGD*>(solver);
   if (apgd && apgd->useAntiRelaxation) return DV_ERR_UNSUPPORTED;
   std::vector<dv_body_desc> desc(bodies.size());
@@ -132,7 +135,7 @@ int System::initializeSystem() {
   P.tolerance = solver->tolerance;
   P.max_iterations = solver->maxIterations;
   P.warm_start = apgd ? apgd->warmStartMode : 0;
-  P.solver = solverType == 5 ? DV_SOLVER_PGJ : DV_SOLVER_APGD;
+  P.solver = solverType == 5 ? DV_SOLVER_PGJ : solverType == 6 ? DV_SOLVER_PGS : DV_SOLVER_APGD;
   if (scene) dv_scene_destroy(scene);
   scene = nullptr;
   int rc = dv_scene_create(desc.data(), (int32_t)desc.size(), &P, &scene);
@@ -271,6 +274,8 @@ int APGD::solve() { return DV_ERR_UNSUPPORTED; }
 // solve entry point in this build.
 int PGJ::setup() { return 0; }
 int PGJ::solve() { return DV_ERR_UNSUPPORTED; }
+int PGS::setup() { return 0; }
+int PGS::solve() { return DV_ERR_UNSUPPORTED; }
 
 int CollisionDetector::setEnvelope(double e) {
   envelope = e;

@@ -878,51 +878,6 @@ void prepare_kernel() {
   done = true;
 }
 
-template <class T>
-KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
-  KArgs<T> a;
-  a.nb = sd.nb;
-  a.nseg = sd.nseg;
-  a.tcap = sd.tcap;
-  a.chunk = cfg.chunk > 0 ? cfg.chunk : 1;
-  a.contiguous = cfg.contiguous;
-  a.S = sd.ccap;
-  a.WS = sd.wtotal;
-  a.p4 = sd.p4;
-  a.v4 = sd.v4;
-  a.k4 = sd.k4;
-  a.f4 = sd.f4;
-  a.fc4 = sd.fc4;
-  a.wd = sd.w4;
-  a.minv = sd.minv;
-  a.bseg = sd.bseg;
-  a.ida = sd.ida;
-  a.idb = sd.idb;
-  a.F = sd.F;
-  a.nf = sd.nf;
-  a.gap = sd.gap;
-  a.r = reinterpret_cast<T*>(sd.r);
-  a.inc_start = sd.inc_start;
-  a.inc = sd.inc;
-  for (int k = 0; k < 5; ++k) {
-    a.G[k] = reinterpret_cast<T*>(sd.G[k]);
-    a.NG[k] = reinterpret_cast<T*>(sd.NG[k]);
-  }
-  a.qd = sd.q;
-  a.gamma = sd.gamma;
-  a.wid = sd.wid;
-  a.ws = sd.ws;
-  a.wc = sd.wc;
-  a.cbase = sd.cbase;
-  a.cnt_cont = sd.cnt_cont;
-  a.part = sd.part;
-  a.seg = sd.seg;
-  a.sst = sd.sst;
-  a.tseg = sd.tseg;
-  a.donemask = sd.donemask;
-  a.ew = sd.ew;
-  return a;
-}
 
 template <class T, int MB>
 void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
@@ -960,6 +915,8 @@ void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, in
   cudaMemsetAsync(&sd.ew->last_release, 0, sizeof(unsigned long long), st);
   if (sd.solver == DV_SOLVER_PGJ) {
     launch_pgj_solve(sd, cfg, st);
+  } else if (sd.solver == DV_SOLVER_PGS) {
+    launch_pgs_solve(sd, cfg, st);
   } else if (sd.precision == DV_PREC_MIXED) {
     if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st);
     else launch_typed<float, 2>(sd, cfg, st);

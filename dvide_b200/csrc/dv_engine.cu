@@ -74,8 +74,10 @@ Engine::~Engine() {
 static int check_params(const dv_params& p) {
   if (!(p.h > 0) || !(p.envelope >= 0) || !(p.mu >= 0) || !(p.tolerance >= 0)) return DV_ERR_ARG;
   if (p.max_iterations < 0 || p.max_backtracks < 0) return DV_ERR_ARG;
-  if (p.solver != DV_SOLVER_APGD && p.solver != DV_SOLVER_PGJ) return DV_ERR_UNSUPPORTED;
+  if (p.solver != DV_SOLVER_APGD && p.solver != DV_SOLVER_PGJ && p.solver != DV_SOLVER_PGS)
+    return DV_ERR_UNSUPPORTED;
   if (p.precision != DV_PREC_FP64 && p.precision != DV_PREC_MIXED) return DV_ERR_UNSUPPORTED;
+  if (p.solver == DV_SOLVER_PGS && p.precision != DV_PREC_FP64) return DV_ERR_UNSUPPORTED;
   if (p.warm_start < 0 || p.warm_start > 2) return DV_ERR_ARG;
   if (p.fp64_narrowphase != 0 && p.fp64_narrowphase != 1) return DV_ERR_ARG;
   return DV_OK;

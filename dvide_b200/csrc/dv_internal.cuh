@@ -226,5 +226,7 @@ void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, in
 // ---- PGJ (dv_pgj.cu) ----
 int pgj_max_ctas(int precision);
 void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st);
+int pgs_max_ctas();
+void launch_pgs_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st);
 
 }  // namespace dv

@@ -22,40 +22,6 @@ namespace {
 constexpr double kPgjOmega = 0.3;
 constexpr double kPgjLambda = 2.0 / 3.0;
 
-// max_c -min(0, scale * x_n - |x_t|), a NaN term counting 0 (PGJ.cu:112-142)
-__device__ inline double pgj_feasible(double xn, double xt1, double xt2, double scale) {
-  double v = scale * xn - sqrt(xt1 * xt1 + xt2 * xt2);
-  if (v != v) v = 0.0;
-  return -fmin(0.0, v);
-}
-
-// Per-tile maxima: each warp folds (exact, order-free) and parks them; the
-// CTA completes the 8-warp fold later and writes planes 0..NQ-1.
-template <int NQ>
-__device__ inline void park_max(DeferBuf& B, int slot, int tile, const double (&m)[NQ]) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    const double v = warp_max(m[q]);
-    if (lane == 0) B.w[slot][q][warp] = v;
-  }
-  if (threadIdx.x == 0) B.tile[slot] = tile;
-}
-
-template <int NQ, class K>
-__device__ inline void fold_parked_max(const K& a, DeferBuf& B, int n) {
-  __syncthreads();
-  for (int i = threadIdx.x; i < n * NQ; i += kThreads) {
-    const int slot = i / NQ, q = i - slot * NQ;
-    const double* w = B.w[slot][q];
-    double r = w[0];
-    for (int k = 1; k < kWarps; ++k) r = fmax(r, w[k]);
-    a.part[(size_t)q * a.tcap + B.tile[slot]] = r;
-  }
-  __threadfence();
-  __syncthreads();
-}
-
 struct PgjCtlArgs {
   double* part;
   int tcap;
@@ -376,51 +342,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
   }
 }
 
-template <class T>
-KArgs<T> make_pgj_args(SceneDev& sd, const SolveConfig& cfg) {
-  KArgs<T> a;
-  a.nb = sd.nb;
-  a.nseg = sd.nseg;
-  a.tcap = sd.tcap;
-  a.chunk = cfg.chunk > 0 ? cfg.chunk : 1;
-  a.contiguous = cfg.contiguous;
-  a.S = sd.ccap;
-  a.WS = sd.wtotal;
-  a.p4 = sd.p4;
-  a.v4 = sd.v4;
-  a.k4 = sd.k4;
-  a.f4 = sd.f4;
-  a.fc4 = sd.fc4;
-  a.wd = sd.w4;
-  a.minv = sd.minv;
-  a.bseg = sd.bseg;
-  a.ida = sd.ida;
-  a.idb = sd.idb;
-  a.F = sd.F;
-  a.nf = sd.nf;
-  a.gap = sd.gap;
-  a.r = reinterpret_cast<T*>(sd.r);
-  a.inc_start = sd.inc_start;
-  a.inc = sd.inc;
-  for (int k = 0; k < 5; ++k) {
-    a.G[k] = reinterpret_cast<T*>(sd.G[k]);
-    a.NG[k] = reinterpret_cast<T*>(sd.NG[k]);
-  }
-  a.qd = sd.q;
-  a.gamma = sd.gamma;
-  a.wid = sd.wid;
-  a.ws = sd.ws;
-  a.wc = sd.wc;
-  a.cbase = sd.cbase;
-  a.cnt_cont = sd.cnt_cont;
-  a.part = sd.part;
-  a.seg = sd.seg;
-  a.sst = sd.sst;
-  a.tseg = sd.tseg;
-  a.donemask = sd.donemask;
-  a.ew = sd.ew;
-  return a;
-}
 
 template <class T>
 int pgj_ctas() {
@@ -441,11 +362,11 @@ int pgj_max_ctas(int precision) {
 void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
   const int grid = std::min(cfg.grid, pgj_max_ctas(sd.precision));
   if (sd.precision == DV_PREC_MIXED) {
-    KArgs<float> a = make_pgj_args<float>(sd, cfg);
+    KArgs<float> a = make_kargs<float>(sd, cfg);
     void* params[] = {&a};
     cudaLaunchCooperativeKernel((const void*)k_pgj_solve<float>, grid, kThreads, params, 0, st);
   } else {
-    KArgs<double> a = make_pgj_args<double>(sd, cfg);
+    KArgs<double> a = make_kargs<double>(sd, cfg);
     void* params[] = {&a};
     cudaLaunchCooperativeKernel((const void*)k_pgj_solve<double>, grid, kThreads, params, 0, st);
   }

@@ -142,6 +142,19 @@ __device__ inline Frame<double> load_frame_fp64(const KArgs<T>& a, int c, bool e
   return frame_d(__ldg(a.F + c), __ldg(a.F + a.S + c), __ldg(a.F + 2 * a.S + c), exact);
 }
 
+// The nine stored frame planes (n, u, v) of contact c, as the narrowphase
+// wrote them: the same bits as load_frame_fp64, read instead of rebuilt.
+template <class T>
+__device__ inline Frame<double> stored_frame(const KArgs<T>& a, int c) {
+  const double* F = a.F;
+  const size_t S = a.S;
+  Frame<double> f;
+  f.n0 = __ldg(F + c); f.n1 = __ldg(F + S + c); f.n2 = __ldg(F + 2 * S + c);
+  f.u0 = __ldg(F + 3 * S + c); f.u1 = __ldg(F + 4 * S + c); f.u2 = __ldg(F + 5 * S + c);
+  f.v0 = __ldg(F + 6 * S + c); f.v1 = __ldg(F + 7 * S + c); f.v2 = __ldg(F + 8 * S + c);
+  return f;
+}
+
 // q = F x : q_k = (n_k x0 + u_k x1) + v_k x2
 template <class T, class V>
 __device__ inline V f_times(const Frame<T>& f, T x0, T x1, T x2) {
@@ -344,6 +357,42 @@ __device__ inline bool fold_parked(const K& a, DeferBuf& B, int n) {
 // Tile arrivals of one segment: a CTA delivers the count of its consecutive
 // tiles of segment s at once (after their partials are written).  True, in
 // every thread, in the CTA whose delivery completes the segment's tiles.
+// ---- maxima reductions of PGJ and PGS (only maxima: no summation order) ----
+// max_c -min(0, scale * x_n - |x_t|), a NaN term counting 0 (PGJ.cu:112-142, PGS.cu:335-365)
+__device__ inline double pgj_feasible(double xn, double xt1, double xt2, double scale) {
+  double v = scale * xn - sqrt(xt1 * xt1 + xt2 * xt2);
+  if (v != v) v = 0.0;
+  return -fmin(0.0, v);
+}
+
+// Per-tile maxima: each warp folds (exact, order-free) and parks them; the
+// CTA completes the 8-warp fold later and writes planes 0..NQ-1.
+template <int NQ>
+__device__ inline void park_max(DeferBuf& B, int slot, int tile, const double (&m)[NQ]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const double v = warp_max(m[q]);
+    if (lane == 0) B.w[slot][q][warp] = v;
+  }
+  if (threadIdx.x == 0) B.tile[slot] = tile;
+}
+
+template <int NQ, class K>
+__device__ inline void fold_parked_max(const K& a, DeferBuf& B, int n) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < n * NQ; i += kThreads) {
+    const int slot = i / NQ, q = i - slot * NQ;
+    const double* w = B.w[slot][q];
+    double r = w[0];
+    for (int k = 1; k < kWarps; ++k) r = fmax(r, w[k]);
+    a.part[(size_t)q * a.tcap + B.tile[slot]] = r;
+  }
+  __threadfence();
+  __syncthreads();
+}
+
+
 template <class K>
 __device__ inline bool seg_arrive(const K& a, int s, int n) {
   __shared__ int s_flag;
@@ -659,6 +708,53 @@ __device__ inline bool wait_warp_stage(const K& a, Staging& st, int s) {
   if (!ok) atomicOr(&a.ew->err, kErrCopyTimeout);
   __syncwarp();
   return ok;
+}
+
+// Kernel arguments of the solve kernels for an engine and a launch shape.
+template <class T>
+KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
+  KArgs<T> a;
+  a.nb = sd.nb;
+  a.nseg = sd.nseg;
+  a.tcap = sd.tcap;
+  a.chunk = cfg.chunk > 0 ? cfg.chunk : 1;
+  a.contiguous = cfg.contiguous;
+  a.S = sd.ccap;
+  a.WS = sd.wtotal;
+  a.p4 = sd.p4;
+  a.v4 = sd.v4;
+  a.k4 = sd.k4;
+  a.f4 = sd.f4;
+  a.fc4 = sd.fc4;
+  a.wd = sd.w4;
+  a.minv = sd.minv;
+  a.bseg = sd.bseg;
+  a.ida = sd.ida;
+  a.idb = sd.idb;
+  a.F = sd.F;
+  a.nf = sd.nf;
+  a.gap = sd.gap;
+  a.r = reinterpret_cast<T*>(sd.r);
+  a.inc_start = sd.inc_start;
+  a.inc = sd.inc;
+  for (int k = 0; k < 5; ++k) {
+    a.G[k] = reinterpret_cast<T*>(sd.G[k]);
+    a.NG[k] = reinterpret_cast<T*>(sd.NG[k]);
+  }
+  a.qd = sd.q;
+  a.gamma = sd.gamma;
+  a.wid = sd.wid;
+  a.ws = sd.ws;
+  a.wc = sd.wc;
+  a.cbase = sd.cbase;
+  a.cnt_cont = sd.cnt_cont;
+  a.part = sd.part;
+  a.seg = sd.seg;
+  a.sst = sd.sst;
+  a.tseg = sd.tseg;
+  a.donemask = sd.donemask;
+  a.ew = sd.ew;
+  return a;
 }
 
 }  // namespace

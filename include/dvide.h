@@ -41,8 +41,9 @@ enum {
 };
 
 enum { DV_PREC_FP64 = 0, DV_PREC_MIXED = 1 };
-/* System(int solverType) numbering (System.cu:77-101): 1 APGD, 5 PGJ. */
-enum { DV_SOLVER_APGD = 1, DV_SOLVER_PGJ = 5 };
+/* System(int solverType) numbering (System.cu:77-101): 1 APGD, 5 PGJ, 6 PGS
+   (PGS: FP64 only). */
+enum { DV_SOLVER_APGD = 1, DV_SOLVER_PGJ = 5, DV_SOLVER_PGS = 6 };
 
 /* One rigid body, as System::initializeSystem flattens it (System.cu:344-424). */
 typedef struct dv_body_desc {

@@ -11,6 +11,7 @@
 #include "../dvide.h"
 #include "APGD.h"
 #include "PGJ.h"
+#include "PGS.h"
 #include "Body.h"
 #include "CollisionDetector.h"
 #include "Solver.h"
@@ -32,6 +33,7 @@ class DeviceArray {
 class System {
   friend class APGD;
   friend class PGJ;
+  friend class PGS;
   friend class CollisionDetector;
   friend class DeviceArray;
 

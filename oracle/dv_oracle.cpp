@@ -888,6 +888,87 @@ void build_k(Scene& S) {
   }
 }
 
+/* PGS.cu:367-459 (solve), :143-224 (updateImpulseVector_CPU, the sweep),
+ * :272-304 (buildB_PGS), :335-365 (getFeasibleX/Y_PGS), :327-333
+ * (getResidual_PGS).  gamma starts at (1, 0, 0), v = Minv D^T gamma + Minv k,
+ * then per iteration a Gauss-Seidel sweep over the contacts in order and the
+ * residual max(feasibleX(gamma), feasibleY(N gamma + r), max |(N gamma + r) . gamma|). */
+void pgs_solve(Scene& S) {
+  const int nc = S.nc, nb = S.nb;
+  const int64_t n3 = 3 * (int64_t)nc;
+  const double omega = 0.3, lambda = 2.0 / 3.0, mu = S.P.mu;
+  std::vector<double> g(n3), T(n3), Bc(nc), bt, fc(3 * (size_t)nb), v(3 * (size_t)nb);
+  for (int c = 0; c < nc; ++c) {
+    g[3 * c] = 1.0;
+    g[3 * c + 1] = 0.0;
+    g[3 * c + 2] = 0.0;
+    const double* F = &S.F[9 * (size_t)c];
+    double sum = F[0] * F[0];
+    for (int k = 1; k < 9; ++k) sum = sum + F[k] * F[k];
+    const double ma = S.minv[3 * (size_t)S.A[c]], mb = S.minv[3 * (size_t)S.B[c]];
+    Bc[c] = 3.0 / ((ma + mb) * sum);
+  }
+  /* :376-379: f_contact = D^T gamma; v = Minv f_contact; tmp = Minv k; v = tmp + v */
+  apply_DT(S, g.data(), fc.data());
+  for (size_t i = 0; i < v.size(); ++i) {
+    const double a1 = S.minv[i] * fc[i], a2 = S.minv[i] * S.k[i];
+    v[i] = a2 + a1;
+  }
+  double residual = 0.0;
+  int k;
+  for (k = 0; k < S.P.max_iterations; ++k) {
+    for (int c = 0; c < nc; ++c) {
+      const double* F = &S.F[9 * (size_t)c];
+      const uint32_t ia = S.A[c], ib = S.B[c];
+      double* va = &v[3 * (size_t)ia];
+      double* vb = &v[3 * (size_t)ib];
+      const double mia = S.minv[3 * (size_t)ia], mib = S.minv[3 * (size_t)ib];
+      const double bn = S.bst[3 * c];
+      const double o0 = g[3 * c], o1 = g[3 * c + 1], o2 = g[3 * c + 2];
+      const double ob = omega * Bc[c];
+      const double ax = va[0], ay = va[1], az = va[2], bx = vb[0], by = vb[1], bz = vb[2];
+      double h[3];
+      h[0] = o0 - ob * (F[0] * ax + F[1] * ay + F[2] * az - F[0] * bx - F[1] * by - F[2] * bz + bn);
+      h[1] = o1 - ob * (F[3] * ax + F[4] * ay + F[5] * az - F[3] * bx - F[4] * by - F[5] * bz);
+      h[2] = o2 - ob * (F[6] * ax + F[7] * ay + F[8] * az - F[6] * bx - F[7] * by - F[8] * bz);
+      project3(h, mu);
+      const double lb = 1.0 - lambda;
+      g[3 * c] = lambda * h[0] + lb * o0;
+      g[3 * c + 1] = lambda * h[1] + lb * o1;
+      g[3 * c + 2] = lambda * h[2] + lb * o2;
+      const double d0 = lambda * (h[0] - o0), d1 = lambda * (h[1] - o1), d2 = lambda * (h[2] - o2);
+      const double ex = F[0] * d0 + F[3] * d1 + F[6] * d2;
+      const double ey = F[1] * d0 + F[4] * d1 + F[7] * d2;
+      const double ez = F[2] * d0 + F[5] * d1 + F[8] * d2;
+      va[0] = ax + mia * ex;
+      va[1] = ay + mia * ey;
+      va[2] = az + mia * ez;
+      vb[0] = bx - mib * ex;
+      vb[1] = by - mib * ey;
+      vb[2] = bz - mib * ez;
+    }
+    const double fx = pgj_feasible(g.data(), mu, nc);
+    schur(S, g.data(), T.data(), bt);
+    for (int64_t i = 0; i < n3; ++i) T[i] = S.r[i] + T[i];
+    double res3 = 0.0;
+    for (int c = 0; c < nc; ++c) {
+      const double d = (T[3 * c] * g[3 * c] + T[3 * c + 1] * g[3 * c + 1]) + T[3 * c + 2] * g[3 * c + 2];
+      res3 = fmax(res3, fabs(d));
+    }
+    const double fy = pgj_feasible(T.data(), 1.0 / mu, nc);
+    residual = fmax(fmax(fx, fy), res3);
+    if (residual < S.P.tolerance) break;
+  }
+  if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
+  for (int64_t i = 0; i < n3; ++i) S.gamma[i] = g[i];
+  S.gsize = nc;
+  S.st.iterations = k;
+  S.st.backtracks = 0;
+  S.st.residual = residual;
+  S.st.objective = 0.0;
+  S.st.status = 0;
+}
+
 void build_r(Scene& S) {
   int nb = S.nb, nc = S.nc;
   std::vector<double> tmp(3 * (size_t)nb);
@@ -911,6 +992,7 @@ int do_step(Scene& S) {
     build_frames(S);
     build_r(S);
     if (S.P.solver == 5) pgj_solve(S);
+    else if (S.P.solver == 6) pgs_solve(S);
     else if (S.P.apgd_mode == 1) apgd_solve(S);
     else apgd_solve_fused(S);
     keep_pairs(S);

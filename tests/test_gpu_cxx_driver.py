@@ -32,8 +32,9 @@ def test_unsupported_solver_type_reports(tmp_path):
     assert "unsupported" in out.stderr
 
 
-@pytest.mark.parametrize("args", [["5", "1e-3", "2000"], ["1", "1e-4", "1000", "2"]],
-                         ids=["pgj", "apgd_matched_warm_start"])
+@pytest.mark.parametrize("args", [["5", "1e-3", "2000"], ["6", "1e-4", "3000"],
+                                  ["1", "1e-4", "1000", "2"]],
+                         ids=["pgj", "pgs", "apgd_matched_warm_start"])
 def test_settle_driver_other_solver_forms(tmp_path, args):
     out = subprocess.run([DRIVER, "120", *args], cwd=tmp_path, capture_output=True, text=True,
                          timeout=300)
