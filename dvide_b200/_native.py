@@ -30,7 +30,7 @@ EXPORTS = [
     "dv_set_gamma", "dv_get_frames", "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
     "dv_contact_forces_per_collision", "dv_get_step_stats", "dv_status_string", "dv_last_error",
     "dv_scene_launch_count", "dv_get_step_history", "dv_clear_step_history",
-    "dv_get_phase_times", "dv_ccp_violation_noalloc",
+    "dv_get_phase_times", "dv_ccp_violation_noalloc", "dv_selftest_bounded_waits",
     "dv_batch_create", "dv_batch_destroy", "dv_batch_set_stream", "dv_batch_step",
     "dv_batch_num_scenes", "dv_batch_get_state", "dv_batch_set_state", "dv_batch_scene_stats",
     "dv_batch_step_history", "dv_batch_get_gamma", "dv_batch_ccp_violation",
@@ -438,6 +438,16 @@ class NativeScene:
 
     def launches(self):
         return int(lib().dv_scene_launch_count(self.h))
+
+
+def selftest_bounded_waits(limit_ms=50):
+    """Runs the solve kernels' bounded waits against conditions that never come
+    true (dv_selftest_bounded_waits); returns (barrier_timed_out,
+    copy_timed_out, error_bits)."""
+    b, c, e = C.c_int32(), C.c_int32(), C.c_uint32()
+    check(lib().dv_selftest_bounded_waits(int(limit_ms), C.byref(b), C.byref(c), C.byref(e)),
+          "dv_selftest_bounded_waits")
+    return b.value, c.value, e.value
 
 
 class NativeBatch:

@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 
-CUDA_SOURCES = ["dv_sort.cu", "dv_collide.cu", "dv_apgd.cu", "dv_pgj.cu", "dv_pgs.cu", "dv_engine.cu", "dv_diag.cu", "dv_scene.cu", "dv_batch.cu", "dv_server.cu", "dv_noalloc.cu"]
+CUDA_SOURCES = ["dv_sort.cu", "dv_collide.cu", "dv_apgd.cu", "dv_pgj.cu", "dv_pgs.cu", "dv_engine.cu", "dv_diag.cu", "dv_scene.cu", "dv_batch.cu", "dv_server.cu", "dv_noalloc.cu", "dv_selftest.cu"]
 CUDA_HEADERS = ["dv_common.cuh", "dv_internal.cuh", "dv_engine.h", "dv_solve.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",

@@ -240,6 +240,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   stg.phase = 0;
   if (threadIdx.x == 0) {
     for (int i = 0; i < 2 * kWarps; ++i) mbar_init(stg.bar + i, 1);
+    for (int w = 0; w < kWarps; ++w) reinterpret_cast<unsigned char*>(stg.bar + 2 * kWarps)[w] = 0;
     fence_mbar_init();
   }
   __syncthreads();
@@ -595,6 +596,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
                        int restart) {
         const int kw = (t - st0) * kTileItems + sub * kSub + warp * 32;
         if (lane == 0 && kw < snc) {
+          mark_stage_issued(stg, sidx);
           const int cw = sc0 + kw;
           const T* nrm = normal_planes<T>(a);
           const T* src[kStagePlanes];
@@ -664,7 +666,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         const int ti = tcur;
         if (sub == 0 && s != run.s) {
           if (run.n) {
-            if (!fold_parked<7, true>(a, s_def, nslot)) return;
+            if (!fold_parked<7, true>(a, s_def, nslot)) {
+              drain_warp_stages(stg, &a.ew->wait_limit_ns);
+              return;
+            }
             nslot = 0;
           }
           flush_run(a, run, ctl);
@@ -679,7 +684,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         }
         const int ns = (nseq >= 0 && nsub == 0) ? sc.s : s;
         __syncwarp();  // the warp's reads of stage sidx^1 are done
-        if (nseq >= 0) {
+        if (nseq >= 0 && !failed) {
           if (ns == s) {
             issue(ntile, st0, sc0, snc, nsub, sidx ^ 1, ps.cur, ps.nw, ps.restart);
           } else {
@@ -764,7 +769,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           bad = false;
           ++run.n;
           if (++nslot == kMaxDefer) {
-            if (!fold_parked<7, true>(a, s_def, nslot)) return;
+            if (!fold_parked<7, true>(a, s_def, nslot)) {
+              drain_warp_stages(stg, &a.ew->wait_limit_ns);
+              return;
+            }
             nslot = 0;
           }
         }
@@ -778,10 +786,16 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           sc0 = sc.c0; st0 = sc.t0; snc = sc.nc;
         }
       }
-      if (!fold_parked<7, true>(a, s_def, nslot)) return;
+      if (!fold_parked<7, true>(a, s_def, nslot)) {
+        drain_warp_stages(stg, &a.ew->wait_limit_ns);
+        return;
+      }
       flush_run(a, run, ctl);
     }
-    if (!grid_sync(a, kPhaseProduct, latch)) return;
+    if (!grid_sync(a, kPhaseProduct, latch)) {
+      drain_warp_stages(stg, &a.ew->wait_limit_ns);
+      return;
+    }
   }
 
   // ---- gamma = gamma_hat (APGD.cu:358) into the warm-start region; q = F gamma (FP64)

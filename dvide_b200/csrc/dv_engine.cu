@@ -202,6 +202,7 @@ int Engine::init(const std::vector<SceneInput>& scenes, int precision) {
   if (cudaMallocHost(&h_ew_, sizeof(EngineWords)) != cudaSuccess)
     return dv_record_cuda_error(cudaErrorMemoryAllocation, "cudaMallocHost", __FILE__, __LINE__);
   memset(h_ew_, 0, sizeof(EngineWords));
+  h_ew_->wait_limit_ns = kBarrierTimeoutNs;
   DV_CUDA_TRY(cudaMemcpyAsync(d.ew, h_ew_, sizeof(EngineWords), cudaMemcpyHostToDevice, st_));
   std::vector<SlotSpec> slots(scenes.size());
   for (size_t i = 0; i < scenes.size(); ++i) slots[i].in = scenes[i];

@@ -120,6 +120,7 @@ struct EngineWords {
   unsigned long long last_release;
   unsigned long long phase_ns[8];
   unsigned long long phase_count[8];
+  unsigned long long wait_limit_ns;  // every bounded wait (grid barrier, bulk copy) ends after this
 };
 
 struct SceneDev {

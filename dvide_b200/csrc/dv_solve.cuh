@@ -492,6 +492,7 @@ __device__ inline bool grid_sync(const K& a, int phase, Fn ctl_fn) {
       E->last_release = now;
     }
   } else if (threadIdx.x == 0) {
+    const uint64_t limit = a.ew->wait_limit_ns;
     uint64_t t0 = global_ns();
     unsigned polls = 0;
     while (ld_acquire(&bar[1]) < s_target) {
@@ -501,7 +502,7 @@ __device__ inline bool grid_sync(const K& a, int phase, Fn ctl_fn) {
           s_fail = 1;
           break;
         }
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
+        if (global_ns() - t0 > limit) {
           atomicOr(&a.ew->err, kErrBarrierTimeout);
           s_fail = 1;
           break;
@@ -681,7 +682,7 @@ __host__ __device__ constexpr unsigned warp_stage_bytes() {
 }
 template <class T>
 __host__ __device__ constexpr size_t dyn_smem_bytes() {
-  return (size_t)kWarps * 2 * warp_stage_bytes<T>() + (size_t)kWarps * 2 * 8;
+  return (size_t)kWarps * 2 * warp_stage_bytes<T>() + (size_t)kWarps * 2 * 8 + 16;
 }
 
 struct Staging {
@@ -691,23 +692,61 @@ struct Staging {
   unsigned phase;       // bit s: parity the next wait on this warp's stage s expects
 };
 
-// Bounded wait for this warp's stage s; false after a timeout (error recorded).
-template <class K>
-__device__ inline bool wait_warp_stage(const K& a, Staging& st, int s) {
-  const int w = threadIdx.x >> 5;
-  unsigned par = (st.phase >> s) & 1u;
-  uint64_t* bar = st.bar + 2 * w + s;
-  bool ok = mbar_try_wait(bar, par);
+// Per warp, bit s: copies issued into stage s and not yet seen complete; one
+// byte per warp after the mbarriers (lane 0 writes it).
+__device__ inline volatile unsigned char* stage_pending(const Staging& st) {
+  return reinterpret_cast<volatile unsigned char*>(st.bar + 2 * kWarps) + (threadIdx.x >> 5);
+}
+__device__ inline void mark_stage_issued(const Staging& st, int s) {
+  if ((threadIdx.x & 31) == 0) *stage_pending(st) |= (unsigned char)(1u << s);
+}
+
+// Waits for the phase of parity `parity` of an mbarrier to complete; false
+// after `*limit_ns` (read only if the first test fails).
+__device__ inline bool bounded_mbar_wait(uint64_t* bar, unsigned parity,
+                                         const unsigned long long* limit_ns) {
+  bool ok = mbar_try_wait(bar, parity);
   if (!ok) {
-    uint64_t t0 = global_ns();
-    while (!(ok = mbar_try_wait(bar, par))) {
-      if (global_ns() - t0 > kBarrierTimeoutNs) break;
+    const uint64_t limit = *limit_ns;
+    const uint64_t t0 = global_ns();
+    while (!(ok = mbar_try_wait(bar, parity))) {
+      if (global_ns() - t0 > limit) break;
     }
   }
-  st.phase ^= (1u << s);
-  if (!ok) atomicOr(&a.ew->err, kErrCopyTimeout);
+  return ok;
+}
+
+// Bounded wait on this warp's stage s.
+__device__ inline bool bounded_stage_wait(Staging& st, int s, const unsigned long long* limit_ns) {
+  const int w = threadIdx.x >> 5;
+  const unsigned par = (st.phase >> s) & 1u;
+  uint64_t* bar = st.bar + 2 * w + s;
+  const bool ok = bounded_mbar_wait(bar, par, limit_ns);
+  if (ok) {
+    st.phase ^= (1u << s);
+    if ((threadIdx.x & 31) == 0) *stage_pending(st) &= (unsigned char)~(1u << s);
+  }
+  return ok;
+}
+
+// Waits for this warp's stage s; false after a timeout (error recorded, the
+// stage left pending for drain_warp_stages).
+template <class K>
+__device__ inline bool wait_warp_stage(const K& a, Staging& st, int s) {
+  const bool ok = bounded_stage_wait(st, s, &a.ew->wait_limit_ns);
+  if (!ok && (threadIdx.x & 31) == 0) atomicOr(&a.ew->err, kErrCopyTimeout);
   __syncwarp();
   return ok;
+}
+
+// Before a CTA leaves the kernel early: waits once more, again with a time
+// limit, for the copies this warp still has in flight into its stages.
+__device__ __noinline__ void drain_warp_stages(Staging st, const unsigned long long* limit_ns) {
+  __syncwarp();
+  const unsigned pend = __shfl_sync(0xffffffffu, (unsigned)*stage_pending(st), 0);
+  for (int s = 0; s < 2; ++s)
+    if ((pend >> s) & 1u) bounded_stage_wait(st, s, limit_ns);
+  __syncwarp();
 }
 
 // Kernel arguments of the solve kernels for an engine and a launch shape.

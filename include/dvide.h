@@ -318,6 +318,15 @@ DV_API int dv_server_poll(dv_server* s, dv_request_result* out, int32_t cap, int
 DV_API int dv_server_result_state(dv_server* s, int64_t id, double* p, double* v);
 DV_API int dv_server_get_stats(dv_server* s, dv_server_stats* out);
 
+/* Failure detection without a fault: runs the solve kernels' bounded waits
+ * (grid barrier, bulk-copy mbarrier) against conditions that never become
+ * true -- a CTA that never arrives, bytes no copy brings -- with a limit of
+ * limit_ms, and reports whether each wait ended by its time limit
+ * (*barrier_timed_out, *copy_timed_out = 1) and the error bits it left.  The
+ * device stays usable afterwards. */
+DV_API int dv_selftest_bounded_waits(int32_t limit_ms, int32_t* barrier_timed_out,
+                                     int32_t* copy_timed_out, uint32_t* error_bits);
+
 #ifdef __cplusplus
 }
 #endif
