@@ -182,8 +182,66 @@ def cpu_baseline_sample(sc, budget_s):
             break
     dt = time.perf_counter() - t0
     return {"value": contacts / dt, "unit": "contact-steps/s", "cores": threads, "kind": "port",
-            "sample": f"first {n} time step(s) from the same initial state, cold warm-start "
-                      f"buffer, {dt:.1f} s"}
+            "sample": f"first {n} time step(s) from the same initial state and stored warm "
+                      f"start, {dt:.1f} s"}
+
+
+def run_mixed_error(N, stream, steps=500, every=10):
+    """Mixed precision (FP32 iterates, FP64 sums and update) against FP64 on the
+    1,000-sphere settling box (h 1e-3, at most 1000 iterations, warm start):
+    every `every`-th of `steps` steps, the mixed solve starts from the FP64
+    run's state and warm start and both take one step; relative 2-norm errors
+    of gamma and v, the largest velocity difference, and both residuals.  At
+    the benchmark tolerance 1e-4 the two solves stop at different iterates, so
+    the difference includes the solver tolerance; at 1e-6 it is the precision.
+    The FP64 path gives the oracle's results bit for bit
+    (tests/test_gpu_parity.py)."""
+    from dvide_b200 import scenes
+
+    def rel(a, b):
+        n = float(np.linalg.norm(b))
+        d = float(np.linalg.norm(a - b))
+        return d / n if n > 0 else d
+
+    out = {"workload": (f"settling_box 1000 spheres, every {every}th of {steps} steps "
+                        f"(teacher-forced from the FP64 run), h 1e-3, maxIter 1000")}
+    for tol in (1e-4, 1e-6):
+        sc = scenes.settling_box(tolerance=tol)
+        f = N.NativeScene.from_scene(sc)
+        m = N.NativeScene.from_scene(sc, precision=N.DV_PREC_MIXED)
+        f.set_stream(stream.cuda_stream)
+        m.set_stream(stream.cuda_stream)
+        rows = []
+        for k in range(steps):
+            if (k + 1) % every:
+                f.step(1)
+                continue
+            p, v = f.state()
+            m.set_state(p, v)
+            m.set_gamma(f.gamma())
+            f.step(1)
+            m.step(1)
+            sf, sm = f.stats(), m.stats()
+            if sf["num_contacts"] == 0:
+                continue
+            vf, vm = f.state()[1], m.state()[1]
+            rows.append((rel(m.gamma(), f.gamma()), rel(vm, vf), float(np.abs(vm - vf).max()),
+                         sf["residual"], sm["residual"], sf["iterations"], sm["iterations"]))
+        f.close()
+        m.close()
+        if not rows:
+            continue
+        a = np.array(rows)
+        out[f"tolerance_{tol:g}"] = {
+            "steps_compared": len(rows),
+            "gamma_rel_err": {"max": float(a[:, 0].max()), "median": float(np.median(a[:, 0]))},
+            "v_rel_err": {"max": float(a[:, 1].max()), "median": float(np.median(a[:, 1]))},
+            "v_abs_err_max_m_per_s": float(a[:, 2].max()),
+            "residual_fp64_max": float(a[:, 3].max()),
+            "residual_mixed_max": float(a[:, 4].max()),
+            "iterations_mean": {"fp64": float(a[:, 5].mean()), "mixed": float(a[:, 6].mean())},
+        }
+    return out
 
 
 def run_batched(args, N, torch, stream):
@@ -348,6 +406,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the headline workload (fp64 is the plain drop-in)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes line")
+    ap.add_argument("--no-mixed-error", action="store_true",
+                    help="skip the mixed-precision error report")
     ap.add_argument("--batch-scenes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--batch-timed", type=int, default=40)
@@ -491,6 +551,8 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(sc, args.cpu_budget_s)
+        if world == 1 and not args.no_mixed_error:
+            line["mixed_precision_error"] = run_mixed_error(N, stream)
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(args, N, torch, stream)
         if world == 1 and not args.no_served:
