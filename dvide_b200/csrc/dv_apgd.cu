@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           const T e0 = x0 + T(-1), e1 = x1 + T(-1), e2 = x2 + T(-1);
           acc[0] = acc[0] + dot3i(e0, e1, e2, e0, e1, e2);
           Frame<T> f = load_frame<T>(a, c, P.exact != 0);
-          qv[c] = f_times<T, V>(f, e0, e1, e2);
+          store_keep(qv + c, f_times<T, V>(f, e0, e1, e2));
         }
       }
       park_tile<1, false>(s_def, nslot, t, acc, 0.0);
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           ft_times<T, V>(f, wa, wb, &n0, &n1, &n2);
           acc[0] = acc[0] + dot3i(n0, n1, n2, n0, n1, n2);
           T y0 = a.G[0][0 * S + c], y1 = a.G[0][1 * S + c], y2 = a.G[0][2 * S + c];
-          qv[c] = f_times<T, V>(f, y0, y1, y2);
+          store_keep(qv + c, f_times<T, V>(f, y0, y1, y2));
         }
       }
       park_tile<1, false>(s_def, nslot, t, acc, 0.0);
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             T x0 = y0 + nt_ * g0, x1 = y1 + nt_ * g1, x2 = y2 + nt_ * g2;
             project_cone<T>(x0, x1, x2, mu);
             Gn[0 * S + c] = x0; Gn[1 * S + c] = x1; Gn[2 * S + c] = x2;
-            qv[c] = f_times<T, V>(f, x0, x1, x2);
+            store_keep(qv + c, f_times<T, V>(f, x0, x1, x2));
             T t0 = x0 + T(-1) * y0, t1 = x1 + T(-1) * y1, t2 = x2 + T(-1) * y2;
             T s0 = x0 + T(-1) * c0v, s1 = x1 + T(-1) * c1v, s2 = x2 + T(-1) * c2v;
             acc[0] = acc[0] + dot3i(g0, g1, g2, t0, t1, t2);
@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           project_cone<T>(z0, z1, z2, (T)ps.mu);
           T* G2 = a.G[ps.nw2];
           G2[0 * S + c] = z0; G2[1 * S + c] = z1; G2[2 * S + c] = z2;
-          qv[c] = f_times<T, V>(f, z0, z1, z2);
+          store_keep(qv + c, f_times<T, V>(f, z0, z1, z2));
           T t0 = z0 + T(-1) * y0, t1 = z1 + T(-1) * y1, t2 = z2 + T(-1) * y2;
           T s0 = z0 + T(-1) * x0, s1 = z1 + T(-1) * x1, s2 = z2 + T(-1) * x2;
           acc[2] = acc[2] + dot3i(g0, g1, g2, t0, t1, t2);

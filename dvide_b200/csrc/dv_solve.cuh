@@ -155,6 +155,31 @@ __device__ inline Frame<double> stored_frame(const KArgs<T>& a, int c) {
   return f;
 }
 
+// Stores of the vectors a pass writes and the next pass reads at once (q for
+// the body pass, w for the contact pass's gathers), with an L2 evict-last
+// priority: each contact pass streams more contact data than L2 holds, and
+// without the hint these lines are the first to go.  A hint, not a value
+// change.
+__device__ inline uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ inline void store_keep(double4* addr, const double4& v) {
+  const uint64_t pol = l2_evict_last_policy();
+  asm volatile(
+      "st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %5;\n\t"
+      "st.global.L2::cache_hint.v2.f64 [%0+16], {%3, %4}, %5;" ::"l"(addr),
+      "d"(v.x), "d"(v.y), "d"(v.z), "d"(v.w), "l"(pol)
+      : "memory");
+}
+__device__ inline void store_keep(float4* addr, const float4& v) {
+  const uint64_t pol = l2_evict_last_policy();
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(addr),
+               "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol)
+               : "memory");
+}
+
 // q = F x : q_k = (n_k x0 + u_k x1) + v_k x2
 template <class T, class V>
 __device__ inline V f_times(const Frame<T>& f, T x0, T x1, T x2) {
@@ -645,12 +670,12 @@ __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask
         T m = (T)mi;
         V o;
         o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
-        w[b] = o;
+        store_keep(w + b, o);
       } else if (sizeof(T) != sizeof(double)) {
         // the FP32 view of w overlays the FP64 setup values: store the zero
         V o;
         o.x = T(0); o.y = T(0); o.z = T(0); o.w = T(0);
-        w[b] = o;
+        store_keep(w + b, o);
       }
     }
   }
