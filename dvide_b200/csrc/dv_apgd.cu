@@ -259,7 +259,12 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   const CtlArgs ca{a.part, a.tcap, sizeof(T) != sizeof(double) ? 1 : 0, a.sst, a.seg, a.ew,
                    a.donemask};
 
-  // ---- per-segment solve state; done mask (bit set: not iterating)
+  // ---- work lists off; per-segment solve state; done mask (bit set: not iterating)
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ew->act_on = 0;
+    a.ew->act_rebuild = 0;
+    a.ew->act_base = a.nseg;
+  }
   for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.nseg; s += gridDim.x * kThreads) {
     SegState& X = a.sst[s];
     X.err = 0u;
@@ -460,18 +465,32 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // the same either way.  A segment's first step is a step pass too (N y_0
   // is a product: w of gamma_0).  Segment scalars are loaded once per run of
   // consecutive tiles of one segment.
+  // the product pass's barrier also decides whether the work lists are rebuilt:
+  // once half the segments iterating at the last build have finished
+  auto latch_product = [&]() {
+    if (threadIdx.x == 0) {
+      volatile EngineWords* E = a.ew;
+      const int n = atomicExch(&a.ew->step_count, 0);
+      E->step_needed = n;
+      const int act = E->active;
+      if (a.nseg > 1 && act > 0 && 2 * act <= E->act_base) E->act_rebuild = 1;
+    }
+  };
   for (;;) {
     if (__ldcg(&a.ew->active) == 0) break;
     // the done mask at the start of a pass holds for every tile this CTA has
     // left in the pass: a segment finishes only after all its tiles
     load_mask(a, s_mask, mwords);
+    const int lon = __ldcg(&a.ew->act_on);
+    const int NTL = lon ? __ldcg(&a.ew->act_nt) : NT;
+    const int NBL = lon ? __ldcg(&a.ew->act_nb) : 0;
     if (__ldcg(&a.ew->step_needed) > 0) {
       SegRun run;
       int nslot = 0;
       auto ctl = [&](int s) { ctl_step(ca, s, scratch); };
       int cs = -1;
       for (int i = 0;; ++i) {
-        const int t = cta_tile(a, NT, i);
+        const int t = pass_tile(a, lon, NTL, i);
         if (t < 0) break;
         locate(a, sc, t);
         const int s = sc.s;
@@ -572,7 +591,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       flush_run(a, run, ctl);
       if (!grid_sync(a, kPhaseStep, NoCtl{})) return;
     }
-    body_pass_schur(a, s_mask);
+    body_pass_schur(a, s_mask, lon, NBL);
     if (!grid_sync(a, kPhaseBody, NoCtl{})) return;
 
     // N gamma_new, objective (APGD.cu:237-238), residual (:90-102); then the
@@ -582,7 +601,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       // this CTA's next iterating tile at or after sequence index i (-1: none)
       auto next_tile = [&](int i, int* tile_out) {
         for (;; ++i) {
-          int t = cta_tile(a, NT, i);
+          int t = pass_tile(a, lon, NTL, i);
           if (t < 0) return -1;
           locate(a, sc, t);
           if (!mask_done(a, s_mask, mwords, sc.s)) {
@@ -792,9 +811,21 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       }
       flush_run(a, run, ctl);
     }
-    if (!grid_sync(a, kPhaseProduct, latch)) {
+    if (!grid_sync(a, kPhaseProduct, latch_product)) {
       drain_warp_stages(stg, &a.ew->wait_limit_ns);
       return;
+    }
+    if (__ldcg(&a.ew->act_rebuild)) {
+      if (blockIdx.x == 0) rebuild_work_lists(a, reinterpret_cast<int*>(scratch));
+      if (!grid_sync(a, kPhaseRebuild, [&]() {
+            if (threadIdx.x == 0) {
+              volatile EngineWords* E = a.ew;
+              E->act_rebuild = 0;
+              E->act_on = 1;
+              E->act_base = E->active;
+            }
+          }))
+        return;
     }
   }
 

@@ -94,7 +94,7 @@ int Engine::alloc_contacts(size_t cap) {
     dfree(q.G[k]);
     dfree(q.NG[k]);
   }
-  dfree(q.q); dfree(q.inc); dfree(q.part); dfree(q.tseg);
+  dfree(q.q); dfree(q.inc); dfree(q.part); dfree(q.tseg); dfree(q.act_tiles);
   q.ccap = cap;
   q.tcap = (int)(cap / kTileItems) + q.nseg + 1;
   TRY(dalloc(&q.ida, cap));
@@ -112,6 +112,7 @@ int Engine::alloc_contacts(size_t cap) {
   TRY(dalloc(&q.inc, 2 * cap));
   TRY(dalloc(&q.part, (size_t)8 * q.tcap));
   TRY(dalloc(&q.tseg, (size_t)q.tcap));
+  TRY(dalloc(&q.act_tiles, (size_t)q.tcap));
   size_t rc = std::max((size_t)q.nb, cap);
   if (rc > q.radix_cap) {
     dfree(q.keyA); dfree(q.valA); dfree(q.keyB); dfree(q.valB); dfree(q.radix_hist);
@@ -469,6 +470,13 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
     TRY(dalloc(&d.inc_start, (size_t)cap + 1));
     TRY(dalloc(&d.bseg, cap));
     nb_cap_ = cap;
+  }
+  // body ranges of the solve's work lists: at most one partial range per segment
+  const size_t need_ab = (size_t)nb2 / kThreads + (size_t)nseg2 + 1;
+  if (need_ab > d.act_bcap) {
+    dfree(d.act_bodies);
+    TRY(dalloc(&d.act_bodies, need_ab));
+    d.act_bcap = need_ab;
   }
   DV_CUDA_TRY(cudaMemsetAsync(d.k4, 0, sizeof(double4) * nbz, st));
   DV_CUDA_TRY(cudaMemsetAsync(d.w4, 0, sizeof(double4) * nbz, st));

@@ -121,6 +121,16 @@ struct EngineWords {
   unsigned long long phase_ns[8];
   unsigned long long phase_count[8];
   unsigned long long wait_limit_ns;  // every bounded wait (grid barrier, bulk copy) ends after this
+  // Work lists of the iterating passes (solve kernel): once half the segments
+  // that were iterating at the last rebuild have finished, the contact tiles
+  // and body ranges of the segments still iterating are gathered into
+  // SceneDev::act_tiles / act_bodies, and the passes walk those instead of
+  // every tile and body.
+  int act_on;           // 1: the lists are in use
+  int act_nt;           // entries of act_tiles
+  int act_nb;           // entries of act_bodies
+  int act_base;         // segments iterating when the lists were last built (nseg before)
+  int act_rebuild;      // 1: rebuild the lists before the next pass
 };
 
 struct SceneDev {
@@ -180,6 +190,9 @@ struct SceneDev {
   double* G[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double* NG[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double4* q = nullptr;
+  int* act_tiles = nullptr;   // tcap: contact tiles of the segments still iterating
+  int4* act_bodies = nullptr; // act_bcap: (first body, end body, segment, 0), at most 256 bodies each
+  size_t act_bcap = 0;
   double* part = nullptr;     // reduction partials, 9 x tcap
   // warm-start arena (System::gamma_d of every segment): 3 planes of stride
   // wtotal; segment s owns [wbase, wbase + wcap), positional within it

@@ -25,6 +25,7 @@ constexpr int kSub = kThreads;  // contacts per sub-tile
 enum Phase : int {
   kPhaseSetup = 0,     // k, r, Lipschitz estimate
   kPhaseStep = 1,      // gamma_new = P(y - t g): first iteration or backtrack
+  kPhaseRebuild = 2,   // work lists of the segments still iterating
   kPhaseBody = 3,      // body gather w = Minv D^T q
   kPhaseProduct = 4,   // N gamma_new, objective, residual, look-ahead step
   kPhaseFinal = 5,     // gamma = gamma_hat, update
@@ -72,6 +73,8 @@ struct KArgs {
   const int* __restrict__ tseg;
   unsigned* donemask;
   EngineWords* ew;
+  int* act_tiles;          // work lists of the iterating passes (EngineWords::act_on)
+  int4* act_bodies;
 };
 
 template <class T>
@@ -559,6 +562,15 @@ __device__ inline int cta_tile(const K& a, int nt, int i) {
   return t < nt ? (int)t : -1;
 }
 
+// Tile at sequence index i of this CTA in an iterating pass: position i of the
+// work list when it is in use (n = its length; the list is rewritten inside
+// the kernel, so it is read through L2), else tile i of all n tiles.
+template <class K>
+__device__ inline int pass_tile(const K& a, int lon, int n, int i) {
+  const int t = cta_tile(a, n, i);
+  return (t < 0 || !lon) ? t : __ldcg(a.act_tiles + t);
+}
+
 // Sum of -q over B-side contacts, then +q over A-side contacts, ascending
 // contact order (the flat incidence list); loads are issued in groups of
 // eight, the additions stay in order.
@@ -654,30 +666,108 @@ __device__ inline void mark_done(const K& a, int s) {
 
 // Schur body pass: w_b = minv_b * (D^T x)_b for bodies of iterating
 // segments; fixed bodies keep w = 0.
+// w_b of one body of an iterating segment.
 template <class T>
-__device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask) {
+__device__ inline void body_w(const KArgs<T>& a, int b) {
   using V = typename Vec4<T>::type;
   V* w = reinterpret_cast<V*>(a.wd);
   const V* q = reinterpret_cast<const V*>(a.qd);
-  const int nbt = (a.nb + kThreads - 1) / kThreads;
+  double mi = __ldg(a.minv + b);
+  if (mi != 0.0) {
+    V s = gather_q<T, V>(a, q, b);
+    T m = (T)mi;
+    V o;
+    o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
+    store_keep(w + b, o);
+  } else if (sizeof(T) != sizeof(double)) {
+    // the FP32 view of w overlays the FP64 setup values: store the zero
+    V o;
+    o.x = T(0); o.y = T(0); o.z = T(0); o.w = T(0);
+    store_keep(w + b, o);
+  }
+}
+
+// Schur body pass: w_b = minv_b * (D^T x)_b for bodies of iterating
+// segments; fixed bodies keep w = 0.  With the work lists in use (lon), over
+// the listed body ranges (one segment each) instead of every body.
+template <class T>
+__device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask, int lon = 0,
+                                       int nlist = 0) {
   const int mwords = (a.nseg + 31) >> 5;
+  if (lon) {
+    for (int p = blockIdx.x; p < nlist; p += gridDim.x) {
+      const int4 r = __ldcg(a.act_bodies + p);
+      if (mask_done(a, s_mask, mwords, r.z)) continue;
+      const int b = r.x + threadIdx.x;
+      if (b < r.y) body_w(a, b);
+    }
+    return;
+  }
+  const int nbt = (a.nb + kThreads - 1) / kThreads;
   for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
-    if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b)))) {
-      double mi = __ldg(a.minv + b);
-      if (mi != 0.0) {
-        V s = gather_q<T, V>(a, q, b);
-        T m = (T)mi;
-        V o;
-        o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
-        store_keep(w + b, o);
-      } else if (sizeof(T) != sizeof(double)) {
-        // the FP32 view of w overlays the FP64 setup values: store the zero
-        V o;
-        o.x = T(0); o.y = T(0); o.z = T(0); o.w = T(0);
-        store_keep(w + b, o);
+    if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b))))
+      body_w(a, b);
+  }
+}
+
+// Work lists of the segments still iterating (CTA 0, all its threads): their
+// contact tiles in segment order into act_tiles and their bodies, in ranges of
+// at most kThreads within one segment, into act_bodies.  Reads the done mask
+// as the last product pass left it.
+template <class T>
+__device__ inline void rebuild_work_lists(const KArgs<T>& a, int* sbuf) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int base_t = 0, base_b = 0;
+  for (int s0 = 0; s0 < a.nseg; s0 += kThreads) {
+    const int s = s0 + tid;
+    int ct = 0, cb = 0, t0 = 0, b0 = 0, b1 = 0;
+    if (s < a.nseg && !((__ldcg(a.donemask + (s >> 5)) >> (s & 31)) & 1u)) {
+      ct = a.sst[s].nt;
+      t0 = a.sst[s].t0;
+      b0 = a.seg[s].b0;
+      b1 = a.seg[s].b1;
+      cb = (b1 - b0 + kThreads - 1) / kThreads;
+    }
+    // exclusive scans of ct and cb over the block (warp shuffles, then warp totals)
+    int it = ct, ib = cb;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int ut = __shfl_up_sync(0xffffffffu, it, off);
+      const int ub = __shfl_up_sync(0xffffffffu, ib, off);
+      if (lane >= off) {
+        it += ut;
+        ib += ub;
       }
     }
+    __syncthreads();
+    if (lane == 31) {
+      sbuf[warp] = it;
+      sbuf[kWarps + warp] = ib;
+    }
+    __syncthreads();
+    int wt = 0, wb = 0, tt = 0, tb = 0;
+    for (int k = 0; k < kWarps; ++k) {
+      if (k < warp) {
+        wt += sbuf[k];
+        wb += sbuf[kWarps + k];
+      }
+      tt += sbuf[k];
+      tb += sbuf[kWarps + k];
+    }
+    const int et = base_t + wt + it - ct, eb = base_b + wb + ib - cb;
+    for (int j = 0; j < ct; ++j) a.act_tiles[et + j] = t0 + j;
+    for (int j = 0; j < cb; ++j) {
+      const int lo = b0 + j * kThreads;
+      a.act_bodies[eb + j] = make_int4(lo, min(b1, lo + kThreads), s, 0);
+    }
+    base_t += tt;
+    base_b += tb;
+  }
+  __threadfence();
+  if (tid == 0) {
+    a.ew->act_nt = base_t;
+    a.ew->act_nb = base_b;
   }
 }
 
@@ -818,6 +908,8 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   a.tseg = sd.tseg;
   a.donemask = sd.donemask;
   a.ew = sd.ew;
+  a.act_tiles = sd.act_tiles;
+  a.act_bodies = sd.act_bodies;
   return a;
 }
 
