@@ -465,9 +465,12 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // the same either way.  A segment's first step is a step pass too (N y_0
   // is a product: w of gamma_0).  Segment scalars are loaded once per run of
   // consecutive tiles of one segment.
+  // one segment: its step and product controllers run at the passes' barriers
+  const bool single = a.nseg == 1;
   // the product pass's barrier also decides whether the work lists are rebuilt:
   // once half the segments iterating at the last build have finished
   auto latch_product = [&]() {
+    if (single) ctl_product(ca, 0, scratch);
     if (threadIdx.x == 0) {
       volatile EngineWords* E = a.ew;
       const int n = atomicExch(&a.ew->step_count, 0);
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             fold_parked<5, false>(a, s_def, nslot);
             nslot = 0;
           }
-          flush_run(a, run, ctl);
+          flush_run(a, run, ctl, single);
           run.s = s;
         }
         const int cur = s_st.cur, prev = s_st.prev, first = s_st.first, yr = s_st.yr;
@@ -588,8 +591,11 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         }
       }
       fold_parked<5, false>(a, s_def, nslot);
-      flush_run(a, run, ctl);
-      if (!grid_sync(a, kPhaseStep, NoCtl{})) return;
+      flush_run(a, run, ctl, single);
+      if (!grid_sync(a, kPhaseStep, [&]() {
+            if (single) ctl_step(ca, 0, scratch);
+          }))
+        return;
     }
     body_pass_schur(a, s_mask, lon, NBL);
     if (!grid_sync(a, kPhaseBody, NoCtl{})) return;
@@ -691,7 +697,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             }
             nslot = 0;
           }
-          flush_run(a, run, ctl);
+          flush_run(a, run, ctl, single);
           run.s = s;
         }
         // the following sub-tile: this tile's second half, or the next tile
@@ -809,7 +815,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         drain_warp_stages(stg, &a.ew->wait_limit_ns);
         return;
       }
-      flush_run(a, run, ctl);
+      flush_run(a, run, ctl, single);
     }
     if (!grid_sync(a, kPhaseProduct, latch_product)) {
       drain_warp_stages(stg, &a.ew->wait_limit_ns);

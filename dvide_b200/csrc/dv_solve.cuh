@@ -475,10 +475,14 @@ struct SegRun {
 
 // Delivers the run's arrivals; the CTA that completes the segment runs ctl(s).
 template <class K, class Fn>
-__device__ inline void flush_run(const K& a, SegRun& run, Fn ctl) {
+// `deferred`: the pass's grid barrier runs the controller instead (an engine
+// with one segment: its controller follows the last arrival anyway, so the
+// arrival counter would only add a serialized atomic to every CTA's exit).
+__device__ inline void flush_run(const K& a, SegRun& run, Fn ctl, bool deferred = false) {
   if (run.n == 0) return;
   const int s = run.s, n = run.n;
   run.n = 0;
+  if (deferred) return;
   if (seg_arrive(a, s, n)) ctl(s);
 }
 
