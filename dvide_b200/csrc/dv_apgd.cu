@@ -541,6 +541,25 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         T* Gn = a.G[s_st.nw];
         const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        {
+          // the second item's lines into L2 while the first one computes
+          const int k = k0 + kThreads + threadIdx.x;
+          if (k < nc) {
+            const int c = c0 + k;
+            const T* nrm = normal_planes<T>(a);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              prefetch_l2(nrm + d * S + c);
+              prefetch_l2(Gc + d * S + c);
+              prefetch_l2(a.r + d * S + c);
+              if (!first) prefetch_l2(NGc + d * S + c);
+              if (!yr) {
+                prefetch_l2(Gp + d * S + c);
+                if (!first) prefetch_l2(NGp + d * S + c);
+              }
+            }
+          }
+        }
         for (int m = 0; m < kItemsPerThread; ++m) {
           int k = k0 + m * kThreads + threadIdx.x;
           if (k < nc) {

@@ -196,6 +196,10 @@ __device__ inline void bulk_g2s(void* dst, const void* src, unsigned bytes, uint
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// A hint to bring the line holding *p into L2 (no register, no value).
+__device__ inline void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 __device__ inline bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   uint32_t ok;
   asm volatile(
