@@ -710,6 +710,13 @@ __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask
   const int nbt = (a.nb + kThreads - 1) / kThreads;
   for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
+    // the next round's per-body words into L2 while this round gathers
+    const int bn = b + gridDim.x * kThreads;
+    if (bn < a.nb) {
+      prefetch_l2(a.inc_start + bn);
+      prefetch_l2(a.minv + bn);
+      if (a.nseg > 1) prefetch_l2(a.bseg + bn);
+    }
     if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b))))
       body_w(a, b);
   }
