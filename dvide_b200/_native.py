@@ -27,7 +27,8 @@ EXPORTS = [
     "dv_params_default", "dv_scene_create", "dv_scene_destroy", "dv_scene_set_stream",
     "dv_set_params", "dv_step", "dv_collide", "dv_get_state", "dv_set_state",
     "dv_get_contact_force", "dv_get_num_contacts", "dv_get_contacts", "dv_get_gamma",
-    "dv_set_gamma", "dv_get_frames", "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
+    "dv_set_gamma", "dv_add_bilateral_dof", "dv_get_bilateral_gamma", "dv_get_frames",
+    "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
     "dv_contact_forces_per_collision", "dv_get_step_stats", "dv_status_string", "dv_last_error",
     "dv_scene_launch_count", "dv_get_step_history", "dv_clear_step_history",
     "dv_get_phase_times", "dv_ccp_violation_noalloc", "dv_selftest_bounded_waits",
@@ -166,6 +167,8 @@ def lib():
         "dv_get_contacts": [vp, up, up, dp, dp],
         "dv_get_gamma": [vp, dp, C.c_int32, ip],
         "dv_set_gamma": [vp, dp, C.c_int32],
+        "dv_add_bilateral_dof": [vp, C.c_int32, C.c_int32, C.c_double, C.c_double],
+        "dv_get_bilateral_gamma": [vp, dp, C.c_int32, ip],
         "dv_get_frames": [vp, dp],
         "dv_get_schur_vector": [vp, dp],
         "dv_ccp_violation": [vp, dp],
@@ -296,6 +299,8 @@ class NativeScene:
                 precision)
         if getattr(scene, "gamma", None) is not None:
             g.set_gamma(scene.gamma)
+        for row in getattr(scene, "bilateral", None) or ():
+            g.add_bilateral(*row)
         return g
 
     def close(self):
@@ -391,6 +396,19 @@ class NativeScene:
     def set_gamma(self, g):
         g = np.ascontiguousarray(g, dtype=np.float64).reshape(-1, 3)
         check(lib().dv_set_gamma(self.h, dptr(g), g.shape[0]), "dv_set_gamma")
+
+    def add_bilateral(self, dof_a, dof_b=-1, velocity=0.0, start_time=0.0):
+        """System::addBilateralConstraintDOF (before the first step)."""
+        check(lib().dv_add_bilateral_dof(self.h, int(dof_a), int(dof_b), float(velocity),
+                                         float(start_time)), "dv_add_bilateral_dof")
+
+    def bilateral_gamma(self):
+        n = C.c_int32()
+        check(lib().dv_get_bilateral_gamma(self.h, None, 0, C.byref(n)))
+        g = np.zeros(n.value)
+        if n.value:
+            check(lib().dv_get_bilateral_gamma(self.h, dptr(g), n.value, C.byref(n)))
+        return g
 
     def ccp_violation(self):
         o = np.zeros(4)

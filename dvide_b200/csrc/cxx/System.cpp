@@ -28,8 +28,13 @@ DeviceArray::operator std::vector<double>() const {
   if (which == kGamma) {
     int32_t n = 0;
     dv_get_gamma(sys->scene, nullptr, 0, &n);
-    std::vector<double> g(3 * (size_t)n);
-    if (n) dv_get_gamma(sys->scene, g.data(), n, &n);
+    // after a solve the reference's vector holds the bilateral rows first
+    // (APGD.cu:166); before the first step it is 3 nb zeros (System.cu:185)
+    int32_t nb = 0;
+    if (sys->timeIndex > 0) dv_get_bilateral_gamma(sys->scene, nullptr, 0, &nb);
+    std::vector<double> g((size_t)nb + 3 * (size_t)n);
+    if (nb) dv_get_bilateral_gamma(sys->scene, g.data(), nb, &nb);
+    if (n) dv_get_gamma(sys->scene, g.data() + nb, n, &n);
     return g;
   }
   int w = which == kPos ? 0 : which == kVel ? 1 : 2;
@@ -38,9 +43,10 @@ DeviceArray::operator std::vector<double>() const {
 
 size_t DeviceArray::size() const {
   if (which == kGamma) {
-    int32_t n = 0;
+    int32_t n = 0, nb = 0;
     dv_get_gamma(sys->scene, nullptr, 0, &n);
-    return 3 * (size_t)n;
+    if (sys->timeIndex > 0) dv_get_bilateral_gamma(sys->scene, nullptr, 0, &nb);
+    return (size_t)nb + 3 * (size_t)n;
   }
   return 3 * sys->bodies.size();
 }
@@ -105,6 +111,15 @@ int System::sync_params() {
   return dv_set_params(scene, &P);
 }
 
+int System::addBilateralConstraintDOF(int DOFA, int DOFB) {
+  return addBilateralConstraintDOF(DOFA, DOFB, 0.0, 0.0);
+}
+
+int System::addBilateralConstraintDOF(int DOFA, int DOFB, double velocity, double startTime) {
+  bilaterals.push_back(BilateralDOF{DOFA, DOFB, velocity, startTime});
+  return 0;
+}
+
 int System::initializeSystem() {
   if (solverType < 1 || solverType > 7) solverType = 1;
   if (solverType != 1 && solverType != 5 && solverType != 6) return DV_ERR_UNSUPPORTED;
@@ -140,6 +155,12 @@ int System::initializeSystem() {
   scene = nullptr;
   int rc = dv_scene_create(desc.data(), (int32_t)desc.size(), &P, &scene);
   if (rc != DV_OK) return rc;
+  // System::processConstraints (System.cu:303-315): the rows reach the
+  // device here, p0 of a single-DOF row from the positions now
+  for (const BilateralDOF& c : bilaterals) {
+    rc = dv_add_bilateral_dof(scene, c.dofA, c.dofB, c.velocity, c.startTime);
+    if (rc != DV_OK) return rc;
+  }
   return solver->setup();
 }
 

@@ -95,7 +95,8 @@ __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
     C->beta = th * (1.0 - th) / (th * th + tn);
     C->residual = 10e30;
     C->objective = 0.0;
-    const double ncd = (double)a.sst[s].nc;
+    // APGD.cu:92: 1 / (contacts + bilateral rows)^2
+    const double ncd = (double)(a.sst[s].nc + a.seg[s].nbil);
     const double gd = 1.0 / (ncd * ncd);
     C->gdiff = gd;
     C->ginv = 1.0 / gd;
@@ -221,6 +222,76 @@ __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
   }
 }
 
+// The arrays of one bilateral tile in the product pass.
+template <class T>
+struct BilRows {
+  const int2* off;
+  const T* w;          // body vector (4 per body)
+  const T* Gc;         // gamma_k
+  const T* Gn;         // gamma_new
+  T* G2;               // the look-ahead iterate
+  const T* NGc;
+  T* NGn;
+  const T* r;
+  T* q;
+};
+
+// Product pass on rows [r0, r0 + min(n, 512)): N gamma_new, the objective and
+// residual items, the look-ahead step, without the cone projection; the tile's
+// partials are parked in slot `slot`.  Called after the contact tiles (where
+// it adds no registers to the contact loops).  Returns whether a residual
+// item of this thread was NaN.
+template <class T>
+__device__ inline bool bil_product_tile(BilRows<T> R, const ProdScalars& ps, int r0, int n,
+                                              bool has_contacts, DeferBuf* def, int slot, int tile) {
+  const T ya = (T)ps.ya, ym = (T)ps.ym, nt2 = (T)ps.nt2;
+  double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  double mx = 0.0;
+  bool bad = false;
+  for (int m = 0; m < kItemsPerThread; ++m) {
+    const int k = m * kThreads + threadIdx.x;
+    if (k < n) {
+      const int r = r0 + k;
+      const T N0 = bil_dw<T>(__ldg(R.off + r), R.w);
+      R.NGn[r] = N0;
+      const T x0 = R.Gn[r], rr = R.r[r];
+      acc[0] = acc[0] + (double)x0 * (double)N0;
+      acc[1] = acc[1] + (double)x0 * (double)rr;
+      // APGD.cu:90-102 on a row: no projection; without contacts the
+      // residual is |N x + r| (the reference skips both axpby)
+      double T0 = (double)rr + (double)N0;
+      if (has_contacts) {
+        const double X0 = x0;
+        T0 = X0 + (-ps.gd) * T0;
+        T0 = ps.gA * X0 + ps.gB * T0;
+      }
+      const double m0 = fabs(T0);
+      bad |= (m0 != m0);
+      mx = fmax(mx, m0);
+      T y0, M0;
+      if (ps.restart) {
+        y0 = x0;
+        M0 = N0;
+      } else {
+        y0 = ya * x0 + ym * R.Gc[r];
+        M0 = ya * N0 + ym * R.NGc[r];
+      }
+      const T g0 = M0 + rr;
+      const T z0 = y0 + nt2 * g0;
+      R.G2[r] = z0;
+      R.q[r] = z0;
+      const T t0 = z0 + T(-1) * y0, s0 = z0 + T(-1) * x0;
+      acc[2] = acc[2] + (double)g0 * (double)t0;
+      acc[3] = acc[3] + (double)t0 * (double)t0;
+      acc[4] = acc[4] + (double)g0 * (double)s0;
+      acc[5] = acc[5] + (double)y0 * (double)M0;
+      acc[6] = acc[6] + (double)y0 * (double)rr;
+    }
+  }
+  park_tile<7, true>(*def, slot, tile, acc, mx);
+  return bad;
+}
+
 template <class T, int kMinB>
 __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   using V = typename Vec4<T>::type;
@@ -270,7 +341,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     X.err = 0u;
     X.arrive = 0u;
     ApgdCtl& C = X.ctl;
-    const bool live = a.seg[s].active && X.nc > 0;
+    // System.cu:560: a solve runs with contacts or bilateral rows
+    const bool live = a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0);
     C.done = live ? 0 : 1;
     C.iterations = 0;
     C.sweeps = 0;
@@ -283,7 +355,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     unsigned m = 0u;
     for (int j = 0; j < 32; ++j) {
       const int s = wi * 32 + j;
-      if (s >= a.nseg || !(a.seg[s].active && a.sst[s].nc > 0)) m |= 1u << j;
+      if (s >= a.nseg || !(a.seg[s].active && (a.sst[s].nc > 0 || a.seg[s].nbil > 0)))
+        m |= 1u << j;
     }
     a.donemask[wi] = m;
   }
@@ -336,7 +409,42 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0, gsize = sc.gsize;
       const double h = P.h;
       double acc[1] = {0.0};
-      for (int m = 0; m < kItemsPerThread; ++m) {
+      const int kb = a.nbil ? bil_tile_k0(t, sc.t0, nc) : -1;
+      if (kb >= 0) {
+        // bilateral rows: b = violation / h (System.cu:1526-1544) at the
+        // step's start time, r = b + (D Minv k)_row, gamma_0, e = gamma_0 - 1
+        const double* pd = reinterpret_cast<const double*>(a.p4);
+        const double* wdv = reinterpret_cast<const double*>(a.wd);
+        const double tm = a.seg_time[s];
+        for (int m = 0; m < kItemsPerThread; ++m) {
+          const int k = kb + m * kThreads + threadIdx.x;
+          if (k < P.nbil) {
+            const int i = P.bil0 + k;
+            const int2 o = __ldg(a.bil_off + i);
+            const double4 inf = a.bil_info[i];  // velocity, start time, p0
+            double velocity = inf.x;
+            if (tm < inf.y) velocity = 0;
+            const double pa = pd[o.x];
+            const double viol = o.y >= 0 ? pa - pd[o.y] - velocity * (tm - inf.y)
+                                         : pa - inf.z - velocity * (tm - inf.y);
+            const double bb = viol / h;
+            a.bil_b[i] = bb;
+            a.br[i] = (T)(bb + bil_dw<double>(o, wdv));
+            // warm start: the row's last impulse.  Without it the reference's
+            // initialiser writes (1, 0, 0) over flat entries [0, 3 nc) with
+            // the rows first (APGD.cu:114-120, 200): row k takes 1 if k is a
+            // multiple of 3, 0 otherwise, and keeps its last impulse from 3 nc on.
+            double g = a.bil_gam[i];
+            if (!P.warm && k < 3 * nc) g = (k % 3 == 0) ? 1.0 : 0.0;
+            const T x0 = (T)g;
+            a.bG[0][i] = x0;
+            const T e0 = x0 + T(-1);
+            acc[0] = acc[0] + (double)e0 * (double)e0;
+            a.bq[i] = e0;
+          }
+        }
+      }
+      for (int m = 0; m < kItemsPerThread && kb < 0; ++m) {
         int k = k0 + m * kThreads + threadIdx.x;
         if (k < nc) {
           const int c = c0 + k;
@@ -373,8 +481,20 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             g0 = k < gsize ? a.gamma[0 * a.WS + wi] : 0.0;
             g1 = k < gsize ? a.gamma[1 * a.WS + wi] : 0.0;
             g2 = k < gsize ? a.gamma[2 * a.WS + wi] : 0.0;
-          } else {
+          } else if (P.nbil == 0) {
             g0 = 1.0; g1 = 0.0; g2 = 0.0;
+          } else {
+            // the initialiser's (1, 0, 0) pattern over flat entries [0, 3 nc)
+            // of a vector whose first nbil entries are the bilateral rows;
+            // flat entries from 3 nc on keep what the resize kept
+            const long long f = (long long)P.nbil + 3LL * k, lim = 3LL * nc;
+            const size_t wi = (size_t)P.wbase + k;
+            double gg[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+              gg[d] = (f + d < lim) ? (((f + d) % 3 == 0) ? 1.0 : 0.0)
+                                    : (k < gsize ? a.gamma[d * a.WS + wi] : 0.0);
+            g0 = gg[0]; g1 = gg[1]; g2 = gg[2];
           }
           const T x0 = (T)g0, x1 = (T)g1, x2 = (T)g2;
           a.G[0][0 * S + c] = x0; a.G[0][1 * S + c] = x1; a.G[0][2 * S + c] = x2;
@@ -419,7 +539,22 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       }
       const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
       double acc[1] = {0.0};
-      for (int m = 0; m < kItemsPerThread; ++m) {
+      const int kb = a.nbil ? bil_tile_k0(t, sc.t0, nc) : -1;
+      if (kb >= 0) {
+        // bilateral rows: (N e)_row; q = gamma_0 for the first N y
+        const SegParams& P = a.seg[s];
+        const T* wt = reinterpret_cast<const T*>(a.wd);
+        for (int m = 0; m < kItemsPerThread; ++m) {
+          const int k = kb + m * kThreads + threadIdx.x;
+          if (k < P.nbil) {
+            const int i = P.bil0 + k;
+            const T n0 = bil_dw<T>(__ldg(a.bil_off + i), wt);
+            acc[0] = acc[0] + (double)n0 * (double)n0;
+            a.bq[i] = a.bG[0][i];
+          }
+        }
+      }
+      for (int m = 0; m < kItemsPerThread && kb < 0; ++m) {
         int k = k0 + m * kThreads + threadIdx.x;
         if (k < nc) {
           const int c = c0 + k;
@@ -541,7 +676,48 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         T* Gn = a.G[s_st.nw];
         const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
         double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        {
+        const int kb = a.nbil ? bil_tile_k0(t, sc.t0, nc) : -1;
+        if (kb >= 0) {
+          // bilateral rows: the same step without the cone projection
+          const SegParams& P = a.seg[s];
+          const T* wt = reinterpret_cast<const T*>(a.wd);
+          const T* bGc = a.bG[cur];
+          const T* bGp = a.bG[prev < 0 ? cur : prev];
+          T* bNGc = a.bNG[cur];
+          const T* bNGp = a.bNG[prev < 0 ? cur : prev];
+          T* bGn = a.bG[s_st.nw];
+          for (int m = 0; m < kItemsPerThread; ++m) {
+            const int k = kb + m * kThreads + threadIdx.x;
+            if (k < P.nbil) {
+              const int i = P.bil0 + k;
+              const T c0v = bGc[i];
+              T y0, N0;
+              if (yr) y0 = c0v;
+              else y0 = ya * c0v + ym * bGp[i];
+              if (first) {
+                N0 = bil_dw<T>(__ldg(a.bil_off + i), wt);
+                bNGc[i] = N0;
+              } else if (yr) {
+                N0 = bNGc[i];
+              } else {
+                N0 = ya * bNGc[i] + ym * bNGp[i];
+              }
+              const T r0 = a.br[i];
+              const T g0 = N0 + r0;
+              const T x0 = y0 + nt_ * g0;
+              bGn[i] = x0;
+              a.bq[i] = x0;
+              const T t0 = x0 + T(-1) * y0, s0 = x0 + T(-1) * c0v;
+              acc[0] = acc[0] + (double)g0 * (double)t0;
+              acc[1] = acc[1] + (double)t0 * (double)t0;
+              acc[2] = acc[2] + (double)g0 * (double)s0;
+              if (first) {
+                acc[3] = acc[3] + (double)y0 * (double)N0;
+                acc[4] = acc[4] + (double)y0 * (double)r0;
+              }
+            }
+          }
+        } else {
           // the second item's lines into L2 while the first one computes
           const int k = k0 + kThreads + threadIdx.x;
           if (k < nc) {
@@ -560,7 +736,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             }
           }
         }
-        for (int m = 0; m < kItemsPerThread; ++m) {
+        for (int m = 0; m < kItemsPerThread && kb < 0; ++m) {
           int k = k0 + m * kThreads + threadIdx.x;
           if (k < nc) {
             const int c = c0 + k;
@@ -629,7 +805,9 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           int t = pass_tile(a, lon, NTL, i);
           if (t < 0) return -1;
           locate(a, sc, t);
-          if (!mask_done(a, s_mask, mwords, sc.s)) {
+          // contact tiles only (the bilateral rows' tiles have their own loop)
+          if (!mask_done(a, s_mask, mwords, sc.s) &&
+              (!a.nbil || (t - sc.t0) * kTileItems < sc.nc)) {
             *tile_out = t;
             return i;
           }
@@ -834,7 +1012,47 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         drain_warp_stages(stg, &a.ew->wait_limit_ns);
         return;
       }
+      nslot = 0;
       flush_run(a, run, ctl, single);
+      if (a.nbil) {
+        // then the bilateral rows' tiles: N gamma_new, the objective and
+        // residual items and the look-ahead step, without the cone projection
+        const T* wt = reinterpret_cast<const T*>(a.wd);
+        for (int i = 0;; ++i) {
+          const int t = pass_tile(a, lon, NTL, i);
+          if (t < 0) break;
+          locate(a, sc, t);
+          const int s = sc.s;
+          if (mask_done(a, s_mask, mwords, s)) continue;
+          const int kb = bil_tile_k0(t, sc.t0, sc.nc);
+          if (kb < 0) continue;
+          if (s != run.s) {
+            if (run.n) {
+              fold_parked<7, true>(a, s_def, nslot);
+              nslot = 0;
+            }
+            flush_run(a, run, ctl, single);
+            run.s = s;
+          }
+          load_ps(s);
+          const SegParams& P = a.seg[s];
+          const ProdScalars& ps = s_ps;
+          BilRows<T> br_{a.bil_off, wt, a.bG[ps.cur], a.bG[ps.nw], a.bG[ps.nw2], a.bNG[ps.cur],
+                         a.bNG[ps.nw], a.br, a.bq};
+          const bool bad = bil_product_tile<T>(br_, ps, P.bil0 + kb, P.nbil - kb, sc.nc > 0,
+                                               &s_def, nslot, t);
+          if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) seg_error(a, s, kErrNaN);
+          ++run.n;
+          if (++nslot == kMaxDefer) {
+            fold_parked<7, true>(a, s_def, nslot);
+            nslot = 0;
+          }
+        }
+        fold_parked<7, true>(a, s_def, nslot);
+        nslot = 0;
+        flush_run(a, run, ctl, single);
+      }
+
     }
     if (!grid_sync(a, kPhaseProduct, latch_product)) {
       drain_warp_stages(stg, &a.ew->wait_limit_ns);
@@ -856,7 +1074,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
 
   // ---- gamma = gamma_hat (APGD.cu:358) into the warm-start region; q = F gamma (FP64)
   {
-    int cs = -1;
+    int cs = -1, cbest = -1;
     const T* src = nullptr;
     for (int i = 0;; ++i) {
       const int t = cta_tile(a, NT, i);
@@ -865,11 +1083,23 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       const int s = sc.s;
       if (s != cs) {
         cs = s;
-        const int best = __ldcg(&a.sst[s].ctl.best);
-        src = best >= 0 ? a.G[best] : nullptr;
+        cbest = __ldcg(&a.sst[s].ctl.best);
+        src = cbest >= 0 ? a.G[cbest] : nullptr;
       }
       const SegParams& P = a.seg[s];
       const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
+      const int kb = a.nbil ? bil_tile_k0(t, sc.t0, nc) : -1;
+      if (kb >= 0) {
+        // the rows' gamma_hat (ones before the first accepted iterate)
+        for (int m = 0; m < kItemsPerThread; ++m) {
+          const int k = kb + m * kThreads + threadIdx.x;
+          if (k < P.nbil) {
+            const int r = P.bil0 + k;
+            a.bil_gam[r] = cbest >= 0 ? (double)a.bG[cbest][r] : 1.0;
+          }
+        }
+        continue;
+      }
       for (int m = 0; m < kItemsPerThread; ++m) {
         int k = k0 + m * kThreads + threadIdx.x;
         if (k < nc) {
@@ -895,7 +1125,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     return;
 
   // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v.
-  // Segments without contacts: v = Minv k, f_contact = 0 (System.cu:577-581).
+  // Segments with neither contacts nor bilateral rows: v = Minv k, f_contact = 0
+  // (System.cu:577-581); the rows' impulses enter f_c like the contacts'.
   for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
     if (b < a.nb) {
@@ -907,8 +1138,9 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         double4 k = a.k4[b];
         double mi = __ldg(a.minv + b);
         double4 v, fcv;
-        if (nc > 0) {
+        if (nc > 0 || P.nbil > 0) {
           double4 fc = gather_q<double, double4>(a, a.qd, b);
+          if (a.nbil) add_bilateral<double, double4>(a.bil_inc_start, a.bil_inc, a.bil_gam, b, fc);
           v = make_double4(mi * (k.x + fc.x), mi * (k.y + fc.y), mi * (k.z + fc.z), 0.0);
           const double invh = 1.0 / h;
           fcv = make_double4(invh * fc.x, invh * fc.y, invh * fc.z, 0.0);
@@ -926,13 +1158,15 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // warm-start length of every segment that solved (System::gamma_d resize)
   for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.nseg; s += gridDim.x * kThreads) {
     SegState& X = a.sst[s];
-    if (a.seg[s].active && X.nc > 0) X.gsize = X.nc;
+    if (a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0)) X.gsize = X.nc;
+    // System::time += h (System.cu:584), read by the next step's rows
+    if (a.nbil && a.seg[s].active) a.seg_time[s] = a.seg_time[s] + a.seg[s].h;
   }
   // matched warm start: where each body's A-contacts went in the warm region
   for (int b = blockIdx.x * kThreads + threadIdx.x; b < a.nb; b += gridDim.x * kThreads) {
     const int s = __ldg(a.bseg + b);
     const SegState& X = a.sst[s];
-    if (a.seg[s].active && X.nc > 0) {
+    if (a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0)) {
       a.ws[b] = a.cbase[b] + X.delta - X.c0;
       a.wc[b] = a.cnt_cont[b];
     }

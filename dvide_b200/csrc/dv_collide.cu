@@ -531,7 +531,8 @@ __global__ void __launch_bounds__(1024) k_seg_layout(int nseg, int nb,
     if (s < nseg && seg[s].active) {
       nc = cbase[seg[s].b1] - cbase[seg[s].b0];
       pad = (nc + kContactAlign - 1) / kContactAlign * kContactAlign;
-      nt = (nc + kTileItems - 1) / kTileItems;
+      // contact tiles, then the tiles of the bilateral rows
+      nt = (nc + kTileItems - 1) / kTileItems + (seg[s].nbil + kTileItems - 1) / kTileItems;
       if (nc > seg[s].wcap) atomicOr(&ew->err, kErrCapacity);  // warm-start region too small
     }
     long long xc = pad, xt = nt;

@@ -59,6 +59,53 @@ __global__ void __launch_bounds__(kThreads) k_violation_items(
   items[3 * (size_t)nc + k] = cv * cv;
 }
 
+// The same items with bilateral rows.  The reference reads entries 3 c,
+// 3 c + 1, 3 c + 2 of gamma and of D v + b, vectors whose first nbil entries
+// are the bilateral rows, with no offset (getNormalComponent,
+// calculateConeViolation, System.cu:1590-1603): flat entry j < nbil is row j,
+// entry j >= nbil component (j - nbil) % 3 of contact (j - nbil) / 3.
+__global__ void __launch_bounds__(kThreads) k_violation_items_flat(
+    int nc, int nbil, int c0, size_t S, int w0, size_t WS, const double* __restrict__ gamma,
+    const double* __restrict__ bil_gam, const double* __restrict__ bil_b,
+    const int2* __restrict__ bil_off, const double* __restrict__ F, const double* __restrict__ gap,
+    const uint32_t* __restrict__ ida, const uint32_t* __restrict__ idb,
+    const double4* __restrict__ v4, double h, double mu, double* __restrict__ items) {
+  int k = blockIdx.x * kThreads + threadIdx.x;
+  if (k >= nc) return;
+  const double* vd = reinterpret_cast<const double*>(v4);
+  auto gam = [&](long long j) -> double {
+    if (j < nbil) return bil_gam[j];
+    const long long q = j - nbil;
+    return gamma[(q % 3) * WS + w0 + q / 3];
+  };
+  // entry j of D v + b (b: the last step's)
+  auto dvb = [&](long long j) -> double {
+    if (j < nbil) {
+      const int2 o = bil_off[j];
+      const double dv = o.y >= 0 ? vd[o.x] - vd[o.y] : vd[o.x];
+      return bil_b[j] + dv;
+    }
+    const long long q = j - nbil;
+    const int row = (int)(q % 3);
+    const int c = c0 + (int)(q / 3);
+    const double4 va = v4[ida[c]], vb = v4[idb[c]];
+    const double d0 = va.x - vb.x, d1 = va.y - vb.y, d2 = va.z - vb.z;
+    const double* f = F + (size_t)(3 * row) * S + c;
+    const double dv = (f[0] * d0 + f[S] * d1) + f[2 * S] * d2;
+    return (row == 0 ? gap[c] / h : 0.0) + dv;
+  };
+  const long long j = 3LL * k;
+  const double g0 = gam(j), g1 = gam(j + 1), g2 = gam(j + 2);
+  const double vn = dvb(j);
+  double gt = sqrt(g1 * g1 + g2 * g2);
+  double cv = mu * g0 - gt;
+  if (cv > 0) cv = 0;
+  items[k] = g0;
+  items[(size_t)nc + k] = vn;
+  items[2 * (size_t)nc + k] = g0 * vn;
+  items[3 * (size_t)nc + k] = cv * cv;
+}
+
 __global__ void __launch_bounds__(kThreads) k_energy_items(int nb, int b0,
                                                            const double4* __restrict__ p4,
                                                            const double4* __restrict__ v4,
@@ -107,9 +154,15 @@ int Engine::ccp_violation(int s, double* out4) {
   if (ensure_red(4 * (size_t)nc + 2 * (size_t)(nt + 2)) != DV_OK) return DV_ERR_OOM;
   double* items = d_red_;
   double* part = d_red_ + 4 * (size_t)nc;
-  k_violation_items<<<(nc + kThreads - 1) / kThreads, kThreads, 0, st_>>>(
-      nc, X.c0, d.ccap, hseg_[s].wbase, d.wtotal, d.gamma, d.F, d.gap, d.ida, d.idb, d.v4,
-      P_[s].h, P_[s].mu, items);
+  if (hseg_[s].nbil > 0)
+    k_violation_items_flat<<<(nc + kThreads - 1) / kThreads, kThreads, 0, st_>>>(
+        nc, hseg_[s].nbil, X.c0, d.ccap, hseg_[s].wbase, d.wtotal, d.gamma,
+        d.bil_gam + hseg_[s].bil0, d.bil_b + hseg_[s].bil0, d.bil_off + hseg_[s].bil0, d.F, d.gap,
+        d.ida, d.idb, d.v4, P_[s].h, P_[s].mu, items);
+  else
+    k_violation_items<<<(nc + kThreads - 1) / kThreads, kThreads, 0, st_>>>(
+        nc, X.c0, d.ccap, hseg_[s].wbase, d.wtotal, d.gamma, d.F, d.gap, d.ida, d.idb, d.v4,
+        P_[s].h, P_[s].mu, items);
   ++launches_;
   ordered_sum_dev(items + 2 * (size_t)nc, nc, part, 0);
   ordered_sum_dev(items + 3 * (size_t)nc, nc, part + nt + 2, 1);

@@ -96,7 +96,7 @@ int Engine::alloc_contacts(size_t cap) {
   }
   dfree(q.q); dfree(q.inc); dfree(q.part); dfree(q.tseg); dfree(q.act_tiles);
   q.ccap = cap;
-  q.tcap = (int)(cap / kTileItems) + q.nseg + 1;
+  q.tcap = (int)(cap / kTileItems) + q.nseg + 1 + (q.nbil + kTileItems - 1) / kTileItems;
   TRY(dalloc(&q.ida, cap));
   TRY(dalloc(&q.idb, cap));
   TRY(dalloc(&q.F, 9 * cap));
@@ -600,6 +600,8 @@ int Engine::set_stream(cudaStream_t s) {
 int Engine::set_segment_params(int s, const dv_params& P) {
   if (s < 0 || s >= d.nseg) return DV_ERR_ARG;
   TRY(check_params(P));
+  // bilateral rows: APGD only (the reference's PGJ and PGS size their vectors 3 nc)
+  if (hseg_[s].nbil > 0 && P.solver != DV_SOLVER_APGD) return DV_ERR_UNSUPPORTED;
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   SegParams& G = hseg_[s];
   if (P.envelope > P_[s].envelope) {
@@ -628,6 +630,7 @@ int Engine::set_segment_params(int s, const dv_params& P) {
 int Engine::set_precision(int precision) {
   if (precision != DV_PREC_FP64 && precision != DV_PREC_MIXED) return DV_ERR_UNSUPPORTED;
   if (precision == d.precision) return DV_OK;
+  if (d.nbil > 0 && precision != DV_PREC_FP64) return DV_ERR_UNSUPPORTED;  // rows: FP64 only
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   d.precision = precision;
   max_ctas_ = apgd_max_ctas(precision, 2);
@@ -789,6 +792,11 @@ int Engine::step(int n) {
     const int m = n - done;
     TRY(ensure_records(m));
     DV_CUDA_TRY(cudaMemsetAsync(&d.ew->err, 0, sizeof(unsigned), st_));
+    // the bilateral rows' clock: System::time of every segment at the first
+    // step (the solve kernel advances it by h per step)
+    if (d.nbil)
+      DV_CUDA_TRY(cudaMemcpyAsync(d.seg_time, time_.data(), sizeof(double) * d.nseg,
+                                  cudaMemcpyHostToDevice, st_));
     for (int i = 0; i < m; ++i) TRY(enqueue_step(i));
     DV_CUDA_TRY(cudaStreamSynchronize(st_));
     DV_CUDA_TRY(cudaGetLastError());
@@ -882,6 +890,97 @@ int Engine::collide_only() {
     }
   }
   return DV_ERR_OOM;
+}
+
+int Engine::add_bilateral(int s, int dof_a, int dof_b, double velocity, double start_time) {
+  if (s < 0 || s >= d.nseg) return DV_ERR_ARG;
+  if (d.nseg != 1) return DV_ERR_UNSUPPORTED;
+  const int nbs = hseg_[s].b1 - hseg_[s].b0;
+  if (dof_a < 0 || dof_a >= 3 * nbs || dof_b >= 3 * nbs) {
+    dv_set_error_text("bilateral DOF index out of range");
+    return DV_ERR_ARG;
+  }
+  if (time_index_[s] > 0) {
+    // System::processConstraints copies the rows to the device once, at
+    // initializeSystem (System.cu:292-296, 303-315)
+    dv_set_error_text("bilateral constraints are added before the first step");
+    return DV_ERR_ARG;
+  }
+  if (P_[s].solver != DV_SOLVER_APGD || d.precision != DV_PREC_FP64) return DV_ERR_UNSUPPORTED;
+  if (dof_b < 0) dof_b = -1;
+  double p0 = 0.0;
+  if (dof_b < 0) {
+    // the DOF's position now (infoConstraintBilateralDOF.z, System.cu:310)
+    double p[3];
+    TRY(copy_state_out(hseg_[s].b0 + dof_a / 3, 1, p, nullptr));
+    p0 = p[dof_a % 3];
+  }
+  bil_a_.push_back(3 * hseg_[s].b0 + dof_a);
+  bil_b_.push_back(dof_b < 0 ? -1 : 3 * hseg_[s].b0 + dof_b);
+  bil_vel_.push_back(velocity);
+  bil_t0_.push_back(start_time);
+  bil_p0_.push_back(p0);
+  return upload_bilateral();
+}
+
+int Engine::upload_bilateral() {
+  DV_CUDA_TRY(cudaStreamSynchronize(st_));
+  const int n = (int)bil_a_.size();
+  const int nb = d.nb;
+  std::vector<int2> off(n);
+  std::vector<double4> info(n);
+  std::vector<std::vector<uint32_t>> per(nb);
+  for (int i = 0; i < n; ++i) {
+    const int a = bil_a_[i], b = bil_b_[i];
+    off[i] = make_int2(4 * (a / 3) + a % 3, b >= 0 ? 4 * (b / 3) + b % 3 : -1);
+    info[i] = make_double4(bil_vel_[i], bil_t0_[i], bil_p0_[i], 0.0);
+    per[a / 3].push_back(((uint32_t)i << 3) | ((uint32_t)(a % 3) << 1));
+    if (b >= 0) per[b / 3].push_back(((uint32_t)i << 3) | ((uint32_t)(b % 3) << 1) | 1u);
+  }
+  std::vector<int> start(nb + 1, 0);
+  std::vector<uint32_t> inc;
+  for (int b = 0; b < nb; ++b) {
+    start[b] = (int)inc.size();
+    inc.insert(inc.end(), per[b].begin(), per[b].end());
+  }
+  start[nb] = (int)inc.size();
+  dfree(d.bil_off); dfree(d.bil_info); dfree(d.bil_inc_start); dfree(d.bil_inc);
+  dfree(d.bil_work); dfree(d.bil_gam); dfree(d.bil_b);
+  TRY(dalloc(&d.bil_off, n));
+  TRY(dalloc(&d.bil_info, n));
+  TRY(dalloc(&d.bil_inc_start, (size_t)nb + 1));
+  TRY(dalloc(&d.bil_inc, inc.size()));
+  TRY(dalloc(&d.bil_work, 12 * (size_t)n));
+  TRY(dalloc(&d.bil_gam, n));
+  TRY(dalloc(&d.bil_b, n));
+  if (!d.seg_time) TRY(dalloc(&d.seg_time, (size_t)d.nseg));
+  DV_CUDA_TRY(cudaMemcpyAsync(d.bil_off, off.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(d.bil_info, info.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, st_));
+  DV_CUDA_TRY(cudaMemcpyAsync(d.bil_inc_start, start.data(), sizeof(int) * (nb + 1),
+                              cudaMemcpyHostToDevice, st_));
+  if (!inc.empty())
+    DV_CUDA_TRY(cudaMemcpyAsync(d.bil_inc, inc.data(), sizeof(uint32_t) * inc.size(),
+                                cudaMemcpyHostToDevice, st_));
+  // System::gamma_d starts as zeros (System.cu:185); b is set by the first step
+  DV_CUDA_TRY(cudaMemsetAsync(d.bil_gam, 0, sizeof(double) * n, st_));
+  DV_CUDA_TRY(cudaMemsetAsync(d.bil_b, 0, sizeof(double) * n, st_));
+  DV_CUDA_TRY(cudaMemsetAsync(d.bil_work, 0, sizeof(double) * 12 * n, st_));
+  d.nbil = n;
+  hseg_[0].bil0 = 0;
+  hseg_[0].nbil = n;
+  TRY(upload_segments());
+  if ((int)(d.ccap / kTileItems) + d.nseg + 1 + (n + kTileItems - 1) / kTileItems > d.tcap)
+    TRY(alloc_contacts(d.ccap));
+  drop_graph();
+  DV_CUDA_TRY(cudaStreamSynchronize(st_));
+  return DV_OK;
+}
+
+int Engine::get_bilateral_gamma(int s, std::vector<double>& g) {
+  const int n = hseg_[s].nbil;
+  g.assign(n, 0.0);
+  if (n == 0) return DV_OK;
+  return download(g.data(), d.bil_gam + hseg_[s].bil0, sizeof(double) * n);
 }
 
 int Engine::get_gamma(int s, std::vector<double>& g, int* n) {

@@ -85,6 +85,15 @@ class Engine {
   int precision() const { return d.precision; }
   int set_precision(int precision);
 
+  // Bilateral DOF row of segment s (System::addBilateralConstraintDOF,
+  // System.cu:510-532): DOF dof_a (3 body + axis) minus DOF dof_b (< 0: dof_a
+  // against its position now) at `velocity` from `start_time` on.  Engines of
+  // one segment, FP64 APGD, before the first step.
+  int add_bilateral(int s, int dof_a, int dof_b, double velocity, double start_time);
+  int num_bilateral(int s) const { return hseg_[s].nbil; }
+  // The rows' impulses of the last solve (System::gamma_d's first entries).
+  int get_bilateral_gamma(int s, std::vector<double>& g);
+
   // Warm-start (System::gamma_d) of segment s.
   int get_gamma(int s, std::vector<double>& g, int* n);
   int set_gamma(int s, const double* g, int n);
@@ -142,6 +151,7 @@ class Engine {
   void drop_graph();
   int ensure_records(int n);
   int upload_segments();
+  int upload_bilateral();
   int sync_words();
   int ensure_red(size_t n);
   void ordered_sum_dev(const double* items, int n, double* part, int slot);
@@ -153,6 +163,9 @@ class Engine {
   std::vector<dv_params> P_;
   std::vector<double> time_;
   std::vector<int> time_index_;
+  // bilateral rows (host copy; segment 0 of a one-segment engine)
+  std::vector<int> bil_a_, bil_b_;
+  std::vector<double> bil_vel_, bil_t0_, bil_p0_;
   int max_ctas_ = 1;
   SolveConfig cfg_{1, 1, 0, 2};
   bool cfg_user_ = false;

@@ -27,6 +27,11 @@
 //                 partial sums are folded per segment in a fixed order.
 //   incidence:    per body, its contacts in ascending contact order: those
 //                 where it is B (bit 31 set), then those where it is A.
+//   bilateral:    DOF rows (System::addBilateralConstraintDOF): segment s
+//                 owns rows [bil0, bil0 + nbil) and the tiles after its
+//                 contact tiles, ceil(nbil / 512) of them (a row is one item);
+//                 per body, its rows in ascending order (bil_inc); iterates
+//                 and products of the rows in 12 planes of nbil doubles.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -61,6 +66,7 @@ struct SegParams {
   int l0, l1;               // large bodies (boxes) in large_ids
   int cell_base, cell_cap;  // global cell ids [cell_base, cell_base + cell_cap)
   int wbase, wcap;          // warm-start region [wbase, wbase + wcap) of the gamma arena
+  int bil0, nbil;           // bilateral DOF rows [bil0, bil0 + nbil) (System.cu:510-532)
 };
 
 // Scalar state of one APGD solve (APGD.cu:208-223, 266-332).  Iterates live in
@@ -194,6 +200,16 @@ struct SceneDev {
   int4* act_bodies = nullptr; // act_bcap: (first body, end body, segment, 0), at most 256 bodies each
   size_t act_bcap = 0;
   double* part = nullptr;     // reduction partials, 9 x tcap
+  // bilateral DOF rows (FP64 APGD only)
+  int nbil = 0;               // rows of all segments
+  int2* bil_off = nullptr;    // per row: element offsets 4 body + axis of DOF A, B (-1: none)
+  double4* bil_info = nullptr;  // per row: velocity, start time, p0 (System.cu:1526-1544), 0
+  int* bil_inc_start = nullptr; // nb + 1
+  uint32_t* bil_inc = nullptr;  // (row << 3) | (axis << 1) | (1: the row's -1 entry)
+  double* bil_work = nullptr; // 12 planes of nbil: G[0..4], NG[0..4], r, q
+  double* bil_gam = nullptr;  // the rows' impulses of the last solve (System::gamma_d head)
+  double* bil_b = nullptr;    // b of the rows at the last step
+  double* seg_time = nullptr; // nseg: System::time at the step's start (rows with a velocity)
   // warm-start arena (System::gamma_d of every segment): 3 planes of stride
   // wtotal; segment s owns [wbase, wbase + wcap), positional within it
   double* gamma = nullptr;

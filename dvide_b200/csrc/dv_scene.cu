@@ -250,6 +250,21 @@ DV_API int dv_set_gamma(dv_scene* s, const double* gamma, int32_t n) {
   return s->E.set_gamma(0, gamma, n);
 }
 
+DV_API int dv_add_bilateral_dof(dv_scene* s, int32_t dof_a, int32_t dof_b, double velocity,
+                                double start_time) {
+  if (!s) return DV_ERR_ARG;
+  return s->E.add_bilateral(0, dof_a, dof_b, velocity, start_time);
+}
+
+DV_API int dv_get_bilateral_gamma(dv_scene* s, double* gamma, int32_t cap, int32_t* n) {
+  if (!s) return DV_ERR_ARG;
+  std::vector<double> g;
+  TRY(s->E.get_bilateral_gamma(0, g));
+  if (n) *n = (int32_t)g.size();
+  if (gamma && cap > 0) memcpy(gamma, g.data(), sizeof(double) * std::min((size_t)cap, g.size()));
+  return DV_OK;
+}
+
 DV_API int dv_ccp_violation(dv_scene* s, double* out4) {
   if (!s || !out4) return DV_ERR_ARG;
   return s->E.ccp_violation(0, out4);

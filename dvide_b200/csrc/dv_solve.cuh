@@ -75,6 +75,19 @@ struct KArgs {
   EngineWords* ew;
   int* act_tiles;          // work lists of the iterating passes (EngineWords::act_on)
   int4* act_bodies;
+  // bilateral DOF rows (nbil = 0: none; FP64 iterates only)
+  int nbil;
+  const int2* __restrict__ bil_off;
+  const double4* __restrict__ bil_info;
+  const int* __restrict__ bil_inc_start;
+  const uint32_t* __restrict__ bil_inc;
+  T* bG[5];            // iterates of the rows (the contacts' G[k] slot k)
+  T* bNG[5];           // their products
+  T* br;               // Schur vector of the rows
+  T* bq;               // the rows' share of the body gather (the contacts' q)
+  double* bil_gam;     // warm start / solution of the rows
+  double* bil_b;       // b of the rows (for the CCP violation)
+  double* seg_time;    // System::time of each segment at the step's start
 };
 
 template <class T>
@@ -611,6 +624,40 @@ __device__ inline V gather_q(const K& a, const V* q, int b) {
   return r;
 }
 
+// Bilateral DOF rows.  Tile t of a segment with contacts [0, nc) and tiles
+// starting at t0 is a tile of its rows when it lies past the contact tiles;
+// returns the tile's first row (segment-relative), else -1.
+__device__ inline int bil_tile_k0(int t, int t0, int nc) {
+  const int ntc = (nc + kTileItems - 1) / kTileItems;
+  return (t - t0) >= ntc ? (t - t0 - ntc) * kTileItems : -1;
+}
+
+// Row i of D w (System.cu:622-638): w[A] - w[B], or w[A] for one DOF.  o holds
+// the DOFs' element offsets (4 body + axis) into a 4-wide body vector.
+template <class T>
+__device__ inline T bil_dw(int2 o, const T* w) {
+  const T wa = w[o.x];
+  return o.y >= 0 ? wa - w[o.y] : wa;
+}
+
+// The rows' part of (D^T x)_b, added after the contacts' part: +x_i at DOF A,
+// -x_i at DOF B, ascending rows.  x is written inside the kernel (read through L2).
+template <class T, class V>
+__device__ inline void add_bilateral(const int* __restrict__ start, const uint32_t* __restrict__ inc,
+                                     const T* x, int b, V& s) {
+  const int e0 = __ldg(start + b), e1 = __ldg(start + b + 1);
+  for (int e = e0; e < e1; ++e) {
+    const uint32_t code = __ldg(inc + e);
+    const T v = __ldcg(x + (code >> 3));
+    const int k = (code >> 1) & 3;
+    if (code & 1u) {
+      if (k == 0) s.x = s.x - v; else if (k == 1) s.y = s.y - v; else s.z = s.z - v;
+    } else {
+      if (k == 0) s.x = s.x + v; else if (k == 1) s.y = s.y + v; else s.z = s.z + v;
+    }
+  }
+}
+
 // A solver error of segment s; with stop_on_seg_err it also stops the steps
 // that follow (every kernel checks EngineWords::err first).
 // A segment's APGD words as its controller finds them: controllers of earlier
@@ -679,6 +726,7 @@ __device__ inline void body_w(const KArgs<T>& a, int b) {
   double mi = __ldg(a.minv + b);
   if (mi != 0.0) {
     V s = gather_q<T, V>(a, q, b);
+    if (a.nbil) add_bilateral<T, V>(a.bil_inc_start, a.bil_inc, a.bq, b, s);
     T m = (T)mi;
     V o;
     o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
@@ -921,6 +969,22 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   a.ew = sd.ew;
   a.act_tiles = sd.act_tiles;
   a.act_bodies = sd.act_bodies;
+  a.nbil = sizeof(T) == sizeof(double) ? sd.nbil : 0;
+  a.bil_off = sd.bil_off;
+  a.bil_info = sd.bil_info;
+  a.bil_inc_start = sd.bil_inc_start;
+  a.bil_inc = sd.bil_inc;
+  T* bw = a.nbil ? reinterpret_cast<T*>(sd.bil_work) : nullptr;
+  const size_t nbl = (size_t)sd.nbil;
+  for (int k = 0; k < 5; ++k) {
+    a.bG[k] = bw ? bw + k * nbl : nullptr;
+    a.bNG[k] = bw ? bw + (5 + k) * nbl : nullptr;
+  }
+  a.br = bw ? bw + 10 * nbl : nullptr;
+  a.bq = bw ? bw + 11 * nbl : nullptr;
+  a.bil_gam = sd.bil_gam;
+  a.bil_b = sd.bil_b;
+  a.seg_time = sd.seg_time;
   return a;
 }
 

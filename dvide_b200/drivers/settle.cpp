@@ -3,8 +3,12 @@
 // spheres (r = 0.05 m, rho = 2600) on a 10x10x10 lattice in an open box of
 // five fixed boxes, mu = 0.25, h = 1e-3, APGD with warm start.
 // Usage: settle <steps> <solverType> <tolerance> [maxIterations] [warmStartMode]
+//               [pinnedSpheres]
 // Prints one line per step: time, contacts, iterations, weight carried by
-// the fixed boxes, and the four CCP violations.
+// the fixed boxes, and the four CCP violations.  With pinnedSpheres = n > 0
+// the x and y DOFs of the first n spheres are held by bilateral constraints
+// (System::addBilateralConstraintDOF, as the reference drivers pin DOFs) and
+// the largest drift of those DOFs is printed at the end.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -27,6 +31,7 @@ int main(int argc, char** argv) {
   double tolerance = argc > 3 ? atof(argv[3]) : 1e-4;
   int maxIterations = argc > 4 ? atoi(argv[4]) : 1000;
   int warmStartMode = argc > 5 ? atoi(argv[5]) : 1;
+  int pinned = argc > 6 ? atoi(argv[6]) : 0;
 
   System* sys = new System(solverType);
   sys->setTimeStep(1e-3);
@@ -61,6 +66,14 @@ int main(int argc, char** argv) {
         totalWeight += b->getMass() * 9.81;
         sys->add(b);
       }
+  std::vector<double> pin0;
+  for (int i = 0; i < pinned; ++i) {
+    Body* b = sys->bodies[5 + i];
+    sys->addBilateralConstraintDOF(3 * (5 + i), -1);
+    sys->addBilateralConstraintDOF(3 * (5 + i) + 1, -1);
+    pin0.push_back(b->getPosition().x);
+    pin0.push_back(b->getPosition().y);
+  }
   int rc = sys->initializeSystem();
   if (rc != 0) {
     fprintf(stderr, "initializeSystem failed: %s\n", dv_status_string(rc));
@@ -79,6 +92,13 @@ int main(int argc, char** argv) {
     for (int i = 0; i < 5; ++i) weight -= sys->f_contact_h[3 * i + 2];
     printf("%f, %u, %d, %.6f, %g, %g, %g, %g, %f\n", sys->time, sys->collisionDetector->numCollisions,
            sys->solver->iterations, weight, v.x, v.y, v.z, v.w, sys->elapsedTime);
+  }
+  if (pinned > 0) {
+    std::vector<double> p = sys->p_d;
+    double drift = 0;
+    for (int i = 0; i < pinned; ++i)
+      for (int k = 0; k < 2; ++k) drift = fmax(drift, fabs(p[3 * (5 + i) + k] - pin0[2 * i + k]));
+    printf("pinned drift: %g\n", drift);
   }
   sys->exportSystem("settle_final.csv");
   delete sys;

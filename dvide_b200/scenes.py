@@ -46,6 +46,9 @@ class Scene:
     # impulses of the previous solve (nc x 3, in that solve's contact order),
     # the warm start the first step reads: System::gamma_d carried over
     gamma: np.ndarray | None = None
+    # bilateral DOF rows (System::addBilateralConstraintDOF): tuples
+    # (dof_a, dof_b, velocity, start_time), DOF 3 i + k = axis k of body i
+    bilateral: list | None = None
 
     @property
     def nb(self) -> int:
@@ -54,7 +57,8 @@ class Scene:
     def copy(self) -> "Scene":
         return Scene(self.pos.copy(), self.vel.copy(), self.mass.copy(), self.geom.copy(),
                      self.fixed.copy(), self.family.copy(), dict(self.params), self.name,
-                     None if self.gamma is None else self.gamma.copy())
+                     None if self.gamma is None else self.gamma.copy(),
+                     None if self.bilateral is None else list(self.bilateral))
 
 
 def default_params(**kw) -> dict:
@@ -237,3 +241,36 @@ def random_cluster(seed, n=40, box=True, radius=0.05, mu=0.25, h=1e-3, warm_star
                             max_iterations=max_iterations, warm_start=warm_start)
     vel = rng.normal(0.0, 0.05, size=(n, 3))
     return _assemble(boxes, pos, r, 2600.0, params, f"cluster_{seed}_{n}", spheres_vel=vel)
+
+
+def free_balls(n=2, spacing=0.5, radius=0.05, h=1e-3, warm_start=1, vel=None,
+               tolerance=1e-10, max_iterations=2000) -> Scene:
+    """n unit-density spheres far apart in free flight under gravity -z (no
+    contacts ever): a scene whose only constraints are bilateral rows."""
+    pos = np.zeros((n, 3))
+    pos[:, 0] = spacing * np.arange(n)
+    pos[:, 2] = 1.0
+    params = default_params(h=h, gravity=(0.0, 0.0, -G), tolerance=tolerance,
+                            max_iterations=max_iterations, warm_start=warm_start)
+    sc = _assemble([], pos, np.full(n, radius), 1000.0, params, f"free_balls_{n}",
+                   spheres_vel=None if vel is None else np.asarray(vel, dtype=np.float64))
+    return sc
+
+
+def bilateral_cluster(seed, n=64, warm_start=1, h=1e-3, max_iterations=400,
+                      tolerance=1e-6) -> Scene:
+    """random_cluster with bilateral rows (System::addBilateralConstraintDOF,
+    as the reference drivers pin DOFs): the first sphere held in x (in z it
+    could start inside the floor, an infeasible pair of rows), the second
+    and third spheres' y coupled (a two-DOF row drives y_A - y_B to 0; these
+    two differ by the lattice jitter only), the fourth sphere's y moved at
+    0.1 m/s from t = 2 h on, and a row on a fixed box's DOF (a zero row of N)."""
+    sc = random_cluster(seed, n=n, warm_start=warm_start, h=h,
+                        max_iterations=max_iterations, tolerance=tolerance)
+    s0 = int(np.argmax(sc.fixed == 0))  # first sphere (the boxes come first)
+    sc.bilateral = [(3 * s0, -1, 0.0, 0.0),
+                    (3 * (s0 + 1) + 1, 3 * (s0 + 2) + 1, 0.0, 0.0),
+                    (3 * (s0 + 3) + 1, -1, 0.1, 2 * h),
+                    (0, -1, 0.0, 0.0)]
+    sc.name = f"bilateral_{seed}_{n}"
+    return sc

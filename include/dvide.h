@@ -131,6 +131,21 @@ DV_API int dv_get_contacts(dv_scene* s, uint32_t* a, uint32_t* b, double* nP, do
 DV_API int dv_get_gamma(dv_scene* s, double* gamma, int32_t cap, int32_t* n);
 /* Overwrites the warm-start buffer (length n contacts). */
 DV_API int dv_set_gamma(dv_scene* s, const double* gamma, int32_t n);
+/* System::addBilateralConstraintDOF(DOFA, DOFB, velocity, startTime)
+ * (System.cu:510-532; the two-argument form is velocity 0, start time 0): a
+ * scalar constraint row, +1 at DOF dof_a and -1 at DOF dof_b, where DOF
+ * 3 i + k is axis k of body i; dof_b < 0 holds DOF dof_a alone at its
+ * position at this call.  Its stabilisation b = (violation minus velocity
+ * times the time since start_time) / h (System.cu:1526-1544).  Only before the
+ * scene's first step (the reference copies the rows to the device once, at
+ * initializeSystem); APGD in FP64 only: DV_ERR_UNSUPPORTED for PGJ, PGS and
+ * the mixed precision, here and in dv_set_params. */
+DV_API int dv_add_bilateral_dof(dv_scene* s, int32_t dof_a, int32_t dof_b, double velocity,
+                                double start_time);
+/* The bilateral rows' impulses of the last solve (the first entries of the
+ * reference's System::gamma_d), in the order the rows were added; their count
+ * through *n. */
+DV_API int dv_get_bilateral_gamma(dv_scene* s, double* gamma, int32_t cap, int32_t* n);
 /* Contact frames n, u, v (9 per contact) and Schur vector r (3 per contact)
  * of the last step: System.cu:753-762, 1561-1580. */
 DV_API int dv_get_frames(dv_scene* s, double* F);

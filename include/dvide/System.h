@@ -43,6 +43,11 @@ class System {
   double tol;
   int solverType;
   int sync_params();
+  struct BilateralDOF {
+    int dofA, dofB;
+    double velocity, startTime;
+  };
+  std::vector<BilateralDOF> bilaterals;  // handed to the scene at initializeSystem
 
  public:
   System();
@@ -69,6 +74,11 @@ class System {
   void setTimeStep(double step_size) { h = step_size; }
   void setFrictionCoefficient(double mu) { frictionCoefficient = mu; }
   int add(Body* body);
+  // System.cu:510-532: +1 at DOF DOFA (3 body + axis), -1 at DOF DOFB, or DOFA
+  // alone held at its position when DOFB < 0; moving at `velocity` from
+  // `startTime` on.  Added before initializeSystem, as in the reference.
+  int addBilateralConstraintDOF(int DOFA, int DOFB);
+  int addBilateralConstraintDOF(int DOFA, int DOFB, double velocity, double startTime);
   int initializeSystem();
   int DoTimeStep();
   // applied forces are not part of the reference dynamics (System.cu:1510)

@@ -104,10 +104,11 @@ double tree256(double* s) {
   return W[0];
 }
 
-double ordered_sum(const double* v, int64_t n) {
-  if (n <= 0) return 0.0;
-  int64_t T = (n + 511) / 512;
-  std::vector<double> P(T);
+/* Partials of the tiles of n items, appended to P. */
+void tile_partials(const double* v, int64_t n, std::vector<double>& P) {
+  if (n <= 0) return;
+  const int64_t T = (n + 511) / 512, base = (int64_t)P.size();
+  P.resize(base + T);
 #pragma omp parallel for schedule(static)
   for (int64_t t = 0; t < T; ++t) {
     double s[256];
@@ -119,8 +120,12 @@ double ordered_sum(const double* v, int64_t n) {
       }
       s[j] = acc;
     }
-    P[t] = tree256(s);
+    P[base + t] = tree256(s);
   }
+}
+
+double fold_partials(const std::vector<double>& P) {
+  const int64_t T = (int64_t)P.size();
   double a[256];
   for (int j = 0; j < 256; ++j) {
     double acc = 0.0;
@@ -128,6 +133,23 @@ double ordered_sum(const double* v, int64_t n) {
     a[j] = acc;
   }
   return tree256(a);
+}
+
+double ordered_sum(const double* v, int64_t n) {
+  if (n <= 0) return 0.0;
+  std::vector<double> P;
+  tile_partials(v, n, P);
+  return fold_partials(P);
+}
+
+/* Two item lists whose tiles are folded as one list: the contacts' tiles,
+ * then the tiles of the bilateral rows (a scene's tile range on the GPU). */
+double ordered_sum2(const double* v, int64_t n, const double* w, int64_t m) {
+  if (n <= 0 && m <= 0) return 0.0;
+  std::vector<double> P;
+  tile_partials(v, n, P);
+  tile_partials(w, m, P);
+  return fold_partials(P);
 }
 
 /* APGD.cu:47-78, friction-cone projection of one contact impulse. */
@@ -181,33 +203,53 @@ struct Scene {
   /* body incidence, ascending contact order, sign +1 = body A */
   std::vector<int> incStart, incC;
   std::vector<signed char> incS;
+  /* bilateral DOF constraints (System.cu:510-532, 622-638, 1526-1544): one
+   * scalar row each, +1 at DOF A and -1 at DOF B (B < 0: DOF A alone).  The
+   * reference puts these rows ahead of the contacts; every solve vector here
+   * holds the contacts' 3 nc entries, then the nbil bilateral entries. */
+  int nbil = 0;
+  std::vector<int> bilA, bilB;
+  std::vector<double> bilVel, bilT0, bilP0;  // infoConstraintBilateralDOF (x, y, z)
+  std::vector<double> gammaB;                // bilateral impulses of the last solve (0 before)
+  std::vector<double> bB;                    // b of the bilateral rows at the last step
+  /* per body, its bilateral entries in ascending row order (A before B):
+   * (row << 3) | (axis << 1) | (1 for the -1 entry of DOF B) */
+  std::vector<int> bincStart, binc;
   or_stats st;
   double time = 0;
   int timeIndex = 0;
 };
 
 /* ------------------------------ reductions ------------------------------ */
+/* x . y over a solve vector (contacts, then bilateral rows): one item per
+ * contact and one per bilateral row, the contacts' tiles first. */
 double dotv(const Scene& S, const double* x, const double* y, int nc) {
+  const int nbil = S.nbil;
+  const double* xb = x + 3 * (int64_t)nc;
+  const double* yb = y + 3 * (int64_t)nc;
   if (S.P.reduce_mode == 1) {
+    /* the flat order of the reference's vectors: bilateral rows first */
     double s = 0.0;
+    for (int i = 0; i < nbil; ++i) s = s + xb[i] * yb[i];
     for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) s = s + x[i] * y[i];
     return s;
   }
-  std::vector<double> it(nc);
+  std::vector<double> it(nc), itb(nbil);
 #pragma omp parallel for schedule(static)
   for (int c = 0; c < nc; ++c) {
     const double* a = x + 3 * c;
     const double* b = y + 3 * c;
     it[c] = (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
   }
-  return ordered_sum(it.data(), nc);
+  for (int i = 0; i < nbil; ++i) itb[i] = xb[i] * yb[i];
+  return ordered_sum2(it.data(), nc, itb.data(), nbil);
 }
 
 double nrm2v(const Scene& S, const double* x, int nc) { return sqrt(dotv(S, x, x, nc)); }
 
-double nrmmaxv(const double* x, int nc, int* nan_flag) {
+double nrmmaxv(const Scene& S, const double* x, int nc, int* nan_flag) {
   double m = 0.0;
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) {
+  for (int64_t i = 0; i < 3 * (int64_t)nc + S.nbil; ++i) {
     double a = fabs(x[i]);
     if (a != a) *nan_flag = 1;
     if (a > m) m = a;
@@ -462,6 +504,25 @@ void build_frames(Scene& S) {
   }
 }
 
+/* The bilateral rows' part of (D^T x)_b, added after the contacts' part:
+ * +x_i at DOF A, -x_i at DOF B of row i (System.cu:622-638), ascending rows. */
+inline void add_bilateral_DT(const Scene& S, const double* x, int b, double* acc) {
+  if (!S.nbil) return;
+  const double* xb = x + 3 * (int64_t)S.nc;
+  for (int e = S.bincStart[b]; e < S.bincStart[b + 1]; ++e) {
+    const int code = S.binc[e];
+    const int row = code >> 3, k = (code >> 1) & 3;
+    if (code & 1) acc[k] = acc[k] - xb[row];
+    else acc[k] = acc[k] + xb[row];
+  }
+}
+
+/* The bilateral rows of D w: w[A] - w[B], or w[A]. */
+inline void bilateral_D(const Scene& S, const double* w, double* out) {
+  for (int i = 0; i < S.nbil; ++i)
+    out[i] = S.bilB[i] >= 0 ? w[S.bilA[i]] - w[S.bilB[i]] : w[S.bilA[i]];
+}
+
 /* D^T x (one value per body DOF). */
 void apply_DT(const Scene& S, const double* x, double* out) {
   int nb = S.nb;
@@ -480,6 +541,7 @@ void apply_DT(const Scene& S, const double* x, double* out) {
         }
         out[3 * b + k] = y;
       }
+      add_bilateral_DT(S, x, b, &out[3 * b]);
     }
     return;
   }
@@ -496,6 +558,7 @@ void apply_DT(const Scene& S, const double* x, double* out) {
         else acc[k] = acc[k] - q;
       }
     }
+    add_bilateral_DT(S, x, b, acc);
     out[3 * b] = acc[0];
     out[3 * b + 1] = acc[1];
     out[3 * b + 2] = acc[2];
@@ -523,6 +586,7 @@ void apply_D(const Scene& S, const double* w, double* out) {
         out[3 * c + row] = y;
       }
     }
+    bilateral_D(S, w, out + 3 * (int64_t)nc);
     return;
   }
 #pragma omp parallel for schedule(static)
@@ -536,6 +600,7 @@ void apply_D(const Scene& S, const double* w, double* out) {
       out[3 * c + row] = (f[0] * d0 + f[1] * d1) + f[2] * d2;
     }
   }
+  bilateral_D(S, w, out + 3 * (int64_t)nc);
 }
 
 /* APGD.cu:81-87: gammaTmp = D (Minv (D^T x)). */
@@ -546,31 +611,31 @@ void schur(const Scene& S, const double* x, double* out, std::vector<double>& bo
   apply_D(S, bodytmp.data(), out);
 }
 
+/* APGD.cu:90-102 with N src already available.  gdiff = 1 / (nc + nbil)^2
+ * (:92); without contacts the reference skips the projection and both axpby
+ * (:96-100), and the residual is max |N src + r|. */
+double residual_from(const Scene& S, const double* src, const double* Nsrc, std::vector<double>& T,
+                     int* nan_flag) {
+  const int nc = S.nc;
+  const int64_t n = 3 * (int64_t)nc + S.nbil;
+  const double m = (double)(nc + S.nbil);
+  double gdiff = 1.0 / (m * m);
+  for (int64_t i = 0; i < n; ++i) T[i] = S.r[i] + Nsrc[i];
+  if (nc) {
+    for (int64_t i = 0; i < n; ++i) T[i] = src[i] + (-gdiff) * T[i];
+    for (int c = 0; c < nc; ++c) project3(&T[3 * c], S.P.mu);
+    double a = 1.0 / gdiff, b = -1.0 / gdiff;
+    for (int64_t i = 0; i < n; ++i) T[i] = a * src[i] + b * T[i];
+  }
+  return nrmmaxv(S, T.data(), nc, nan_flag);
+}
+
 /* APGD.cu:90-102 */
 double get_residual(const Scene& S, const double* src, std::vector<double>& T,
                     std::vector<double>& bt, int* nan_flag) {
-  int nc = S.nc;
-  double gdiff = 1.0 / ((double)nc * (double)nc);
-  schur(S, src, T.data(), bt);
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = S.r[i] + T[i];
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = src[i] + (-gdiff) * T[i];
-  for (int c = 0; c < nc; ++c) project3(&T[3 * c], S.P.mu);
-  double a = 1.0 / gdiff, b = -1.0 / gdiff;
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = a * src[i] + b * T[i];
-  return nrmmaxv(T.data(), nc, nan_flag);
-}
-
-/* APGD.cu:90-102 with N src already available. */
-double residual_from(const Scene& S, const double* src, const double* Nsrc, std::vector<double>& T,
-                     int* nan_flag) {
-  int nc = S.nc;
-  double gdiff = 1.0 / ((double)nc * (double)nc);
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = S.r[i] + Nsrc[i];
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = src[i] + (-gdiff) * T[i];
-  for (int c = 0; c < nc; ++c) project3(&T[3 * c], S.P.mu);
-  double a = 1.0 / gdiff, b = -1.0 / gdiff;
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) T[i] = a * src[i] + b * T[i];
-  return nrmmaxv(T.data(), nc, nan_flag);
+  std::vector<double> N(3 * (size_t)S.nc + S.nbil);
+  schur(S, src, N.data(), bt);
+  return residual_from(S, src, N.data(), T, nan_flag);
 }
 
 /* warm_start 2 (an opt-in improvement over the reference, not parity
@@ -617,12 +682,43 @@ void resize_gamma(Scene& S) {
   if (S.gsize < nc)
     for (int64_t i = 3 * (int64_t)S.gsize; i < n3; ++i) S.gamma[i] = 0.0;
   S.gsize = nc;
-  if (!S.P.warm_start)
+  if (!S.P.warm_start && S.nbil == 0) {
     for (int c = 0; c < nc; ++c) {
       S.gamma[3 * c] = 1.0;
       S.gamma[3 * c + 1] = 0.0;
       S.gamma[3 * c + 2] = 0.0;
     }
+  } else if (!S.P.warm_start) {
+    /* initializeImpulseVector_APGD (APGD.cu:114-120, called at :200) writes
+     * (1, 0, 0) to flat entries 0 .. 3 nc - 1 of the vector whose first nbil
+     * entries are the bilateral rows (no offset): flat entry j < 3 nc takes
+     * 1 if j is a multiple of 3, else 0; entries from 3 nc on keep what the
+     * resize kept (the last solve's value at that position, or 0). */
+    const int64_t lim = 3 * (int64_t)nc;
+    for (int i = 0; i < S.nbil; ++i)
+      if (i < lim) S.gammaB[i] = (i % 3 == 0) ? 1.0 : 0.0;
+    for (int64_t j = 0; j < n3; ++j) {
+      const int64_t f = S.nbil + j;
+      if (f < lim) S.gamma[j] = (f % 3 == 0) ? 1.0 : 0.0;
+    }
+  }
+}
+
+/* The solve's starting vector: the contacts' held impulses, then the
+ * bilateral rows'. */
+std::vector<double> solve_vector(const Scene& S) {
+  const int64_t n3 = 3 * (int64_t)S.nc;
+  std::vector<double> x(n3 + S.nbil);
+  for (int64_t i = 0; i < n3; ++i) x[i] = S.gamma[i];
+  for (int i = 0; i < S.nbil; ++i) x[n3 + i] = S.gammaB[i];
+  return x;
+}
+
+/* gamma = gamma_hat (APGD.cu:358), split back into contacts and rows. */
+void store_solution(Scene& S, const std::vector<double>& x) {
+  const int64_t n3 = 3 * (int64_t)S.nc;
+  for (int64_t i = 0; i < n3; ++i) S.gamma[i] = x[i];
+  for (int i = 0; i < S.nbil; ++i) S.gammaB[i] = x[n3 + i];
 }
 
 /* APGD.cu:164-361 in the order the GPU evaluates it.  The reference computes
@@ -633,10 +729,9 @@ void resize_gamma(Scene& S) {
  * residual) plus one per backtrack.  The first iteration's N y_0 is a product. */
 void apgd_solve_fused(Scene& S) {
   int nc = S.nc;
-  int64_t n3 = 3 * (int64_t)nc;
+  int64_t n3 = 3 * (int64_t)nc + S.nbil;  // contacts, then bilateral rows
   resize_gamma(S);
-  double* gamma = S.gamma.data();
-  std::vector<double> Gc(gamma, gamma + n3), Gp(n3, 0.0), NGc(n3), NGp(n3, 0.0);
+  std::vector<double> Gc = solve_vector(S), Gp(n3, 0.0), NGc(n3), NGp(n3, 0.0);
   std::vector<double> gNew(n3), NgNew(n3), g(n3), y(n3), Ny(n3), T(n3), best(n3, 1.0), bt;
   double theta = 1.0, thetaNew = theta, Beta = 0.0, obj1 = 0.0, obj2 = 0.0;
   double residual = 10e30;
@@ -712,7 +807,7 @@ void apgd_solve_fused(Scene& S) {
   (void)have_best;
   schur(S, best.data(), T.data(), bt);
   double objective = 0.5 * dotv(S, best.data(), T.data(), nc) + dotv(S, best.data(), S.r.data(), nc);
-  for (int64_t i = 0; i < n3; ++i) gamma[i] = best[i];
+  store_solution(S, best);
   S.st.iterations = k;
   S.st.backtracks = backtracks;
   S.st.residual = residual;
@@ -724,12 +819,11 @@ void apgd_solve_fused(Scene& S) {
 /* APGD.cu:164-361, literally: four Schur products per iteration. */
 void apgd_solve(Scene& S) {
   int nc = S.nc;
-  int64_t n3 = 3 * (int64_t)nc;
+  int64_t n3 = 3 * (int64_t)nc + S.nbil;  // contacts, then bilateral rows
   resize_gamma(S);
-  double* gamma = S.gamma.data();
+  std::vector<double> gam = solve_vector(S);
+  double* gamma = gam.data();
   std::vector<double> gHat(n3, 1.0), gNew(n3), g(n3), y(n3), yNew(n3), T(n3), bt;
-  if (!S.P.warm_start)
-    for (int c = 0; c < nc; ++c) { gamma[3 * c] = 1.0; gamma[3 * c + 1] = 0.0; gamma[3 * c + 2] = 0.0; }
   for (int64_t i = 0; i < n3; ++i) y[i] = gamma[i];
 
   double theta = 1.0, thetaNew = theta, Beta = 0.0, obj1 = 0.0, obj2 = 0.0;
@@ -797,7 +891,7 @@ void apgd_solve(Scene& S) {
   /* APGD.cu:353-354 */
   schur(S, gHat.data(), T.data(), bt);
   double objective = 0.5 * dotv(S, gHat.data(), T.data(), nc) + dotv(S, gHat.data(), S.r.data(), nc);
-  for (int64_t i = 0; i < n3; ++i) gamma[i] = gHat[i];
+  store_solution(S, gHat);
   S.st.iterations = k;
   S.st.backtracks = backtracks;
   S.st.residual = residual;
@@ -973,9 +1067,22 @@ void build_r(Scene& S) {
   int nb = S.nb, nc = S.nc;
   std::vector<double> tmp(3 * (size_t)nb);
   for (int i = 0; i < 3 * nb; ++i) tmp[i] = S.minv[i] * S.k[i];
-  S.r.assign(3 * (size_t)nc, 0.0);
+  S.r.assign(3 * (size_t)nc + S.nbil, 0.0);
   apply_D(S, tmp.data(), S.r.data());
   for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) S.r[i] = S.bst[i] + S.r[i];
+  /* buildStabilizationBilateral (System.cu:1526-1544): b = violation / h at
+   * the step's start time, the prescribed velocity 0 before its start time */
+  double* rb = S.r.data() + 3 * (int64_t)nc;
+  for (int i = 0; i < S.nbil; ++i) {
+    const double ts = S.bilT0[i];
+    double velocity = S.bilVel[i];
+    if (S.time < ts) velocity = 0;
+    double violation;
+    if (S.bilB[i] < 0) violation = S.p[S.bilA[i]] - S.bilP0[i] - velocity * (S.time - ts);
+    else violation = S.p[S.bilA[i]] - S.p[S.bilB[i]] - velocity * (S.time - ts);
+    S.bB[i] = violation / S.P.h;
+    rb[i] = S.bB[i] + rb[i];
+  }
 }
 
 int do_step(Scene& S) {
@@ -988,7 +1095,12 @@ int do_step(Scene& S) {
   build_k(S);
   int n = 3 * S.nb;
   double h = S.P.h;
-  if (S.nc) {
+  if (S.nbil && S.P.solver != 1) {
+    S.st.status = 4;  /* PGJ / PGS take no bilateral rows (PGJ.cu, PGS.cu size 3 nc) */
+    return S.st.status;
+  }
+  /* System.cu:560: the solve runs with contacts or bilateral rows */
+  if (S.nc || S.nbil) {
     build_frames(S);
     build_r(S);
     if (S.P.solver == 5) pgj_solve(S);
@@ -997,7 +1109,7 @@ int do_step(Scene& S) {
     else apgd_solve_fused(S);
     keep_pairs(S);
     std::vector<double> fc(n);
-    apply_DT(S, S.gamma.data(), fc.data());
+    apply_DT(S, solve_vector(S).data(), fc.data());
     for (int i = 0; i < n; ++i) {
       double tmp = S.k[i] + fc[i];
       S.v[i] = S.minv[i] * tmp;
@@ -1149,8 +1261,8 @@ int or_get_frames(void* s, double* F) {
 
 int or_get_r(void* s, double* r) {
   Scene* S = (Scene*)s;
-  if ((int64_t)S->r.size() != 3 * (int64_t)S->nc) return -1;
-  memcpy(r, S->r.data(), sizeof(double) * S->r.size());
+  if ((int64_t)S->r.size() < 3 * (int64_t)S->nc) return -1;
+  memcpy(r, S->r.data(), sizeof(double) * 3 * (size_t)S->nc);
   return S->nc;
 }
 
@@ -1160,13 +1272,27 @@ int or_ccp_violation(void* s, double* out4) {
   out4[0] = out4[1] = out4[2] = out4[3] = 0.0;
   int nc = S->nc;
   if (!nc) return 0;
-  const double* gm = S->gamma.data();
+  /* With bilateral rows the reference reads entry 3 c (and 3 c + 1, 3 c + 2)
+   * of vectors whose first nbil entries are the bilateral rows, with no
+   * offset (getNormalComponent, calculateConeViolation: System.cu:1590-1603);
+   * gm and tg below are those flat vectors.  tg = D v + b over every row (the
+   * reference's temporary holds 3 nc entries, :1613; the entries read are the
+   * same). */
+  const int nbil = S->nbil;
+  const int64_t n3 = 3 * (int64_t)nc;
+  std::vector<double> gm(n3 + nbil), tg(n3 + nbil), dv(n3 + nbil);
+  apply_D(*S, S->v.data(), dv.data());
+  for (int i = 0; i < nbil; ++i) {
+    gm[i] = S->gammaB[i];
+    tg[i] = S->bB[i] + dv[n3 + i];
+  }
+  for (int64_t i = 0; i < n3; ++i) {
+    gm[nbil + i] = S->gamma[i];
+    tg[nbil + i] = S->bst[i] + dv[i];
+  }
   double x = gm[0];
   for (int c = 1; c < nc; ++c) x = std::min(x, gm[3 * c]);
   if (x > 0) x = 0;
-  std::vector<double> tg(3 * (size_t)nc);
-  apply_D(*S, S->v.data(), tg.data());
-  for (int64_t i = 0; i < 3 * (int64_t)nc; ++i) tg[i] = S->bst[i] + tg[i];
   double y = tg[0];
   for (int c = 1; c < nc; ++c) y = std::min(y, tg[3 * c]);
   if (y > 0) y = 0;
@@ -1221,6 +1347,45 @@ double or_potential_energy(void* s) {
   for (int b = 0; b < S->nb; ++b)
     it[b] = (S->f[3 * b] * S->p[3 * b] + S->f[3 * b + 1] * S->p[3 * b + 1]) + S->f[3 * b + 2] * S->p[3 * b + 2];
   return -ordered_sum(it.data(), S->nb);
+}
+
+/* System::addBilateralConstraintDOF (System.cu:510-532) and processConstraints
+ * (:303-315): p0 = the DOF's position now, for a single-DOF row. */
+int or_add_bilateral(void* s, int dofA, int dofB, double velocity, double start_time) {
+  Scene* S = (Scene*)s;
+  const int n = 3 * S->nb;
+  if (dofA < 0 || dofA >= n || dofB >= n) return -1;
+  if (dofB < 0) dofB = -1;
+  const int row = S->nbil++;
+  S->bilA.push_back(dofA);
+  S->bilB.push_back(dofB);
+  S->bilVel.push_back(velocity);
+  S->bilT0.push_back(start_time);
+  S->bilP0.push_back(dofB < 0 ? S->p[dofA] : 0.0);
+  S->gammaB.push_back(0.0);
+  S->bB.push_back(0.0);
+  /* per-body entries, ascending rows, A before B */
+  std::vector<std::vector<int>> per(S->nb);
+  for (int i = 0; i <= row; ++i) {
+    per[S->bilA[i] / 3].push_back((i << 3) | ((S->bilA[i] % 3) << 1));
+    if (S->bilB[i] >= 0) per[S->bilB[i] / 3].push_back((i << 3) | ((S->bilB[i] % 3) << 1) | 1);
+  }
+  S->bincStart.assign(S->nb + 1, 0);
+  S->binc.clear();
+  for (int b = 0; b < S->nb; ++b) {
+    S->bincStart[b] = (int)S->binc.size();
+    S->binc.insert(S->binc.end(), per[b].begin(), per[b].end());
+  }
+  S->bincStart[S->nb] = (int)S->binc.size();
+  return 0;
+}
+
+/* The bilateral rows' impulses of the last solve (System::gamma's first
+ * nbil entries); returns nbil. */
+int or_get_bilateral_gamma(void* s, double* out) {
+  Scene* S = (Scene*)s;
+  if (out && S->nbil) memcpy(out, S->gammaB.data(), sizeof(double) * S->nbil);
+  return S->nbil;
 }
 
 void or_project(double* x3, double mu) { project3(x3, mu); }

@@ -48,7 +48,7 @@ typedef struct or_stats {
   int backtracks;         /* total Lipschitz doublings in the last solve */
   double residual;        /* best residual of the last solve */
   double objective;       /* System::objectiveCCP */
-  int status;             /* 0 ok, 2 = NaN, 3 = backtracking cap hit */
+  int status;             /* 0 ok, 2 = NaN, 3 = backtracking cap hit, 4 = bilateral rows with PGJ/PGS */
   int gamma_size;         /* warm-start buffer length in contacts */
 } or_stats;
 
@@ -70,6 +70,9 @@ int or_get_contacts(void* s, uint32_t* a, uint32_t* b, double* nP, double* loc);
 int or_get_frames(void* s, double* F);     /* 9 per contact: n, u, v */
 int or_get_r(void* s, double* r);          /* 3 per contact (Schur vector of the last step) */
 int or_ccp_violation(void* s, double* out4);
+/* System::addBilateralConstraintDOF (before the first step); 0 or -1 */
+int or_add_bilateral(void* s, int dofA, int dofB, double velocity, double start_time);
+int or_get_bilateral_gamma(void* s, double* out);  /* returns the row count */
 double or_kinetic_energy(void* s);
 double or_potential_energy(void* s);
 

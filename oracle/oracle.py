@@ -75,6 +75,8 @@ def lib():
         L.or_get_frames.argtypes = [C.c_void_p, dp]
         L.or_get_r.argtypes = [C.c_void_p, dp]
         L.or_ccp_violation.argtypes = [C.c_void_p, dp]
+        L.or_add_bilateral.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.or_get_bilateral_gamma.argtypes = [C.c_void_p, dp]
         L.or_kinetic_energy.restype = C.c_double
         L.or_kinetic_energy.argtypes = [C.c_void_p]
         L.or_potential_energy.restype = C.c_double
@@ -140,6 +142,8 @@ class OracleScene:
                              _ip(a[5]), C.byref(self.params))
         if getattr(scene, "gamma", None) is not None:
             self.set_gamma(scene.gamma)
+        for row in getattr(scene, "bilateral", None) or ():
+            self.add_bilateral(*row)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -207,6 +211,19 @@ class OracleScene:
         if nc:
             lib().or_get_r(self.h, _dp(r))
         return r
+
+    def add_bilateral(self, dof_a, dof_b=-1, velocity=0.0, start_time=0.0):
+        """System::addBilateralConstraintDOF (before the first step)."""
+        if lib().or_add_bilateral(self.h, int(dof_a), int(dof_b), float(velocity),
+                                  float(start_time)) != 0:
+            raise ValueError("bilateral DOF out of range")
+
+    def bilateral_gamma(self):
+        n = lib().or_get_bilateral_gamma(self.h, None)
+        g = np.zeros(n)
+        if n:
+            lib().or_get_bilateral_gamma(self.h, _dp(g))
+        return g
 
     def ccp_violation(self):
         o = np.zeros(4)

@@ -45,3 +45,17 @@ def test_settle_driver_other_solver_forms(tmp_path, args):
     assert last[1] > 100
     assert all(np.isfinite(float(x)) for x in lines[-1].split(","))
 
+
+
+def test_settle_driver_with_pinned_spheres(tmp_path):
+    """System::addBilateralConstraintDOF through the C++ layer: the x and y
+    DOFs of a column of 10 spheres stay where they started while the pile
+    settles around them."""
+    out = subprocess.run([DRIVER, "120", "1", "1e-4", "1000", "1", "10"], cwd=tmp_path,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [l for l in out.stdout.splitlines() if l and l[0].isdigit()]
+    assert len(lines) == 120
+    drift = [l for l in out.stdout.splitlines() if l.startswith("pinned drift:")]
+    assert len(drift) == 1
+    assert float(drift[0].split(":")[1]) < 1e-5
