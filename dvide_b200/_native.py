@@ -25,7 +25,7 @@ STATUS = {0: "DV_OK", 1: "DV_ERR_ARG", 2: "DV_ERR_CUDA", 3: "DV_ERR_NAN", 4: "DV
 # Every entry point declared in include/dvide.h (checked by the CPU tests).
 EXPORTS = [
     "dv_params_default", "dv_scene_create", "dv_scene_destroy", "dv_scene_set_stream",
-    "dv_set_params", "dv_step", "dv_collide", "dv_get_state", "dv_set_state",
+    "dv_set_params", "dv_step", "dv_collide", "dv_apgd_solve", "dv_get_state", "dv_set_state",
     "dv_get_contact_force", "dv_get_num_contacts", "dv_get_contacts", "dv_get_gamma",
     "dv_set_gamma", "dv_add_bilateral_dof", "dv_get_bilateral_gamma", "dv_get_frames",
     "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
@@ -159,6 +159,7 @@ def lib():
         "dv_scene_set_stream": [vp, vp],
         "dv_set_params": [vp, C.POINTER(Params)],
         "dv_step": [vp, C.c_int32],
+        "dv_apgd_solve": [vp],
         "dv_collide": [vp],
         "dv_get_state": [vp, dp, dp],
         "dv_set_state": [vp, dp, dp],
@@ -333,6 +334,13 @@ class NativeScene:
 
     def collide(self):
         check(lib().dv_collide(self.h), "dv_collide")
+
+    def solve(self, raise_on_error=True):
+        """The scene solver's solve() alone (dv_apgd_solve): no update."""
+        st = lib().dv_apgd_solve(self.h)
+        if raise_on_error:
+            check(st, "dv_apgd_solve")
+        return st
 
     def state(self):
         p = np.zeros((self.nb, 3))

@@ -287,16 +287,27 @@ int System::outputContactForcePerCollision(std::string filename) {
 
 int APGD::setup() { return 0; }
 
-// The APGD iterations run inside System::DoTimeStep's device step; a
-// separate solve() is not exposed by the B200 step and reports unsupported.
-int APGD::solve() { return DV_ERR_UNSUPPORTED; }
+// Solver::solve() (APGD.cu:164-361, PGJ.cu:152-224, PGS.cu:367-459): the
+// step's solve on the current state and the last collision detection's
+// contacts, without the update (dv_apgd_solve); System::objectiveCCP and
+// iterations as the reference sets them.
+int System::solveNow() {
+  if (!scene) return DV_ERR_ARG;
+  int rc = sync_params();
+  if (rc != DV_OK) return rc;
+  rc = dv_apgd_solve(scene);
+  dv_step_stats st;
+  dv_get_step_stats(scene, &st);
+  objectiveCCP = st.objective;
+  solver->iterations = st.iterations;
+  return rc;
+}
 
-// PGJ runs inside the GPU time step (dv_step); like APGD it has no separate
-// solve entry point in this build.
+int APGD::solve() { return system ? system->solveNow() : DV_ERR_ARG; }
 int PGJ::setup() { return 0; }
-int PGJ::solve() { return DV_ERR_UNSUPPORTED; }
+int PGJ::solve() { return system ? system->solveNow() : DV_ERR_ARG; }
 int PGS::setup() { return 0; }
-int PGS::solve() { return DV_ERR_UNSUPPORTED; }
+int PGS::solve() { return system ? system->solveNow() : DV_ERR_ARG; }
 
 int CollisionDetector::setEnvelope(double e) {
   envelope = e;

@@ -1120,14 +1120,14 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     }
   }
   if (!grid_sync(a, kPhaseFinal, [&]() {
-        if (threadIdx.x == 0) atomicAdd(&a.ew->steps_done, 1);
+        if (threadIdx.x == 0 && !a.solve_only) atomicAdd(&a.ew->steps_done, 1);
       }))
     return;
 
   // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v.
   // Segments with neither contacts nor bilateral rows: v = Minv k, f_contact = 0
   // (System.cu:577-581); the rows' impulses enter f_c like the contacts'.
-  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
+  for (int bt = blockIdx.x; bt < nbt && !a.solve_only; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
     if (b < a.nb) {
       const int s = __ldg(a.bseg + b);
@@ -1160,7 +1160,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     SegState& X = a.sst[s];
     if (a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0)) X.gsize = X.nc;
     // System::time += h (System.cu:584), read by the next step's rows
-    if (a.nbil && a.seg[s].active) a.seg_time[s] = a.seg_time[s] + a.seg[s].h;
+    if (a.nbil && a.seg[s].active && !a.solve_only) a.seg_time[s] = a.seg_time[s] + a.seg[s].h;
   }
   // matched warm start: where each body's A-contacts went in the warm region
   for (int b = blockIdx.x * kThreads + threadIdx.x; b < a.nb; b += gridDim.x * kThreads) {
@@ -1184,9 +1184,10 @@ void prepare_kernel() {
 
 
 template <class T, int MB>
-void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
+void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only) {
   prepare_kernel<T, MB>();
   KArgs<T> a = make_kargs<T>(sd, cfg);
+  a.solve_only = solve_only ? 1 : 0;
   void* params[] = {&a};
   cudaLaunchCooperativeKernel((const void*)k_step_solve<T, MB>, cfg.grid, kThreads, params,
                               dyn_smem_bytes<T>(), st);
@@ -1214,18 +1215,19 @@ int apgd_max_ctas(int precision, int blocks_per_sm) {
   return max_ctas_of<double, 2>();
 }
 
-void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches) {
+void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches,
+                       bool solve_only) {
   cudaMemsetAsync(sd.ew->bar, 0, sizeof(sd.ew->bar), st);
   cudaMemsetAsync(&sd.ew->last_release, 0, sizeof(unsigned long long), st);
   if (sd.solver == DV_SOLVER_PGJ) {
-    launch_pgj_solve(sd, cfg, st);
+    launch_pgj_solve(sd, cfg, st, solve_only);
   } else if (sd.solver == DV_SOLVER_PGS) {
-    launch_pgs_solve(sd, cfg, st);
+    launch_pgs_solve(sd, cfg, st, solve_only);
   } else if (sd.precision == DV_PREC_MIXED) {
-    if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st);
-    else launch_typed<float, 2>(sd, cfg, st);
+    if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st, solve_only);
+    else launch_typed<float, 2>(sd, cfg, st, solve_only);
   } else {
-    launch_typed<double, 2>(sd, cfg, st);
+    launch_typed<double, 2>(sd, cfg, st, solve_only);
   }
   ++*launches;
 }

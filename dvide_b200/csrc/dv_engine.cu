@@ -983,6 +983,24 @@ int Engine::get_bilateral_gamma(int s, std::vector<double>& g) {
   return download(g.data(), d.bil_gam + hseg_[s].bil0, sizeof(double) * n);
 }
 
+int Engine::solve_only() {
+  DV_CUDA_TRY(cudaStreamSynchronize(st_));
+  DV_CUDA_TRY(cudaMemsetAsync(&d.ew->err, 0, sizeof(unsigned), st_));
+  if (d.nbil)
+    DV_CUDA_TRY(cudaMemcpyAsync(d.seg_time, time_.data(), sizeof(double) * d.nseg,
+                                cudaMemcpyHostToDevice, st_));
+  launch_step_solve(d, cfg_, st_, &launches_, true);
+  DV_CUDA_TRY(cudaGetLastError());
+  TRY(sync_words());
+  const EngineWords& w = *h_ew_;
+  if (w.err & (kErrBarrierTimeout | kErrCopyTimeout)) {
+    dv_set_error_text("a bounded wait of the solve kernel expired");
+    return DV_ERR_TIMEOUT;
+  }
+  if (w.err & kErrCapacity) return DV_ERR_OOM;
+  return DV_OK;
+}
+
 int Engine::get_gamma(int s, std::vector<double>& g, int* n) {
   TRY(sync_words());
   int m = h_sst_[s].gsize;

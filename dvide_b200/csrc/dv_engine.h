@@ -59,6 +59,12 @@ class Engine {
   int step(int n);
   // Collision detection only (System::DoTimeStep's first half), synchronous.
   int collide_only();
+  // The solve of a step on the current state and the contacts of the last
+  // collision detection, without the update (the solver's own solve()):
+  // k, r, the solve, gamma into the warm start; v, p, f_contact and the
+  // clock are left as they are (PGS leaves its working velocities in v, as
+  // the reference's PGS::solve does).  Synchronous.
+  int solve_only();
 
   // Per-step records of the last step() call (one per step, in order).
   const std::vector<StepRecord>& records() const { return recs_; }

@@ -252,11 +252,14 @@ struct SolveConfig {
   int blocks_per_sm;  // register budget: 2 (128 per thread) or 3 (80, FP32 iterates only)
 };
 int apgd_max_ctas(int precision, int blocks_per_sm);
-void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches);
+// solve_only: System::DoTimeStep's solve without the update (the solver's
+// own solve(): v, p, f_contact and the clock are left as they are)
+void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, int64_t* launches,
+                       bool solve_only = false);
 // ---- PGJ (dv_pgj.cu) ----
 int pgj_max_ctas(int precision);
-void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st);
+void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only);
 int pgs_max_ctas();
-void launch_pgs_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st);
+void launch_pgs_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only);
 
 }  // namespace dv

@@ -304,12 +304,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgj_solve(KArgs<T> a) {
     }
   }
   if (!grid_sync(a, kPhaseFinal, [&]() {
-        if (threadIdx.x == 0) atomicAdd(&a.ew->steps_done, 1);
+        if (threadIdx.x == 0 && !a.solve_only) atomicAdd(&a.ew->steps_done, 1);
       }))
     return;
 
   // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v
-  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
+  for (int bt = blockIdx.x; bt < nbt && !a.solve_only; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
     if (b < a.nb) {
       const int s = __ldg(a.bseg + b);
@@ -359,14 +359,16 @@ int pgj_max_ctas(int precision) {
   return precision == DV_PREC_MIXED ? pgj_ctas<float>() : pgj_ctas<double>();
 }
 
-void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
+void launch_pgj_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only) {
   const int grid = std::min(cfg.grid, pgj_max_ctas(sd.precision));
   if (sd.precision == DV_PREC_MIXED) {
     KArgs<float> a = make_kargs<float>(sd, cfg);
+    a.solve_only = solve_only ? 1 : 0;
     void* params[] = {&a};
     cudaLaunchCooperativeKernel((const void*)k_pgj_solve<float>, grid, kThreads, params, 0, st);
   } else {
     KArgs<double> a = make_kargs<double>(sd, cfg);
+    a.solve_only = solve_only ? 1 : 0;
     void* params[] = {&a};
     cudaLaunchCooperativeKernel((const void*)k_pgj_solve<double>, grid, kThreads, params, 0, st);
   }

@@ -363,12 +363,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_pgs_solve(KArgs<double> a) {
     }
   }
   if (!grid_sync(a, kPhaseFinal, [&]() {
-        if (threadIdx.x == 0) atomicAdd(&a.ew->steps_done, 1);
+        if (threadIdx.x == 0 && !a.solve_only) atomicAdd(&a.ew->steps_done, 1);
       }))
     return;
 
   // ---- f_c = D^T gamma; v = Minv (k + f_c); f_contact = f_c / h; p += h v
-  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
+  for (int bt = blockIdx.x; bt < nbt && !a.solve_only; bt += gridDim.x) {
     int b = bt * kThreads + threadIdx.x;
     if (b < a.nb) {
       const int s = __ldg(a.bseg + b);
@@ -412,9 +412,10 @@ int pgs_max_ctas() {
   return sms * per_sm;
 }
 
-void launch_pgs_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st) {
+void launch_pgs_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only) {
   const int grid = std::min(cfg.grid, pgs_max_ctas());
   KArgs<double> a = make_kargs<double>(sd, cfg);
+  a.solve_only = solve_only ? 1 : 0;
   void* params[] = {&a};
   cudaLaunchCooperativeKernel((const void*)k_pgs_solve, grid, kThreads, params, 0, st);
 }

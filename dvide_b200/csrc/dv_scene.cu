@@ -158,6 +158,22 @@ DV_API int dv_collide(dv_scene* s) {
   return DV_OK;
 }
 
+DV_API int dv_apgd_solve(dv_scene* s) {
+  if (!s) return DV_ERR_ARG;
+  TRY(s->E.solve_only());
+  const SegState& X = s->E.seg_state(0);
+  dv_step_stats& L = s->last;
+  L.num_contacts = X.nc;
+  L.num_possible = X.npossible;
+  L.iterations = X.ctl.iterations;
+  L.backtracks = X.ctl.backtracks;
+  L.residual = X.ctl.residual;
+  L.objective = X.ctl.objective;
+  L.sweeps = X.ctl.sweeps;
+  L.status = status_from_bits(X.err);
+  return L.status;
+}
+
 DV_API int dv_get_state(dv_scene* s, double* p, double* v) {
   if (!s) return DV_ERR_ARG;
   return s->E.copy_state_out(0, s->E.d.nb, p, v);

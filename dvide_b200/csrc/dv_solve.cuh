@@ -38,6 +38,7 @@ template <> struct Vec4<float> { using type = float4; };
 template <class T>
 struct KArgs {
   int nb, nseg;
+  int solve_only;     // 1: the solve without the update (v, p, f_contact, clock untouched)
   int tcap;           // plane stride of the partials
   int chunk, contiguous;
   size_t S;           // plane stride of contact arrays
@@ -929,6 +930,7 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   KArgs<T> a;
   a.nb = sd.nb;
   a.nseg = sd.nseg;
+  a.solve_only = 0;
   a.tcap = sd.tcap;
   a.chunk = cfg.chunk > 0 ? cfg.chunk : 1;
   a.contiguous = cfg.contiguous;

@@ -115,6 +115,15 @@ DV_API int dv_step(dv_scene* s, int32_t nsteps);
  * (CollisionDetector.cu:547-665): detection only, no solve or update. */
 DV_API int dv_collide(dv_scene* s);
 
+/* The scene solver's solve() (APGD::solve, APGD.cu:164-361; PGJ, PGS
+ * likewise): k = M v + h f, the Schur vector and the solve on the current
+ * state and the contacts of the last collision detection (dv_collide, or the
+ * last step's), gamma into the warm start, and the statistics of
+ * dv_get_step_stats; v, p, the contact forces and the clock are left as they
+ * are (PGS leaves its working velocities in v, as the reference's PGS::solve
+ * does with System::v).  dv_collide + dv_apgd_solve + the update is dv_step. */
+DV_API int dv_apgd_solve(dv_scene* s);
+
 /* Body state, 3 doubles per body as System::p_d / v_d (System.cu:355-366). */
 DV_API int dv_get_state(dv_scene* s, double* p, double* v);
 DV_API int dv_set_state(dv_scene* s, const double* p, const double* v);

@@ -43,6 +43,7 @@ class System {
   double tol;
   int solverType;
   int sync_params();
+  int solveNow();  // Solver::solve() of this System's solver (dv_apgd_solve)
   struct BilateralDOF {
     int dofA, dofB;
     double velocity, startTime;

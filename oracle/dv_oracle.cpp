@@ -1056,6 +1056,9 @@ void pgs_solve(Scene& S) {
   if ((int64_t)S.gamma.size() < n3) S.gamma.resize(n3, 0.0);
   for (int64_t i = 0; i < n3; ++i) S.gamma[i] = g[i];
   S.gsize = nc;
+  /* the sweep works on System::v (PGS.cu:376-379, 143-224): it keeps the last
+   * sweep's velocities (the step's update then overwrites them) */
+  S.v = v;
   S.st.iterations = k;
   S.st.backtracks = 0;
   S.st.residual = residual;
@@ -1083,6 +1086,33 @@ void build_r(Scene& S) {
     S.bB[i] = violation / S.P.h;
     rb[i] = S.bB[i] + rb[i];
   }
+}
+
+/* Solver::solve() alone (APGD.cu:164-361 and the System calls before it,
+ * System.cu:559-566): k, the frames, r and the solve on the current state and
+ * the contacts of the last collision detection; no update, no clock. */
+int solve_only(Scene& S) {
+  S.st.status = 0;
+  S.st.iterations = 0;
+  S.st.backtracks = 0;
+  S.st.residual = 0;
+  S.st.objective = 0;
+  if (S.nbil && S.P.solver != 1) {
+    S.st.status = 4;
+    return S.st.status;
+  }
+  build_k(S);
+  if (S.nc || S.nbil) {
+    build_frames(S);
+    build_r(S);
+    if (S.P.solver == 5) pgj_solve(S);
+    else if (S.P.solver == 6) pgs_solve(S);
+    else if (S.P.apgd_mode == 1) apgd_solve(S);
+    else apgd_solve_fused(S);
+    keep_pairs(S);
+  }
+  S.st.gamma_size = S.gsize;
+  return S.st.status;
 }
 
 int do_step(Scene& S) {
@@ -1188,6 +1218,8 @@ int or_step(void* s, int nsteps) {
   }
   return st;
 }
+
+int or_solve(void* s) { return solve_only(*(Scene*)s); }
 
 int or_collide(void* s) {
   Scene* S = (Scene*)s;

@@ -60,6 +60,7 @@ int or_set_params(void* s, const or_params* prm);
 
 int or_step(void* s, int nsteps);          /* System::DoTimeStep */
 int or_collide(void* s);                   /* AABB + broadphase + narrowphase only */
+int or_solve(void* s);                     /* Solver::solve() alone: no update, no clock */
 int or_get_stats(void* s, or_stats* out);
 int or_get_state(void* s, double* p, double* v);
 int or_set_state(void* s, const double* p, const double* v);

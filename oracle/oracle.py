@@ -65,6 +65,7 @@ def lib():
         for name in ("or_step",):
             getattr(L, name).argtypes = [C.c_void_p, C.c_int]
         L.or_collide.argtypes = [C.c_void_p]
+        L.or_solve.argtypes = [C.c_void_p]
         L.or_get_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
         L.or_get_state.argtypes = [C.c_void_p, dp, dp]
         L.or_set_state.argtypes = [C.c_void_p, dp, dp]
@@ -155,6 +156,10 @@ class OracleScene:
 
     def collide(self):
         return lib().or_collide(self.h)
+
+    def solve(self):
+        """Solver::solve() alone: no update, no clock."""
+        return lib().or_solve(self.h)
 
     def stats(self):
         s = OrStats()
