@@ -68,7 +68,7 @@ class Params(C.Structure):
                 ("envelope", C.c_double), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int32), ("warm_start", C.c_int32), ("solver", C.c_int32),
                 ("precision", C.c_int32), ("max_backtracks", C.c_int32), ("verbose", C.c_int32),
-                ("fp64_narrowphase", C.c_int32)]
+                ("fp64_narrowphase", C.c_int32), ("anti_relaxation", C.c_int32)]
 
 
 class StepStats(C.Structure):
@@ -256,6 +256,7 @@ def make_params(p: dict, precision=DV_PREC_FP64) -> Params:
     o.precision = int(p.get("precision", precision))
     o.verbose = int(p.get("verbose", 0))
     o.fp64_narrowphase = int(p.get("fp64_narrowphase", 0))
+    o.anti_relaxation = int(p.get("anti_relaxation", 0))
     return o
 
 

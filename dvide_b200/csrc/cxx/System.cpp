@@ -107,6 +107,7 @@ int System::sync_params() {
   P.warm_start = apgd ? apgd->warmStartMode : 0;
   P.solver = solverType == 5 ? DV_SOLVER_PGJ : solverType == 6 ? DV_SOLVER_PGS : DV_SOLVER_APGD;
   P.verbose = solver->verbose ? 1 : 0;
+  P.anti_relaxation = apgd && apgd->useAntiRelaxation ? 1 : 0;
   if (!scene) return DV_ERR_ARG;
   return dv_set_params(scene, &P);
 }
@@ -124,7 +125,6 @@ int System::initializeSystem() {
   if (solverType < 1 || solverType > 7) solverType = 1;
   if (solverType != 1 && solverType != 5 && solverType != 6) return DV_ERR_UNSUPPORTED;
   APGD* apgd = dynamic_cast<APGD*>(solver);
-  if (apgd && apgd->useAntiRelaxation) return DV_ERR_UNSUPPORTED;
   std::vector<dv_body_desc> desc(bodies.size());
   for (size_t j = 0; j < bodies.size(); ++j) {
     Body* b = bodies[j];
@@ -151,6 +151,7 @@ int System::initializeSystem() {
   P.max_iterations = solver->maxIterations;
   P.warm_start = apgd ? apgd->warmStartMode : 0;
   P.solver = solverType == 5 ? DV_SOLVER_PGJ : solverType == 6 ? DV_SOLVER_PGS : DV_SOLVER_APGD;
+  P.anti_relaxation = apgd && apgd->useAntiRelaxation ? 1 : 0;
   if (scene) dv_scene_destroy(scene);
   scene = nullptr;
   int rc = dv_scene_create(desc.data(), (int32_t)desc.size(), &P, &scene);

@@ -51,11 +51,11 @@ namespace {
 // (written by thread 0 when the CTA moves to another segment) so that they
 // take no registers in the contact loops.
 struct ProdScalars {
-  int cur, nw, nw2, restart, exact;
+  int cur, nw, nw2, restart, exact, rsel;
   double ya, ym, nt2, gd, gA, gB, mu;
 };
 struct StepScalars {
-  int part, first, cur, prev, nw, yr, exact;
+  int part, first, cur, prev, nw, yr, exact, rsel;
   double ya, ym, nt, mu;
 };
 
@@ -64,6 +64,7 @@ struct CtlArgs {
   double* part;
   int tcap;
   int mixed;  // FP32 iterates: the Lipschitz test allows float-noise differences
+  int ar;     // anti-relaxation: an accepted, unconverged iterate moves r to the next plane
   SegState* sst;
   const SegParams* seg;
   EngineWords* ew;
@@ -116,6 +117,8 @@ __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
     C->obj1 = 0.0;
     C->obj2 = 0.0;
     C->obj2_base = 0.0;
+    C->rsel = 0;
+    C->objN = 0.0;
     if (P.max_iter <= 0) {
       mark_done(a, s);
     } else {
@@ -182,11 +185,15 @@ __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
         residual = res;
         C->residual = res;
         C->objective = obj1;
+        C->objN = 0.5 * sm[0];
         C->best = c.nw;
       }
       if (residual < P.tol) {
         finished = true;
       } else {
+        // APGD.cu:335-345 after this iteration: r moves to the plane the
+        // product pass wrote for the look-ahead
+        if (a.ar) C->rsel = c.rsel ^ 1;
         const double th = c.restart ? 1.0 : c.theta_new;
         C->yb = c.beta;
         C->yr = c.restart;
@@ -292,7 +299,8 @@ __device__ inline bool bil_product_tile(BilRows<T> R, const ProdScalars& ps, int
   return bad;
 }
 
-template <class T, int kMinB>
+// kAR: APGD's anti-relaxation (APGD.cu:335-345), FP64 one-scene engines.
+template <class T, int kMinB, bool kAR>
 __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   using V = typename Vec4<T>::type;
   __shared__ double scratch[kNQ * 8 + 8];
@@ -327,8 +335,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     s_def.fail = 0;
   }
   __syncthreads();
-  const CtlArgs ca{a.part, a.tcap, sizeof(T) != sizeof(double) ? 1 : 0, a.sst, a.seg, a.ew,
-                   a.donemask};
+  const CtlArgs ca{a.part, a.tcap, sizeof(T) != sizeof(double) ? 1 : 0, kAR ? 1 : 0, a.sst,
+                   a.seg, a.ew, a.donemask};
 
   // ---- work lists off; per-segment solve state; done mask (bit set: not iterating)
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -454,6 +462,11 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           ft_times<double, double4>(fd, wa, wb, &d0, &d1, &d2);
           double bn = __ldg(a.gap + c) / h;
           a.r[0 * S + c] = (T)(bn + d0);
+          if (kAR) {
+            // r_n and the anti-relaxation vector (0 at the start, APGD.cu:196)
+            a.ar_r0[c] = bn + d0;
+            a.ar_v[c] = 0.0;
+          }
           a.r[1 * S + c] = (T)(0.0 + d1);
           a.r[2 * S + c] = (T)(0.0 + d2);
           double g0, g1, g2;
@@ -516,7 +529,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   }
   if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
   load_mask(a, s_mask, mwords);
-  body_pass_schur(a, s_mask);
+  body_pass_schur<T, kAR>(a, s_mask);
   if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
   // ---- L = ||N e|| / ||e||; q = F gamma_0 for the first N y
@@ -586,7 +599,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   };
   if (!grid_sync(a, kPhaseSetup, latch)) return;
   load_mask(a, s_mask, mwords);
-  body_pass_schur(a, s_mask);
+  body_pass_schur<T, kAR>(a, s_mask);
   if (!grid_sync(a, kPhaseSetup, NoCtl{})) return;
 
   // ---- APGD iterations (APGD.cu:227-350)
@@ -652,6 +665,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
               s_st.nt = -__ldcg(&C->t);
               s_st.mu = a.seg[s].mu;
               s_st.exact = a.seg[s].exact;
+              s_st.rsel = __ldcg(&C->rsel);
             }
             s_st.part = part;
           }
@@ -761,7 +775,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
               N1 = ya * NGc[1 * S + c] + ym * NGp[1 * S + c];
               N2 = ya * NGc[2 * S + c] + ym * NGp[2 * S + c];
             }
-            T r0 = a.r[0 * S + c], r1 = a.r[1 * S + c], r2 = a.r[2 * S + c];
+            T r0 = kAR ? (T)a.ar_r0[(size_t)s_st.rsel * S + c] : a.r[0 * S + c];
+            T r1 = a.r[1 * S + c], r2 = a.r[2 * S + c];
             T g0 = N0 + r0, g1 = N1 + r1, g2 = N2 + r2;
             T x0 = y0 + nt_ * g0, x1 = y1 + nt_ * g1, x2 = y2 + nt_ * g2;
             project_cone<T>(x0, x1, x2, mu);
@@ -792,7 +807,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           }))
         return;
     }
-    body_pass_schur(a, s_mask, lon, NBL);
+    body_pass_schur<T, kAR>(a, s_mask, lon, NBL);
     if (!grid_sync(a, kPhaseBody, NoCtl{})) return;
 
     // N gamma_new, objective (APGD.cu:237-238), residual (:90-102); then the
@@ -815,7 +830,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       };
       // bulk copies of (tile t of segment s, sub-tile sub) for this warp into stage sidx
       auto issue = [&](int t, int st0, int sc0, int snc, int sub, int sidx, int cur, int nw,
-                       int restart) {
+                       int restart, int rsel) {
         const int kw = (t - st0) * kTileItems + sub * kSub + warp * 32;
         if (lane == 0 && kw < snc) {
           mark_stage_issued(stg, sidx);
@@ -830,6 +845,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             src[9 + k] = a.G[cur] + k * S;
             src[12 + k] = a.NG[cur] + k * S;
           }
+          // anti-relaxation: the current plane of r_n
+          if (kAR) src[6] = reinterpret_cast<const T*>(a.ar_r0 + (size_t)rsel * S);
           const int nd = restart ? 9 : kStagePlanes;
           const unsigned pbytes = 32u * (unsigned)sizeof(T);
           unsigned char* dst = stg.base + (size_t)(2 * warp + sidx) * stg.stage_bytes;
@@ -862,6 +879,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           s_ps.gB = -1.0 / gd;
           s_ps.mu = a.seg[s].mu;
           s_ps.exact = a.seg[s].exact;
+          s_ps.rsel = __ldcg(&C->rsel);
         }
         __syncthreads();
       };
@@ -882,7 +900,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         s = sc.s;
         load_ps(s);
         sc0 = sc.c0; st0 = sc.t0; snc = sc.nc;
-        issue(tcur, st0, sc0, snc, 0, 0, ps.cur, ps.nw, ps.restart);
+        issue(tcur, st0, sc0, snc, 0, 0, ps.cur, ps.nw, ps.restart, ps.rsel);
       }
       while (seq >= 0) {
         const int ti = tcur;
@@ -908,11 +926,11 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         __syncwarp();  // the warp's reads of stage sidx^1 are done
         if (nseq >= 0 && !failed) {
           if (ns == s) {
-            issue(ntile, st0, sc0, snc, nsub, sidx ^ 1, ps.cur, ps.nw, ps.restart);
+            issue(ntile, st0, sc0, snc, nsub, sidx ^ 1, ps.cur, ps.nw, ps.restart, ps.rsel);
           } else {
             const ApgdCtl* C = &a.sst[ns].ctl;
             issue(ntile, sc.t0, sc.c0, sc.nc, nsub, sidx ^ 1, __ldcg(&C->cur), __ldcg(&C->nw),
-                  __ldcg(&C->restart));
+                  __ldcg(&C->restart), __ldcg(&C->rsel));
           }
         }
         const int kw = (ti - st0) * kTileItems + sub * kSub + warp * 32;
@@ -968,7 +986,23 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
             M1 = ya * N1 + ym * sd[13 * 32 + j];
             M2 = ya * N2 + ym * sd[14 * 32 + j];
           }
-          T g0 = M0 + r0, g1 = M1 + r1, g2 = M2 + r2;
+          T rn0 = r0;  // r_n of the next iteration
+          if (kAR) {
+            // APGD.cu:335-345 for gamma_new = x: v = Minv (k + D^T x) of the
+            // body pass, s = (D v)_(u, v), ar = sqrt(s_u^2 + s_v^2) mu;
+            // r_n' = ar + (-ar_old + r_n), into the next plane
+            const double4 va = a.v_ar[su[j]], vb = a.v_ar[su[32 + j]];
+            const double d0 = va.x - vb.x, d1 = va.y - vb.y, d2 = va.z - vb.z;
+            const double s_u = (f.u0 * d0 + f.u1 * d1) + f.u2 * d2;
+            const double s_v = (f.v0 * d0 + f.v1 * d1) + f.v2 * d2;
+            const double arn = sqrt(s_u * s_u + s_v * s_v) * ps.mu;
+            const size_t cur_p = (size_t)ps.rsel * S + c, nxt_p = (size_t)(ps.rsel ^ 1) * S + c;
+            const double rnn = arn + (-a.ar_v[cur_p] + (double)r0);
+            a.ar_r0[nxt_p] = rnn;
+            a.ar_v[nxt_p] = arn;
+            rn0 = (T)rnn;
+          }
+          T g0 = M0 + rn0, g1 = M1 + r1, g2 = M2 + r2;
           T z0 = y0 + nt2 * g0, z1 = y1 + nt2 * g1, z2 = y2 + nt2 * g2;
           project_cone<T>(z0, z1, z2, (T)ps.mu);
           T* G2 = a.G[ps.nw2];
@@ -980,7 +1014,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           acc[3] = acc[3] + dot3i(t0, t1, t2, t0, t1, t2);
           acc[4] = acc[4] + dot3i(g0, g1, g2, s0, s1, s2);
           acc[5] = acc[5] + dot3i(y0, y1, y2, M0, M1, M2);
-          acc[6] = acc[6] + dot3i(y0, y1, y2, r0, r1, r2);
+          acc[6] = acc[6] + dot3i(y0, y1, y2, rn0, r1, r2);
         }
         if (sub == kItemsPerThread - 1) {
           if (__any_sync(0xffffffffu, bad) && lane == 0) seg_error(a, s, kErrNaN);
@@ -1070,6 +1104,48 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           }))
         return;
     }
+  }
+
+  // ---- anti-relaxation: objectiveCCP = 1/2 gamma_hat' N gamma_hat + gamma_hat' r
+  // with the last r (APGD.cu:353-354); the first term was kept when gamma_hat was
+  // found, the second is folded over the tiles here (one scene)
+  if (kAR) {
+    int nslot = 0;
+    for (int i = 0;; ++i) {
+      const int t = cta_tile(a, NT, i);
+      if (t < 0) break;
+      locate(a, sc, t);
+      const ApgdCtl* C = &a.sst[sc.s].ctl;
+      const int best = __ldcg(&C->best), rsel = __ldcg(&C->rsel);
+      const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
+      double acc[1] = {0.0};
+      if (best >= 0) {
+        const T* B = a.G[best];
+        for (int m = 0; m < kItemsPerThread; ++m) {
+          const int k = k0 + m * kThreads + threadIdx.x;
+          if (k < nc) {
+            const int c = c0 + k;
+            acc[0] = acc[0] + dot3i(B[c], B[S + c], B[2 * S + c], a.ar_r0[(size_t)rsel * S + c],
+                                    (double)a.r[S + c], (double)a.r[2 * S + c]);
+          }
+        }
+      }
+      park_tile<1, false>(s_def, nslot, t, acc, 0.0);
+      if (++nslot == kMaxDefer) {
+        fold_parked<1, false>(a, s_def, nslot);
+        nslot = 0;
+      }
+    }
+    fold_parked<1, false>(a, s_def, nslot);
+    if (!grid_sync(a, kPhaseFinal, [&]() {
+          double sm[1];
+          fold_tiles<1>(a, a.sst[0].t0, a.sst[0].nt, sm, scratch);
+          if (threadIdx.x == 0) {
+            ApgdCtl* C = &a.sst[0].ctl;
+            if (__ldcg(&C->best) >= 0) C->objective = __ldcg(&C->objN) + sm[0];
+          }
+        }))
+      return;
   }
 
   // ---- gamma = gamma_hat (APGD.cu:358) into the warm-start region; q = F gamma (FP64)
@@ -1173,23 +1249,23 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   }
 }
 
-template <class T, int MB>
+template <class T, int MB, bool AR>
 void prepare_kernel() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_step_solve<T, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_step_solve<T, MB, AR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)dyn_smem_bytes<T>());
   done = true;
 }
 
 
-template <class T, int MB>
+template <class T, int MB, bool AR = false>
 void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only) {
-  prepare_kernel<T, MB>();
+  prepare_kernel<T, MB, AR>();
   KArgs<T> a = make_kargs<T>(sd, cfg);
   a.solve_only = solve_only ? 1 : 0;
   void* params[] = {&a};
-  cudaLaunchCooperativeKernel((const void*)k_step_solve<T, MB>, cfg.grid, kThreads, params,
+  cudaLaunchCooperativeKernel((const void*)k_step_solve<T, MB, AR>, cfg.grid, kThreads, params,
                               dyn_smem_bytes<T>(), st);
 }
 
@@ -1198,8 +1274,8 @@ int max_ctas_of() {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  prepare_kernel<T, MB>();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<T, MB>, kThreads,
+  prepare_kernel<T, MB, false>();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_solve<T, MB, false>, kThreads,
                                                 dyn_smem_bytes<T>());
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
@@ -1226,6 +1302,8 @@ void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, in
   } else if (sd.precision == DV_PREC_MIXED) {
     if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st, solve_only);
     else launch_typed<float, 2>(sd, cfg, st, solve_only);
+  } else if (sd.anti_relax) {
+    launch_typed<double, 2, true>(sd, cfg, st, solve_only);
   } else {
     launch_typed<double, 2>(sd, cfg, st, solve_only);
   }

@@ -80,6 +80,10 @@ static int check_params(const dv_params& p) {
   if (p.solver == DV_SOLVER_PGS && p.precision != DV_PREC_FP64) return DV_ERR_UNSUPPORTED;
   if (p.warm_start < 0 || p.warm_start > 2) return DV_ERR_ARG;
   if (p.fp64_narrowphase != 0 && p.fp64_narrowphase != 1) return DV_ERR_ARG;
+  if (p.anti_relaxation != 0 && p.anti_relaxation != 1) return DV_ERR_ARG;
+  // anti-relaxation: an APGD option, FP64 only
+  if (p.anti_relaxation && (p.solver != DV_SOLVER_APGD || p.precision != DV_PREC_FP64))
+    return DV_ERR_UNSUPPORTED;
   return DV_OK;
 }
 
@@ -95,6 +99,7 @@ int Engine::alloc_contacts(size_t cap) {
     dfree(q.NG[k]);
   }
   dfree(q.q); dfree(q.inc); dfree(q.part); dfree(q.tseg); dfree(q.act_tiles);
+  dfree(q.ar_r0); dfree(q.ar_v);
   q.ccap = cap;
   q.tcap = (int)(cap / kTileItems) + q.nseg + 1 + (q.nbil + kTileItems - 1) / kTileItems;
   TRY(dalloc(&q.ida, cap));
@@ -110,6 +115,10 @@ int Engine::alloc_contacts(size_t cap) {
   }
   TRY(dalloc(&q.q, cap));
   TRY(dalloc(&q.inc, 2 * cap));
+  if (q.anti_relax) {
+    TRY(dalloc(&q.ar_r0, 2 * cap));
+    TRY(dalloc(&q.ar_v, 2 * cap));
+  }
   TRY(dalloc(&q.part, (size_t)8 * q.tcap));
   TRY(dalloc(&q.tseg, (size_t)q.tcap));
   TRY(dalloc(&q.act_tiles, (size_t)q.tcap));
@@ -208,6 +217,7 @@ int Engine::init(const std::vector<SceneInput>& scenes, int precision) {
   std::vector<SlotSpec> slots(scenes.size());
   for (size_t i = 0; i < scenes.size(); ++i) slots[i].in = scenes[i];
   TRY(reconfigure(slots));
+  if (scenes.size() == 1 && scenes[0].P.anti_relaxation) TRY(enable_anti_relax());
   max_ctas_ = apgd_max_ctas(precision, 2);
   DV_CUDA_TRY(cudaGetLastError());
   cfg_.grid = std::max(1, std::min(max_ctas_, (d.nb + kThreads - 1) / kThreads));
@@ -233,6 +243,9 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
   for (const SlotSpec& sl : slots) {
     if (sl.keep >= d.nseg) return DV_ERR_ARG;
     if (sl.keep < 0) TRY(validate_scene(sl.in));
+    // anti-relaxation: the first layout of a one-scene engine only
+    if (sl.keep < 0 && sl.in.P.anti_relaxation && !(nseg2 == 1 && d.nseg == 0))
+      return DV_ERR_UNSUPPORTED;
   }
   // one solver for every segment of an engine
   int solver = -1;
@@ -294,6 +307,7 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
       G.max_bt = P.max_backtracks;
       G.warm = P.warm_start;
       G.exact = P.fp64_narrowphase;
+      G.ar = P.anti_relaxation;
       G.active = 1;
       G.b0 = nb2;
       G.b1 = nb2 + n;
@@ -602,6 +616,14 @@ int Engine::set_segment_params(int s, const dv_params& P) {
   TRY(check_params(P));
   // bilateral rows: APGD only (the reference's PGJ and PGS size their vectors 3 nc)
   if (hseg_[s].nbil > 0 && P.solver != DV_SOLVER_APGD) return DV_ERR_UNSUPPORTED;
+  // anti-relaxation: one-scene engines without bilateral rows (the reference's
+  // anti-relaxation vector is indexed without the rows' offset, APGD.cu:104-112)
+  if (P.anti_relaxation && (d.nseg != 1 || hseg_[s].nbil > 0)) return DV_ERR_UNSUPPORTED;
+  if (P.anti_relaxation && !d.anti_relax) TRY(enable_anti_relax());
+  if (!P.anti_relaxation && d.anti_relax) {
+    d.anti_relax = 0;
+    drop_graph();
+  }
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   SegParams& G = hseg_[s];
   if (P.envelope > P_[s].envelope) {
@@ -616,6 +638,7 @@ int Engine::set_segment_params(int s, const dv_params& P) {
   G.max_bt = P.max_backtracks;
   G.warm = P.warm_start;
   G.exact = P.fp64_narrowphase;
+  G.ar = P.anti_relaxation;
   if (P.solver != P_[s].solver) {
     if (d.nseg != 1) return DV_ERR_UNSUPPORTED;
     d.solver = P.solver;
@@ -892,6 +915,24 @@ int Engine::collide_only() {
   return DV_ERR_OOM;
 }
 
+// Turns the anti-relaxation kernel on, with its buffers for the current
+// contact capacity (alloc_contacts keeps them sized while it is on).
+int Engine::enable_anti_relax() {
+  DV_CUDA_TRY(cudaStreamSynchronize(st_));
+  d.anti_relax = 1;
+  dfree(d.ar_r0);
+  dfree(d.ar_v);
+  TRY(dalloc(&d.ar_r0, 2 * d.ccap));
+  TRY(dalloc(&d.ar_v, 2 * d.ccap));
+  if (d.v_ar_cap < (size_t)d.nb) {
+    dfree(d.v_ar);
+    TRY(dalloc(&d.v_ar, (size_t)d.nb));
+    d.v_ar_cap = d.nb;
+  }
+  drop_graph();
+  return DV_OK;
+}
+
 int Engine::add_bilateral(int s, int dof_a, int dof_b, double velocity, double start_time) {
   if (s < 0 || s >= d.nseg) return DV_ERR_ARG;
   if (d.nseg != 1) return DV_ERR_UNSUPPORTED;
@@ -906,7 +947,8 @@ int Engine::add_bilateral(int s, int dof_a, int dof_b, double velocity, double s
     dv_set_error_text("bilateral constraints are added before the first step");
     return DV_ERR_ARG;
   }
-  if (P_[s].solver != DV_SOLVER_APGD || d.precision != DV_PREC_FP64) return DV_ERR_UNSUPPORTED;
+  if (P_[s].solver != DV_SOLVER_APGD || d.precision != DV_PREC_FP64 || P_[s].anti_relaxation)
+    return DV_ERR_UNSUPPORTED;
   if (dof_b < 0) dof_b = -1;
   double p0 = 0.0;
   if (dof_b < 0) {
@@ -984,6 +1026,8 @@ int Engine::get_bilateral_gamma(int s, std::vector<double>& g) {
 }
 
 int Engine::solve_only() {
+  // the reference's anti-relaxation leaves its own velocities in System::v
+  if (d.anti_relax) return DV_ERR_UNSUPPORTED;
   DV_CUDA_TRY(cudaStreamSynchronize(st_));
   DV_CUDA_TRY(cudaMemsetAsync(&d.ew->err, 0, sizeof(unsigned), st_));
   if (d.nbil)

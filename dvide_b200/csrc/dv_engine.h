@@ -158,6 +158,7 @@ class Engine {
   int ensure_records(int n);
   int upload_segments();
   int upload_bilateral();
+  int enable_anti_relax();
   int sync_words();
   int ensure_red(size_t n);
   void ordered_sum_dev(const double* items, int n, double* part, int slot);

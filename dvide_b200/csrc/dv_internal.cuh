@@ -67,6 +67,7 @@ struct SegParams {
   int cell_base, cell_cap;  // global cell ids [cell_base, cell_base + cell_cap)
   int wbase, wcap;          // warm-start region [wbase, wbase + wcap) of the gamma arena
   int bil0, nbil;           // bilateral DOF rows [bil0, bil0 + nbil) (System.cu:510-532)
+  int ar;                   // APGD anti-relaxation (APGD.cu:335-345)
 };
 
 // Scalar state of one APGD solve (APGD.cu:208-223, 266-332).  Iterates live in
@@ -94,6 +95,8 @@ struct ApgdCtl {
   unsigned err;
   int iterations;
   int sweeps;           // iterations executed
+  int rsel;             // anti-relaxation: plane of the current r_n and ar (the other: next)
+  double objN;          // anti-relaxation: half of gamma_hat . N gamma_hat
 };
 
 // Per-segment results of the current step (device-written).
@@ -210,6 +213,14 @@ struct SceneDev {
   double* bil_gam = nullptr;  // the rows' impulses of the last solve (System::gamma_d head)
   double* bil_b = nullptr;    // b of the rows at the last step
   double* seg_time = nullptr; // nseg: System::time at the step's start (rows with a velocity)
+  // APGD anti-relaxation (one-scene engines, FP64): the normal component of r
+  // and the anti-relaxation vector, current and next (2 planes of ccap each),
+  // and v = Minv (k + D^T x) of the iterate x under test (nb)
+  int anti_relax = 0;
+  double* ar_r0 = nullptr;
+  double* ar_v = nullptr;
+  double4* v_ar = nullptr;
+  size_t v_ar_cap = 0;
   // warm-start arena (System::gamma_d of every segment): 3 planes of stride
   // wtotal; segment s owns [wbase, wbase + wcap), positional within it
   double* gamma = nullptr;

@@ -89,6 +89,11 @@ struct KArgs {
   double* bil_gam;     // warm start / solution of the rows
   double* bil_b;       // b of the rows (for the CCP violation)
   double* seg_time;    // System::time of each segment at the step's start
+  // APGD anti-relaxation (the kAR kernel): r_n and ar planes (current, next;
+  // stride S), v = Minv (k + D^T x) of the iterate under test
+  double* ar_r0;
+  double* ar_v;
+  double4* v_ar;
 };
 
 template <class T>
@@ -677,6 +682,7 @@ __device__ inline ApgdCtl ctl_read(const ApgdCtl* C) {
   c.nw = __ldcg(&C->nw); c.best = __ldcg(&C->best); c.yr = __ldcg(&C->yr);
   c.first = __ldcg(&C->first); c.backtracks = __ldcg(&C->backtracks); c.err = __ldcg(&C->err);
   c.iterations = __ldcg(&C->iterations); c.sweeps = __ldcg(&C->sweeps);
+  c.rsel = __ldcg(&C->rsel); c.objN = __ldcg(&C->objN);
   return c;
 }
 
@@ -719,7 +725,9 @@ __device__ inline void mark_done(const K& a, int s) {
 // Schur body pass: w_b = minv_b * (D^T x)_b for bodies of iterating
 // segments; fixed bodies keep w = 0.
 // w_b of one body of an iterating segment.
-template <class T>
+// kAR: also v = Minv (k + D^T x) for the anti-relaxation (APGD.cu:338-340;
+// 0 for fixed bodies, whose v enters only as squares).
+template <class T, bool kAR = false>
 __device__ inline void body_w(const KArgs<T>& a, int b) {
   using V = typename Vec4<T>::type;
   V* w = reinterpret_cast<V*>(a.wd);
@@ -732,6 +740,13 @@ __device__ inline void body_w(const KArgs<T>& a, int b) {
     V o;
     o.x = m * s.x; o.y = m * s.y; o.z = m * s.z; o.w = T(0);
     store_keep(w + b, o);
+    if (kAR) {
+      const double4 k = a.k4[b];
+      a.v_ar[b] = make_double4(mi * (k.x + (double)s.x), mi * (k.y + (double)s.y),
+                               mi * (k.z + (double)s.z), 0.0);
+    }
+  } else if (kAR) {
+    a.v_ar[b] = make_double4(0.0, 0.0, 0.0, 0.0);
   } else if (sizeof(T) != sizeof(double)) {
     // the FP32 view of w overlays the FP64 setup values: store the zero
     V o;
@@ -743,7 +758,7 @@ __device__ inline void body_w(const KArgs<T>& a, int b) {
 // Schur body pass: w_b = minv_b * (D^T x)_b for bodies of iterating
 // segments; fixed bodies keep w = 0.  With the work lists in use (lon), over
 // the listed body ranges (one segment each) instead of every body.
-template <class T>
+template <class T, bool kAR = false>
 __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask, int lon = 0,
                                        int nlist = 0) {
   const int mwords = (a.nseg + 31) >> 5;
@@ -752,7 +767,7 @@ __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask
       const int4 r = __ldcg(a.act_bodies + p);
       if (mask_done(a, s_mask, mwords, r.z)) continue;
       const int b = r.x + threadIdx.x;
-      if (b < r.y) body_w(a, b);
+      if (b < r.y) body_w<T, kAR>(a, b);
     }
     return;
   }
@@ -767,7 +782,7 @@ __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask
       if (a.nseg > 1) prefetch_l2(a.bseg + bn);
     }
     if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b))))
-      body_w(a, b);
+      body_w<T, kAR>(a, b);
   }
 }
 
@@ -987,6 +1002,9 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   a.bil_gam = sd.bil_gam;
   a.bil_b = sd.bil_b;
   a.seg_time = sd.seg_time;
+  a.ar_r0 = sd.ar_r0;
+  a.ar_v = sd.ar_v;
+  a.v_ar = sd.v_ar;
   return a;
 }
 

@@ -71,6 +71,9 @@ typedef struct dv_params {
                                narrowphase and the tangent frame with FP64 square roots
                                (the reference's are float, helper_math_double.h:576-597);
                                not the reference's results, so never with parity checks */
+  int32_t anti_relaxation;  /* APGD::setAntiRelaxation (APGD.cuh:63, APGD.cu:335-345), default 0;
+                               FP64 APGD scenes of their own (not in batches or servers),
+                               without bilateral rows and without dv_apgd_solve */
 } dv_params;
 
 /* Per-step report (System.cu:586-599 and APGD.cu:351-357). */

@@ -1,6 +1,7 @@
 // APGD.h -- accelerated projected gradient descent (src/APGD.cuh:18-68):
 // defaults tolerance 1e-4, maxIterations 100000, warm start and
-// anti-relaxation off (src/APGD.cu:6-16).  The iterations run inside the
+// anti-relaxation off (src/APGD.cu:6-16); setAntiRelaxation(true) runs the
+// reference's anti-relaxation block (APGD.cu:335-345).  The iterations run inside the
 // GPU time step; solve() runs the step's solve alone on the current state and
 // the last collision detection's contacts (no update; dv_apgd_solve).
 #pragma once

@@ -704,6 +704,31 @@ void resize_gamma(Scene& S) {
   }
 }
 
+/* APGD.cu:335-345, the anti-relaxation block at the end of an iteration that
+ * did not converge, with gamma the new iterate: r -= ar; v = Minv (k + D^T
+ * gamma); ar_c = (sqrt(s_u^2 + s_v^2) mu, 0, 0) with s = (D v)_c
+ * (updateAntiRelaxationVector, :104-112); r += ar.  Contacts only (the
+ * reference indexes ar without the bilateral rows' offset). */
+void anti_relax(Scene& S, const double* gamma, std::vector<double>& ar) {
+  const int nc = S.nc, nb = S.nb;
+  const int64_t n3 = 3 * (int64_t)nc;
+  for (int64_t i = 0; i < n3; ++i) S.r[i] = (-1.0 * ar[i]) + S.r[i];
+  std::vector<double> fc(3 * (size_t)nb), v(3 * (size_t)nb), dv(n3);
+  apply_DT(S, gamma, fc.data());
+  for (int i = 0; i < 3 * nb; ++i) {
+    const double tmp = S.k[i] + fc[i];
+    v[i] = S.minv[i] * tmp;
+  }
+  apply_D(S, v.data(), dv.data());
+  for (int c = 0; c < nc; ++c) {
+    const double su = dv[3 * c + 1], sv = dv[3 * c + 2];
+    ar[3 * c] = sqrt(su * su + sv * sv) * S.P.mu;
+    ar[3 * c + 1] = 0.0;
+    ar[3 * c + 2] = 0.0;
+  }
+  for (int64_t i = 0; i < n3; ++i) S.r[i] = (1.0 * ar[i]) + S.r[i];
+}
+
 /* The solve's starting vector: the contacts' held impulses, then the
  * bilateral rows'. */
 std::vector<double> solve_vector(const Scene& S) {
@@ -731,7 +756,7 @@ void apgd_solve_fused(Scene& S) {
   int nc = S.nc;
   int64_t n3 = 3 * (int64_t)nc + S.nbil;  // contacts, then bilateral rows
   resize_gamma(S);
-  std::vector<double> Gc = solve_vector(S), Gp(n3, 0.0), NGc(n3), NGp(n3, 0.0);
+  std::vector<double> Gc = solve_vector(S), Gp(n3, 0.0), NGc(n3), NGp(n3, 0.0), ar(n3, 0.0);
   std::vector<double> gNew(n3), NgNew(n3), g(n3), y(n3), Ny(n3), T(n3), best(n3, 1.0), bt;
   double theta = 1.0, thetaNew = theta, Beta = 0.0, obj1 = 0.0, obj2 = 0.0;
   double residual = 10e30;
@@ -803,6 +828,7 @@ void apgd_solve_fused(Scene& S) {
     NGc = NgNew;
     y_restart = restart;
     yb = Beta;
+    if (S.P.anti_relaxation) anti_relax(S, Gc.data(), ar);
   }
   (void)have_best;
   schur(S, best.data(), T.data(), bt);
@@ -823,7 +849,7 @@ void apgd_solve(Scene& S) {
   resize_gamma(S);
   std::vector<double> gam = solve_vector(S);
   double* gamma = gam.data();
-  std::vector<double> gHat(n3, 1.0), gNew(n3), g(n3), y(n3), yNew(n3), T(n3), bt;
+  std::vector<double> gHat(n3, 1.0), gNew(n3), g(n3), y(n3), yNew(n3), T(n3), ar(n3, 0.0), bt;
   for (int64_t i = 0; i < n3; ++i) y[i] = gamma[i];
 
   double theta = 1.0, thetaNew = theta, Beta = 0.0, obj1 = 0.0, obj2 = 0.0;
@@ -887,6 +913,7 @@ void apgd_solve(Scene& S) {
     theta = thetaNew;
     for (int64_t i = 0; i < n3; ++i) gamma[i] = gNew[i];
     for (int64_t i = 0; i < n3; ++i) y[i] = yNew[i];
+    if (S.P.anti_relaxation) anti_relax(S, gamma, ar);
   }
   /* APGD.cu:353-354 */
   schur(S, gHat.data(), T.data(), bt);
@@ -1125,7 +1152,7 @@ int do_step(Scene& S) {
   build_k(S);
   int n = 3 * S.nb;
   double h = S.P.h;
-  if (S.nbil && S.P.solver != 1) {
+  if ((S.nbil && S.P.solver != 1) || (S.nbil && S.P.anti_relaxation)) {
     S.st.status = 4;  /* PGJ / PGS take no bilateral rows (PGJ.cu, PGS.cu size 3 nc) */
     return S.st.status;
   }

@@ -37,6 +37,7 @@ typedef struct or_params {
   int threads;            /* OpenMP threads, 0 = runtime default */
   int apgd_mode;          /* 0 = fused sequence shared with the GPU, 1 = literal reference sequence */
   int solver;             /* System(solverType): 1 = APGD (APGD.cu), 5 = PGJ (PGJ.cu) */
+  int anti_relaxation;    /* APGD::setAntiRelaxation (APGD.cuh:63, APGD.cu:335-345) */
   int fp64_narrowphase;   /* extension: 1 = FP64 sqrt in length/normalize of the narrowphase and
                              the tangent frame (the reference uses float, helper_math_double.h) */
 } or_params;

@@ -37,7 +37,8 @@ class OrParams(C.Structure):
                 ("max_iterations", C.c_int), ("warm_start", C.c_int),
                 ("reduce_mode", C.c_int), ("spmv_mode", C.c_int),
                 ("max_backtracks", C.c_int), ("threads", C.c_int), ("apgd_mode", C.c_int),
-                ("solver", C.c_int), ("fp64_narrowphase", C.c_int)]
+                ("solver", C.c_int), ("anti_relaxation", C.c_int),
+                ("fp64_narrowphase", C.c_int)]
 
 
 class OrStats(C.Structure):
@@ -122,6 +123,7 @@ def make_params(p: dict, reduce_mode=0, spmv_mode=0, threads=0, apgd_mode=0) -> 
     o.apgd_mode = apgd_mode
     o.solver = int(p.get("solver", 1))
     o.fp64_narrowphase = int(p.get("fp64_narrowphase", 0))
+    o.anti_relaxation = int(p.get("anti_relaxation", 0))
     return o
 
 
