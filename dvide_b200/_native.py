@@ -28,7 +28,7 @@ EXPORTS = [
     "dv_set_params", "dv_step", "dv_collide", "dv_apgd_solve", "dv_get_state", "dv_set_state",
     "dv_get_contact_force", "dv_get_num_contacts", "dv_get_contacts", "dv_get_gamma",
     "dv_set_gamma", "dv_add_bilateral_dof", "dv_get_bilateral_gamma", "dv_get_frames",
-    "dv_get_schur_vector", "dv_ccp_violation", "dv_energies",
+    "dv_get_schur_vector", "dv_get_step_vectors", "dv_ccp_violation", "dv_energies",
     "dv_contact_forces_per_collision", "dv_get_step_stats", "dv_status_string", "dv_last_error",
     "dv_scene_launch_count", "dv_get_step_history", "dv_clear_step_history",
     "dv_get_phase_times", "dv_ccp_violation_noalloc", "dv_selftest_bounded_waits",
@@ -169,6 +169,7 @@ def lib():
         "dv_get_gamma": [vp, dp, C.c_int32, ip],
         "dv_set_gamma": [vp, dp, C.c_int32],
         "dv_add_bilateral_dof": [vp, C.c_int32, C.c_int32, C.c_double, C.c_double],
+        "dv_get_step_vectors": [vp, dp, dp, dp],
         "dv_get_bilateral_gamma": [vp, dp, C.c_int32, ip],
         "dv_get_frames": [vp, dp],
         "dv_get_schur_vector": [vp, dp],
@@ -418,6 +419,14 @@ class NativeScene:
         if n.value:
             check(lib().dv_get_bilateral_gamma(self.h, dptr(g), n.value, C.byref(n)))
         return g
+
+    def step_vectors(self):
+        """r, b (bilateral rows first, then 3 per contact) and k (3 per body)
+        of the last step (System::r_d, b_d, k_d)."""
+        n = 3 * self.num_contacts()[0] + len(self.bilateral_gamma())
+        r, b, k = np.zeros(n), np.zeros(n), np.zeros(3 * self.nb)
+        check(lib().dv_get_step_vectors(self.h, dptr(r), dptr(b), dptr(k)))
+        return r, b, k
 
     def ccp_violation(self):
         o = np.zeros(4)

@@ -286,6 +286,101 @@ int System::outputContactForcePerCollision(std::string filename) {
   return 0;
 }
 
+// System.cu:1297-1319: the contact forces of the last step on stdout.
+int System::outputContactForcePerCollision() {
+  if (!scene) return DV_ERR_ARG;
+  int32_t nc = 0, np = 0;
+  dv_get_num_contacts(scene, &nc, &np);
+  std::vector<uint32_t> a(nc), b(nc);
+  std::vector<double> loc(3 * (size_t)nc), fn(3 * (size_t)nc), ff(3 * (size_t)nc);
+  if (nc) {
+    dv_get_contacts(scene, a.data(), b.data(), nullptr, loc.data());
+    dv_contact_forces_per_collision(scene, fn.data(), ff.data());
+  }
+  for (int i = 0; i < nc; ++i) {
+    printf("Collision #%d: Body %u to %u\n", i, a[i], b[i]);
+    printf("  Collision location: (%f, %f, %f)\n", loc[3 * i], loc[3 * i + 1], loc[3 * i + 2]);
+    printf("  Collision normal:   (%f, %f, %f)\n", fn[3 * i], fn[3 * i + 1], fn[3 * i + 2]);
+    printf("  Collision friction: (%f, %f, %f)\n\n", ff[3 * i], ff[3 * i + 1], ff[3 * i + 2]);
+  }
+  return 0;
+}
+
+namespace {
+
+struct MMEntry {
+  int i, j;
+  double v;
+};
+
+// Matrix Market files as cusp::io::write_matrix_market_file writes them
+// (coordinate for sparse matrices, array for vectors; 1-based indices);
+// values with 17 significant digits.
+int write_mm_coo(const std::string& path, int rows, int cols, const std::vector<MMEntry>& e) {
+  FILE* f = fopen(path.c_str(), "w");
+  if (!f) return DV_ERR_ARG;
+  fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n\t%d\t%d\t%zu\n", rows, cols,
+          e.size());
+  for (const MMEntry& x : e) fprintf(f, "%d %d %.17g\n", x.i + 1, x.j + 1, x.v);
+  fclose(f);
+  return 0;
+}
+
+int write_mm_array(const std::string& path, const std::vector<double>& v) {
+  FILE* f = fopen(path.c_str(), "w");
+  if (!f) return DV_ERR_ARG;
+  fprintf(f, "%%%%MatrixMarket matrix array real general\n\t%zu\t1\n", v.size());
+  for (double x : v) fprintf(f, "%.17g\n", x);
+  fclose(f);
+  return 0;
+}
+
+}  // namespace
+
+// System.cu:1912-1934: D, Minv, r, b and k of the last step in
+// <directory>/{D,Minv,r,b,k}.mtx.  D's rows: the bilateral rows (+1 at DOF A,
+// -1 at DOF B), then per contact the n, u and v rows with +F at body A's
+// three columns and -F at body B's (System.cu:622-638, 676-1257).
+int System::exportMatrices(std::string directory) {
+  if (!scene) return DV_ERR_ARG;
+  int32_t nc = 0, np = 0;
+  int rc = dv_get_num_contacts(scene, &nc, &np);
+  if (rc != DV_OK) return rc;
+  const int nb = (int)bodies.size(), nbil = (int)bilaterals.size();
+  const int rows = 3 * nc + nbil, cols = 3 * nb;
+  std::vector<uint32_t> ia(nc), ib(nc);
+  std::vector<double> F(9 * (size_t)nc);
+  if (nc) {
+    if ((rc = dv_get_contacts(scene, ia.data(), ib.data(), nullptr, nullptr)) != DV_OK) return rc;
+    if ((rc = dv_get_frames(scene, F.data())) != DV_OK) return rc;
+  }
+  std::vector<MMEntry> D;
+  D.reserve((size_t)nbil * 2 + 18 * (size_t)nc);
+  for (int i = 0; i < nbil; ++i) {
+    D.push_back(MMEntry{i, bilaterals[i].dofA, 1.0});
+    if (bilaterals[i].dofB >= 0) D.push_back(MMEntry{i, bilaterals[i].dofB, -1.0});
+  }
+  for (int c = 0; c < nc; ++c)
+    for (int k = 0; k < 3; ++k) {
+      const int row = nbil + 3 * c + k;
+      const double* f = &F[9 * (size_t)c + 3 * k];
+      for (int j = 0; j < 3; ++j) D.push_back(MMEntry{row, 3 * (int)ia[c] + j, f[j]});
+      for (int j = 0; j < 3; ++j) D.push_back(MMEntry{row, 3 * (int)ib[c] + j, -f[j]});
+    }
+  if ((rc = write_mm_coo(directory + "/D.mtx", rows, cols, D)) != 0) return rc;
+  std::vector<MMEntry> M;
+  for (int i = 0; i < nb; ++i) {
+    const double mi = bodies[i]->isFixed() ? 0.0 : 1.0 / bodies[i]->getMass();
+    for (int k = 0; k < 3; ++k) M.push_back(MMEntry{3 * i + k, 3 * i + k, mi});
+  }
+  if ((rc = write_mm_coo(directory + "/Minv.mtx", cols, cols, M)) != 0) return rc;
+  std::vector<double> r(rows), b(rows), k(cols);
+  if ((rc = dv_get_step_vectors(scene, r.data(), b.data(), k.data())) != DV_OK) return rc;
+  if ((rc = write_mm_array(directory + "/r.mtx", r)) != 0) return rc;
+  if ((rc = write_mm_array(directory + "/b.mtx", b)) != 0) return rc;
+  return write_mm_array(directory + "/k.mtx", k);
+}
+
 int APGD::setup() { return 0; }
 
 // Solver::solve() (APGD.cu:164-361, PGJ.cu:152-224, PGS.cu:367-459): the

@@ -185,7 +185,7 @@ __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
         residual = res;
         C->residual = res;
         C->objective = obj1;
-        C->objN = 0.5 * sm[0];
+        if (a.ar) C->objN = 0.5 * sm[0];
         C->best = c.nw;
       }
       if (residual < P.tol) {
@@ -665,7 +665,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
               s_st.nt = -__ldcg(&C->t);
               s_st.mu = a.seg[s].mu;
               s_st.exact = a.seg[s].exact;
-              s_st.rsel = __ldcg(&C->rsel);
+              if (kAR) s_st.rsel = __ldcg(&C->rsel);
             }
             s_st.part = part;
           }
@@ -879,7 +879,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           s_ps.gB = -1.0 / gd;
           s_ps.mu = a.seg[s].mu;
           s_ps.exact = a.seg[s].exact;
-          s_ps.rsel = __ldcg(&C->rsel);
+          if (kAR) s_ps.rsel = __ldcg(&C->rsel);
         }
         __syncthreads();
       };
@@ -900,7 +900,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         s = sc.s;
         load_ps(s);
         sc0 = sc.c0; st0 = sc.t0; snc = sc.nc;
-        issue(tcur, st0, sc0, snc, 0, 0, ps.cur, ps.nw, ps.restart, ps.rsel);
+        issue(tcur, st0, sc0, snc, 0, 0, ps.cur, ps.nw, ps.restart, kAR ? ps.rsel : 0);
       }
       while (seq >= 0) {
         const int ti = tcur;
@@ -926,11 +926,12 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         __syncwarp();  // the warp's reads of stage sidx^1 are done
         if (nseq >= 0 && !failed) {
           if (ns == s) {
-            issue(ntile, st0, sc0, snc, nsub, sidx ^ 1, ps.cur, ps.nw, ps.restart, ps.rsel);
+            issue(ntile, st0, sc0, snc, nsub, sidx ^ 1, ps.cur, ps.nw, ps.restart,
+                  kAR ? ps.rsel : 0);
           } else {
             const ApgdCtl* C = &a.sst[ns].ctl;
             issue(ntile, sc.t0, sc.c0, sc.nc, nsub, sidx ^ 1, __ldcg(&C->cur), __ldcg(&C->nw),
-                  __ldcg(&C->restart), __ldcg(&C->rsel));
+                  __ldcg(&C->restart), kAR ? __ldcg(&C->rsel) : 0);
           }
         }
         const int kw = (ti - st0) * kTileItems + sub * kSub + warp * 32;

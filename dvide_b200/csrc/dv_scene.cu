@@ -249,6 +249,47 @@ DV_API int dv_get_schur_vector(dv_scene* s, double* r) {
   return DV_OK;
 }
 
+DV_API int dv_get_step_vectors(dv_scene* s, double* r, double* b, double* k) {
+  if (!s) return DV_ERR_ARG;
+  Engine& E = s->E;
+  TRY(E.sync_state());
+  const int nc = E.seg_state(0).nc, c0 = E.seg_state(0).c0, nbil = E.num_bilateral(0);
+  const double h = s->P.h;
+  std::vector<double> hv;
+  if (r) {
+    if (nc) {
+      if (E.precision() == DV_PREC_MIXED)
+        TRY(E.download_planes_f(reinterpret_cast<const float*>(E.d.r), E.d.ccap, 3, c0, nc, hv));
+      else
+        TRY(E.download_planes(E.d.r, E.d.ccap, 3, c0, nc, hv));
+      interleave(hv, nc, 3, r + nbil, 3);
+    }
+    if (nbil) TRY(E.download(r, E.d.bil_work + 10 * (size_t)E.d.nbil, sizeof(double) * nbil));
+  }
+  if (b) {
+    // System.cu:1516-1524: (gap / h, 0, 0) per contact, as the solve kernel forms it
+    std::vector<double> g(nc);
+    if (nc) TRY(E.download(g.data(), E.d.gap + c0, sizeof(double) * nc));
+    for (int i = 0; i < nc; ++i) {
+      b[nbil + 3 * (size_t)i] = g[i] / h;
+      b[nbil + 3 * (size_t)i + 1] = 0.0;
+      b[nbil + 3 * (size_t)i + 2] = 0.0;
+    }
+    if (nbil) TRY(E.download(b, E.d.bil_b, sizeof(double) * nbil));
+  }
+  if (k) {
+    const int nb = E.d.nb;
+    std::vector<double4> k4(nb);
+    TRY(E.download(k4.data(), E.d.k4, sizeof(double4) * nb));
+    for (int i = 0; i < nb; ++i) {
+      k[3 * (size_t)i] = k4[i].x;
+      k[3 * (size_t)i + 1] = k4[i].y;
+      k[3 * (size_t)i + 2] = k4[i].z;
+    }
+  }
+  return DV_OK;
+}
+
 DV_API int dv_get_gamma(dv_scene* s, double* gamma, int32_t cap, int32_t* n) {
   if (!s) return DV_ERR_ARG;
   std::vector<double> g;

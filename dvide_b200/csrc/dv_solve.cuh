@@ -682,7 +682,7 @@ __device__ inline ApgdCtl ctl_read(const ApgdCtl* C) {
   c.nw = __ldcg(&C->nw); c.best = __ldcg(&C->best); c.yr = __ldcg(&C->yr);
   c.first = __ldcg(&C->first); c.backtracks = __ldcg(&C->backtracks); c.err = __ldcg(&C->err);
   c.iterations = __ldcg(&C->iterations); c.sweeps = __ldcg(&C->sweeps);
-  c.rsel = __ldcg(&C->rsel); c.objN = __ldcg(&C->objN);
+  c.rsel = __ldcg(&C->rsel);
   return c;
 }
 

@@ -101,6 +101,7 @@ int main(int argc, char** argv) {
     printf("pinned drift: %g\n", drift);
   }
   sys->exportSystem("settle_final.csv");
+  sys->exportMatrices(".");
   delete sys;
   return 0;
 }

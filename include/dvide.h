@@ -162,6 +162,11 @@ DV_API int dv_get_bilateral_gamma(dv_scene* s, double* gamma, int32_t cap, int32
  * of the last step: System.cu:753-762, 1561-1580. */
 DV_API int dv_get_frames(dv_scene* s, double* F);
 DV_API int dv_get_schur_vector(dv_scene* s, double* r);
+/* The last step's vectors as the reference holds them (System::r_d, b_d,
+ * k_d; System.cu:1502-1524, 1526-1580): r and b with 3 nc + nbil entries, the
+ * bilateral rows first (dv_add_bilateral_dof), then 3 per contact; k with 3
+ * per body.  Any pointer may be NULL.  System::exportMatrices writes them. */
+DV_API int dv_get_step_vectors(dv_scene* s, double* r, double* b, double* k);
 
 /* System::getCCPViolation (System.cu:1605-1643): out4 = (min gamma_n,
  * min v_n, gamma_n . v_n, ||cone violation||). */

@@ -93,7 +93,10 @@ class System {
   int exportSystem(std::string filename);
   int importSystem(std::string filename);
   int calculateContactForcePerCollision();
+  int outputContactForcePerCollision();
   int outputContactForcePerCollision(std::string filename);
+  // D, Minv, r, b, k of the last step as Matrix Market files in `directory`
+  int exportMatrices(std::string directory);
   std::vector<double> getPositions();
   std::vector<double> getVelocities();
   std::vector<double> getContactForces();

@@ -1318,6 +1318,25 @@ int or_get_frames(void* s, double* F) {
   return S->nc;
 }
 
+/* System::r_d, b_d, k_d of the last step (System.cu:1502-1580), the
+ * reference's layout: r and b with the bilateral rows first. */
+int or_get_step_vectors(void* s, double* r, double* b, double* k) {
+  Scene* S = (Scene*)s;
+  const int nc = S->nc, nbil = S->nbil;
+  const int64_t n3 = 3 * (int64_t)nc;
+  if ((int64_t)S->r.size() < n3 + nbil || (int64_t)S->bst.size() < n3) return -1;
+  for (int i = 0; i < nbil; ++i) {
+    if (r) r[i] = S->r[n3 + i];
+    if (b) b[i] = S->bB[i];
+  }
+  for (int64_t i = 0; i < n3; ++i) {
+    if (r) r[nbil + i] = S->r[i];
+    if (b) b[nbil + i] = S->bst[i];
+  }
+  if (k) memcpy(k, S->k.data(), sizeof(double) * 3 * (size_t)S->nb);
+  return (int)(n3 + nbil);
+}
+
 int or_get_r(void* s, double* r) {
   Scene* S = (Scene*)s;
   if ((int64_t)S->r.size() < 3 * (int64_t)S->nc) return -1;

@@ -71,6 +71,8 @@ int or_set_gamma(void* s, const double* gamma, int ncont);
 int or_get_contacts(void* s, uint32_t* a, uint32_t* b, double* nP, double* loc);
 int or_get_frames(void* s, double* F);     /* 9 per contact: n, u, v */
 int or_get_r(void* s, double* r);          /* 3 per contact (Schur vector of the last step) */
+/* r, b (bilateral rows first, then 3 per contact) and k (3 per body) of the last step */
+int or_get_step_vectors(void* s, double* r, double* b, double* k);
 int or_ccp_violation(void* s, double* out4);
 /* System::addBilateralConstraintDOF (before the first step); 0 or -1 */
 int or_add_bilateral(void* s, int dofA, int dofB, double velocity, double start_time);

@@ -67,6 +67,7 @@ def lib():
             getattr(L, name).argtypes = [C.c_void_p, C.c_int]
         L.or_collide.argtypes = [C.c_void_p]
         L.or_solve.argtypes = [C.c_void_p]
+        L.or_get_step_vectors.argtypes = [C.c_void_p, dp, dp, dp]
         L.or_get_stats.argtypes = [C.c_void_p, C.POINTER(OrStats)]
         L.or_get_state.argtypes = [C.c_void_p, dp, dp]
         L.or_set_state.argtypes = [C.c_void_p, dp, dp]
@@ -231,6 +232,13 @@ class OracleScene:
         if n:
             lib().or_get_bilateral_gamma(self.h, _dp(g))
         return g
+
+    def step_vectors(self):
+        """r, b (bilateral rows first) and k (3 per body) of the last step."""
+        n = 3 * self.stats()["num_contacts"] + len(self.bilateral_gamma())
+        r, b, k = np.zeros(n), np.zeros(n), np.zeros(3 * self.nb)
+        lib().or_get_step_vectors(self.h, _dp(r), _dp(b), _dp(k))
+        return r, b, k
 
     def ccp_violation(self):
         o = np.zeros(4)

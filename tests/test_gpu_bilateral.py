@@ -36,6 +36,8 @@ def _run(native, oracle_mod, sc, steps, min_solved=None):
         assert sg["objective"] == so["objective"], k
         assert sg["backtracks"] == so["backtracks"], k
         assert np.array_equal(g.ccp_violation(), o.ccp_violation()), k
+        for x, y in zip(g.step_vectors(), o.step_vectors()):  # r, b (rows first), k
+            assert np.array_equal(x, y), k
         solved += 1
     if min_solved is not None:
         assert solved >= min_solved

@@ -59,3 +59,35 @@ def test_settle_driver_with_pinned_spheres(tmp_path):
     drift = [l for l in out.stdout.splitlines() if l.startswith("pinned drift:")]
     assert len(drift) == 1
     assert float(drift[0].split(":")[1]) < 1e-5
+
+
+def _mm(path):
+    with open(path) as f:
+        head = f.readline()
+        dims = [int(x) for x in f.readline().split()]
+        body = [l.split() for l in f if l.strip()]
+    return head, dims, body
+
+
+def test_export_matrices(tmp_path):
+    """System::exportMatrices (System.cu:1912-1934), as models/test_compaction.cu
+    calls it: D (3 nc + nbil rows, 3 nb columns, 18 entries per contact and 1
+    per single-DOF row), Minv, r, b, k of the last step."""
+    out = subprocess.run([DRIVER, "30", "1", "1e-4", "1000", "1", "3"], cwd=tmp_path,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    nc = int([l for l in out.stdout.splitlines() if l and l[0].isdigit()][-1].split(",")[1])
+    nbil, nb = 6, 1005
+    head, dims, body = _mm(tmp_path / "D.mtx")
+    assert head.startswith("%%MatrixMarket matrix coordinate real general")
+    assert dims == [3 * nc + nbil, 3 * nb, 18 * nc + nbil] and len(body) == dims[2]
+    rows = np.array([int(b[0]) for b in body])
+    assert np.all(np.diff(rows) >= 0) and rows.min() == 1 and rows.max() == 3 * nc + nbil
+    head, dims, body = _mm(tmp_path / "Minv.mtx")
+    assert dims == [3 * nb, 3 * nb, 3 * nb]
+    assert all(float(b[2]) == 0.0 for b in body[:15])  # the five fixed boxes
+    for name, n in (("r", 3 * nc + nbil), ("b", 3 * nc + nbil), ("k", 3 * nb)):
+        head, dims, body = _mm(tmp_path / f"{name}.mtx")
+        assert head.startswith("%%MatrixMarket matrix array real general")
+        assert dims == [n, 1] and len(body) == n
+        assert all(np.isfinite(float(b[0])) for b in body)
