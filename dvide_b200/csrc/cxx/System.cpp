@@ -432,6 +432,30 @@ std::vector<uint32_t> CollisionDetector::getCollisionIdentifierB() {
   return b;
 }
 
+std::vector<double3> CollisionDetector::getCollisionLocations() {
+  std::vector<double> raw(3 * (size_t)numCollisions);
+  if (numCollisions) dv_get_contacts(system->scene, nullptr, nullptr, nullptr, raw.data());
+  std::vector<double3> out(numCollisions);
+  for (uint i = 0; i < numCollisions; ++i)
+    out[i] = make_double3(raw[3 * i], raw[3 * i + 1], raw[3 * i + 2]);
+  return out;
+}
+
+ContactIdArray::operator std::vector<uint>() const {
+  std::vector<uint32_t> v = b_ ? cd_->getCollisionIdentifierB() : cd_->getCollisionIdentifierA();
+  return std::vector<uint>(v.begin(), v.end());
+}
+size_t ContactIdArray::size() const { return cd_->numCollisions; }
+uint ContactIdArray::operator[](size_t i) const {
+  return static_cast<std::vector<uint>>(*this).at(i);
+}
+
+ContactLocationArray::operator std::vector<double3>() const { return cd_->getCollisionLocations(); }
+size_t ContactLocationArray::size() const { return cd_->numCollisions; }
+double3 ContactLocationArray::operator[](size_t i) const {
+  return cd_->getCollisionLocations().at(i);
+}
+
 std::vector<double4> CollisionDetector::getNormalsAndPenetrations() {
   std::vector<double> raw(4 * (size_t)numCollisions);
   if (numCollisions) dv_get_contacts(system->scene, nullptr, nullptr, raw.data(), nullptr);

@@ -100,6 +100,17 @@ int main(int argc, char** argv) {
       for (int k = 0; k < 2; ++k) drift = fmax(drift, fabs(p[3 * (5 + i) + k] - pin0[2 * i + k]));
     printf("pinned drift: %g\n", drift);
   }
+  // the contact list through the reference's field names (handles)
+  std::vector<uint> ida = sys->collisionDetector->collisionIdentifierA_d;
+  std::vector<double3> loc = sys->collisionDetector->collisionLocations_d;
+  sys->gamma_h = sys->gamma_d;
+  bool handles_ok = ida.size() == sys->collisionDetector->numCollisions &&
+                    loc.size() == sys->collisionDetector->collisionLocations_d.size() &&
+                    sys->gamma_h.size() == sys->gamma_d.size();
+  for (size_t i = 0; i < ida.size() && i < 16; ++i)
+    handles_ok = handles_ok && ida[i] == sys->collisionDetector->collisionIdentifierA_d[i] &&
+                 ida[i] < sys->collisionDetector->collisionIdentifierB_d[i];
+  printf("contact handles: %s\n", handles_ok ? "ok" : "mismatch");
   sys->exportSystem("settle_final.csv");
   sys->exportMatrices(".");
   delete sys;

@@ -66,7 +66,7 @@ class System {
   double totalGPUMemoryUsed;
   double objectiveCCP;
   DeviceArray p_d, v_d, f_contact_d, gamma_d;
-  std::vector<double> p_h, v_h, f_contact_h;
+  std::vector<double> p_h, v_h, f_contact_h, gamma_h;
 
   double getCurrentTime() const { return time; }
   double getTimeStep() const { return h; }

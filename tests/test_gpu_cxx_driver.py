@@ -23,6 +23,7 @@ def test_settle_driver_runs(tmp_path):
     assert os.path.exists(tmp_path / "settle_final.csv")
     rows = open(tmp_path / "settle_final.csv").read().splitlines()
     assert rows[0].startswith("1005,") and len(rows) == 1006
+    assert "contact handles: ok" in out.stdout
 
 
 def test_unsupported_solver_type_reports(tmp_path):
