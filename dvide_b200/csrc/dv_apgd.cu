@@ -148,7 +148,9 @@ __device__ __noinline__ void ctl_step(CtlArgs a, int s, double* scratch) {
   }
 }
 
-__device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
+// `direct`: an engine of one scene, whose controller runs at the product
+// pass's barrier: it sets step_needed itself (no arrival counter to latch).
+__device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch, bool direct = false) {
   double sm[7], res;
   fold_tiles_sm<7, 1>(a, a.sst[s].t0, a.sst[s].nt, sm, &res, kQMax, scratch);
   if (threadIdx.x == 0) {
@@ -175,10 +177,12 @@ __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch) {
         C->L = L;
         C->t = 1.0 / L;
         C->mode = 1;
-        atomicAdd(&a.ew->step_count, 1);
+        if (direct) *(volatile int*)&a.ew->step_needed = 1;
+        else atomicAdd(&a.ew->step_count, 1);
       }
     } else {
       C->mode = 0;
+      if (direct) *(volatile int*)&a.ew->step_needed = 0;
       C->sweeps = c.sweeps + 1;
       double residual = c.residual;
       if (res < residual) {
@@ -618,7 +622,10 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // the product pass's barrier also decides whether the work lists are rebuilt:
   // once half the segments iterating at the last build have finished
   auto latch_product = [&]() {
-    if (single) ctl_product(ca, 0, scratch);
+    if (single) {
+      ctl_product(ca, 0, scratch, true);
+      return;
+    }
     if (threadIdx.x == 0) {
       volatile EngineWords* E = a.ew;
       const int n = atomicExch(&a.ew->step_count, 0);
