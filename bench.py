@@ -60,7 +60,7 @@ def solve_bytes(nc, nb, sweeps, backtracks):
 # DRAM bytes per algorithmic byte of the solve kernel, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum = 6.350 GB) on a 30-iteration
 # launch on this workload (11.415 GB algorithmic); the full launch is scaled by it.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 6.350105 / 11.415179
+TRAFFIC_PER_ALGORITHMIC_BYTE = 6.244004 / 11.415179
 
 
 def collide_bytes(nc, nb, npossible):
