@@ -92,7 +92,12 @@ struct dv_server {
       E.reset(new Engine());
       rc = E->init(in, cfg.precision);
       if (rc == DV_OK && user_stream) rc = E->set_stream(user_stream);
-      if (rc == DV_OK) E->set_launch(E->max_ctas(), 1, 0, 2);
+      // FP32 iterates fit three CTAs per SM (80 registers); results do not
+      // depend on the launch shape
+      if (rc == DV_OK) {
+        if (cfg.precision == DV_PREC_MIXED) E->set_launch(E->max_ctas_for(3), 1, 1, 3);
+        else E->set_launch(E->max_ctas(), 1, 0, 2);
+      }
     } else {
       rc = E->reconfigure(slots);
     }
