@@ -8,7 +8,7 @@ failure reports its size."""
 import numpy as np
 import pytest
 
-from dvide_b200 import scenes
+from dvide_b200 import scenes, workloads
 
 pytestmark = pytest.mark.gpu
 
@@ -226,3 +226,46 @@ def test_repeatable_bits(native):
         out.append(g.state() + (g.gamma(),))
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+def _free_running(native, oracle_mod, sc, steps):
+    """Both sides step the same scene on their own; every step bit-identical."""
+    g, o = _pair(native, oracle_mod, sc)
+    for k in range(steps):
+        assert o.step(1) == 0, k
+        g.step(1)
+        so, sg = o.stats(), g.stats()
+        assert sg["num_contacts"] == so["num_contacts"], k
+        for key in ("iterations", "backtracks", "residual", "objective"):
+            assert sg[key] == so[key], (k, key)
+        assert np.array_equal(g.gamma(), o.gamma()), k
+        pg, vg = g.state()
+        po, vo = o.state()
+        assert np.array_equal(vg, vo) and np.array_equal(pg, po), k
+        assert np.array_equal(g.ccp_violation(), o.ccp_violation()), k
+    return o.stats()
+
+
+def test_c0_compressed_free_running(native, oracle_mod):
+    """The 1,000-sphere settling box (C0 settings: mu 0.25, h 1e-3, tolerance 1e-4,
+    1,000 iterations, warm start) with the lattice squeezed so that ~1,800 contacts
+    are active from the first step, free running for 25 steps while it springs apart."""
+    sc = scenes.settling_box()
+    p = sc.pos.copy()
+    p[5:, :2] *= 0.905
+    p[5:, 2] = 0.05 + (p[5:, 2] - 0.06) * 0.905
+    sc.pos = p
+    st = _free_running(native, oracle_mod, sc, 25)
+    assert st["num_contacts"] > 100
+
+
+def test_column_sample_free_running(native, oracle_mod):
+    """The lowest 5,000 spheres of the settled 200,000-sphere column (its
+    settings: mu 0.3, h 5e-4, tolerance 1e-4, 500 iterations, warm start):
+    ~16,400 contacts, free running for 6 steps."""
+    d = np.load(workloads.COLUMN_FILE)
+    order = np.argsort(d["pos"][:, 2])[:5000]
+    sc = workloads._column_scene(d["pos"][order].astype(np.float64),
+                                 d["radius"][order].astype(np.float64), float(d["wall_height"]))
+    st = _free_running(native, oracle_mod, sc, 6)
+    assert st["num_contacts"] > 15000
