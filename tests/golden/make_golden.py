@@ -52,8 +52,9 @@ def oracle_fixtures():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None,
+                    help="reference source tree (needed for the helper_math golden vectors)")
     args = ap.parse_args()
-    if os.path.isdir(os.path.join(args.ref, "src")):
+    if args.ref and os.path.isdir(os.path.join(args.ref, "src")):
         helper_golden(args.ref)
     oracle_fixtures()
