@@ -68,7 +68,8 @@ class Params(C.Structure):
                 ("envelope", C.c_double), ("tolerance", C.c_double),
                 ("max_iterations", C.c_int32), ("warm_start", C.c_int32), ("solver", C.c_int32),
                 ("precision", C.c_int32), ("max_backtracks", C.c_int32), ("verbose", C.c_int32),
-                ("fp64_narrowphase", C.c_int32), ("anti_relaxation", C.c_int32)]
+                ("fp64_narrowphase", C.c_int32), ("anti_relaxation", C.c_int32),
+                ("refine_iterations", C.c_int32)]
 
 
 class StepStats(C.Structure):
@@ -76,7 +77,8 @@ class StepStats(C.Structure):
                 ("iterations", C.c_int32), ("backtracks", C.c_int32), ("residual", C.c_double),
                 ("objective", C.c_double), ("elapsed_ms", C.c_double), ("time", C.c_double),
                 ("time_index", C.c_int32), ("status", C.c_int32), ("collide_ms", C.c_double),
-                ("solve_ms", C.c_double), ("sweeps", C.c_int32), ("pad_", C.c_int32)]
+                ("solve_ms", C.c_double), ("sweeps", C.c_int32),
+                ("refine_iterations", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -258,6 +260,7 @@ def make_params(p: dict, precision=DV_PREC_FP64) -> Params:
     o.verbose = int(p.get("verbose", 0))
     o.fp64_narrowphase = int(p.get("fp64_narrowphase", 0))
     o.anti_relaxation = int(p.get("anti_relaxation", 0))
+    o.refine_iterations = int(p.get("refine_iterations", 0))
     return o
 
 

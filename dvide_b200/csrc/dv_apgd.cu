@@ -41,6 +41,8 @@
 //
 // Work is split in tiles of 512 contacts (2 per thread) and 256 bodies.
 // Every wait has a time limit.
+#include <algorithm>
+
 #include "dv_solve.cuh"
 
 namespace dv {
@@ -59,12 +61,17 @@ struct StepScalars {
   double ya, ym, nt, mu;
 };
 
+// Mixed precision with refinement: the FP32 phase of a solve ends when its
+// best residual has not improved for this many accepted iterations.
+constexpr int kStallIterations = 50;
+
 // What the segment controllers read and write, passed by value.
 struct CtlArgs {
   double* part;
   int tcap;
   int mixed;  // FP32 iterates: the Lipschitz test allows float-noise differences
   int ar;     // anti-relaxation: an accepted, unconverged iterate moves r to the next plane
+  int refine; // FP64 refinement launch: only the solves the FP32 launch marked, <= seg.refine iterations
   SegState* sst;
   const SegParams* seg;
   EngineWords* ew;
@@ -86,6 +93,8 @@ __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
   if (threadIdx.x == 0) {
     const SegParams& P = a.seg[s];
     ApgdCtl* C = &a.sst[s].ctl;
+    // refinement launch: a solve the FP32 phase finished keeps its result
+    if (a.refine && !__ldcg(&C->refined)) return;
     const double L = sqrt(sm[0]) / __ldcg(&C->L0);
     C->L = L;
     C->t = 1.0 / L;
@@ -119,7 +128,8 @@ __device__ __noinline__ void ctl_lipschitz(CtlArgs a, int s, double* scratch) {
     C->obj2_base = 0.0;
     C->rsel = 0;
     C->objN = 0.0;
-    if (P.max_iter <= 0) {
+    C->since_best = 0;
+    if ((a.refine ? P.refine : P.max_iter) <= 0) {
       mark_done(a, s);
     } else {
       C->done = 0;
@@ -185,14 +195,21 @@ __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch, bool
       if (direct) *(volatile int*)&a.ew->step_needed = 0;
       C->sweeps = c.sweeps + 1;
       double residual = c.residual;
+      int since_best = c.since_best + 1;
       if (res < residual) {
         residual = res;
         C->residual = res;
         C->objective = obj1;
         if (a.ar) C->objN = 0.5 * sm[0];
         C->best = c.nw;
+        since_best = 0;
       }
+      C->since_best = since_best;
       if (residual < P.tol) {
+        finished = true;
+      } else if (a.mixed && P.refine > 0 && since_best >= kStallIterations) {
+        // FP32 iterates no longer improve: the FP64 refinement continues
+        // from gamma_hat
         finished = true;
       } else {
         // APGD.cu:335-345 after this iteration: r moves to the plane the
@@ -210,7 +227,7 @@ __device__ __noinline__ void ctl_product(CtlArgs a, int s, double* scratch, bool
         C->nw = free_slot(c.nw, c.cur, c.prev, c.best);
         k += 1;
         C->k = k;
-        if (k >= P.max_iter) {
+        if (k >= (a.refine ? P.refine : P.max_iter)) {
           finished = true;
         } else {
           const double tn = (-(th * th) + th * sqrt(th * th + 4.0)) / 2.0;
@@ -339,8 +356,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     s_def.fail = 0;
   }
   __syncthreads();
-  const CtlArgs ca{a.part, a.tcap, sizeof(T) != sizeof(double) ? 1 : 0, kAR ? 1 : 0, a.sst,
-                   a.seg, a.ew, a.donemask};
+  const CtlArgs ca{a.part,  a.tcap, sizeof(T) != sizeof(double) ? 1 : 0, kAR ? 1 : 0, a.refine,
+                   a.sst,   a.seg,  a.ew, a.donemask};
 
   // ---- work lists off; per-segment solve state; done mask (bit set: not iterating)
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -350,11 +367,25 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   }
   for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.nseg; s += gridDim.x * kThreads) {
     SegState& X = a.sst[s];
-    X.err = 0u;
     X.arrive = 0u;
     ApgdCtl& C = X.ctl;
     // System.cu:560: a solve runs with contacts or bilateral rows
     const bool live = a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0);
+    if (a.refine) {
+      // FP64 refinement: only the solves the FP32 launch marked; the others
+      // keep their result, counts and error bits
+      if (!(live && C.refined)) {
+        C.done = 1;
+        continue;
+      }
+      C.it_lo = C.iterations;
+      C.bt_lo = C.backtracks;
+      C.sw_lo = C.sweeps;
+    } else {
+      C.refined = 0;
+      C.refine_it = 0;
+    }
+    X.err = 0u;
     C.done = live ? 0 : 1;
     C.iterations = 0;
     C.sweeps = 0;
@@ -367,7 +398,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
     unsigned m = 0u;
     for (int j = 0; j < 32; ++j) {
       const int s = wi * 32 + j;
-      if (s >= a.nseg || !(a.seg[s].active && (a.sst[s].nc > 0 || a.seg[s].nbil > 0)))
+      if (s >= a.nseg || !(a.seg[s].active && (a.sst[s].nc > 0 || a.seg[s].nbil > 0)) ||
+          (a.refine && !a.sst[s].ctl.refined))
         m |= 1u << j;
     }
     a.donemask[wi] = m;
@@ -474,7 +506,9 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           a.r[1 * S + c] = (T)(0.0 + d1);
           a.r[2 * S + c] = (T)(0.0 + d2);
           double g0, g1, g2;
-          if (P.warm == 2) {
+          // refinement: positional, from the FP32 phase's gamma_hat of this step
+          const int warm = a.refine ? 1 : P.warm;
+          if (warm == 2) {
             // matched: the impulse the same (A, B) pair had at the last solve;
             // A's earlier contacts are sorted by B, so a binary search finds it
             const uint32_t ia = __ldg(a.ida + c);
@@ -493,7 +527,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
               g1 = a.gamma[1 * a.WS + wj];
               g2 = a.gamma[2 * a.WS + wj];
             }
-          } else if (P.warm) {
+          } else if (warm) {
             const size_t wi = (size_t)P.wbase + k;
             g0 = k < gsize ? a.gamma[0 * a.WS + wi] : 0.0;
             g1 = k < gsize ? a.gamma[1 * a.WS + wi] : 0.0;
@@ -761,7 +795,9 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           int k = k0 + m * kThreads + threadIdx.x;
           if (k < nc) {
             const int c = c0 + k;
-            Frame<T> f = load_frame<T>(a, c, s_st.exact != 0);
+            const T* nrm = normal_planes<T>(a);
+            Frame<T> f = iter_frame<T, (DV_STORED_FRAME & 2) != 0>(a, c, nrm[c], nrm[S + c],
+                                                                   nrm[2 * S + c], s_st.exact != 0);
             T c0v = Gc[0 * S + c], c1v = Gc[1 * S + c], c2v = Gc[2 * S + c];
             T y0, y1, y2, N0, N1, N2;
             if (yr) {
@@ -953,7 +989,8 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           const uint32_t* su = reinterpret_cast<const uint32_t*>(sd + (size_t)kStagePlanes * 32);
           const int j = lane;
           Frame<T> f =
-              make_frame<T>(sd[0 * 32 + j], sd[1 * 32 + j], sd[2 * 32 + j], ps.exact != 0);
+              iter_frame<T, (DV_STORED_FRAME & 1) != 0>(a, c, sd[0 * 32 + j], sd[1 * 32 + j],
+                                                         sd[2 * 32 + j], ps.exact != 0);
           V wa = wv[su[j]], wb = wv[su[32 + j]];
           T N0, N1, N2;
           ft_times<T, V>(f, wa, wb, &N0, &N1, &N2);
@@ -1159,6 +1196,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // ---- gamma = gamma_hat (APGD.cu:358) into the warm-start region; q = F gamma (FP64)
   {
     int cs = -1, cbest = -1;
+    bool keep = false;
     const T* src = nullptr;
     for (int i = 0;; ++i) {
       const int t = cta_tile(a, NT, i);
@@ -1169,6 +1207,9 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         cs = s;
         cbest = __ldcg(&a.sst[s].ctl.best);
         src = cbest >= 0 ? a.G[cbest] : nullptr;
+        // refinement launch: a solve it did not refine, or whose FP64 phase
+        // accepted no iterate, keeps the FP32 phase's gamma_hat
+        keep = a.refine && (!__ldcg(&a.sst[s].ctl.refined) || cbest < 0);
       }
       const SegParams& P = a.seg[s];
       const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
@@ -1189,13 +1230,17 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         if (k < nc) {
           const int c = c0 + k;
           double x0 = 1.0, x1 = 1.0, x2 = 1.0;
-          if (src) {
-            x0 = (double)src[0 * S + c]; x1 = (double)src[1 * S + c]; x2 = (double)src[2 * S + c];
-          }
           const size_t wi = (size_t)P.wbase + k;
-          a.gamma[0 * a.WS + wi] = x0;
-          a.gamma[1 * a.WS + wi] = x1;
-          a.gamma[2 * a.WS + wi] = x2;
+          if (keep) {
+            x0 = a.gamma[0 * a.WS + wi]; x1 = a.gamma[1 * a.WS + wi]; x2 = a.gamma[2 * a.WS + wi];
+          } else {
+            if (src) {
+              x0 = (double)src[0 * S + c]; x1 = (double)src[1 * S + c]; x2 = (double)src[2 * S + c];
+            }
+            a.gamma[0 * a.WS + wi] = x0;
+            a.gamma[1 * a.WS + wi] = x1;
+            a.gamma[2 * a.WS + wi] = x2;
+          }
           a.wid[wi] = __ldg(a.idb + c) - (uint32_t)P.b0;
           Frame<double> f = load_frame_fp64(a, c, P.exact != 0);
           a.qd[c] = f_times<double, double4>(f, x0, x1, x2);
@@ -1242,7 +1287,20 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // warm-start length of every segment that solved (System::gamma_d resize)
   for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.nseg; s += gridDim.x * kThreads) {
     SegState& X = a.sst[s];
-    if (a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0)) X.gsize = X.nc;
+    const bool live = a.seg[s].active && (X.nc > 0 || a.seg[s].nbil > 0);
+    if (live) X.gsize = X.nc;
+    ApgdCtl& C = X.ctl;
+    if (sizeof(T) != sizeof(double) && a.seg[s].refine > 0 && live) {
+      // mixed precision: a solve that ended above the tolerance is refined
+      // in FP64 by the launch that follows
+      C.refined = (X.err == 0u && !(C.residual < a.seg[s].tol)) ? 1 : 0;
+    }
+    if (a.refine && live && C.refined) {
+      C.refine_it = C.iterations;
+      C.iterations += C.it_lo;
+      C.backtracks += C.bt_lo;
+      C.sweeps += C.sw_lo;
+    }
     // System::time += h (System.cu:584), read by the next step's rows
     if (a.nbil && a.seg[s].active && !a.solve_only) a.seg_time[s] = a.seg_time[s] + a.seg[s].h;
   }
@@ -1268,10 +1326,12 @@ void prepare_kernel() {
 
 
 template <class T, int MB, bool AR = false>
-void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only) {
+void launch_typed(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, bool solve_only,
+                  bool refine = false) {
   prepare_kernel<T, MB, AR>();
   KArgs<T> a = make_kargs<T>(sd, cfg);
   a.solve_only = solve_only ? 1 : 0;
+  a.refine = refine ? 1 : 0;
   void* params[] = {&a};
   cudaLaunchCooperativeKernel((const void*)k_step_solve<T, MB, AR>, cfg.grid, kThreads, params,
                               dyn_smem_bytes<T>(), st);
@@ -1308,8 +1368,20 @@ void launch_step_solve(SceneDev& sd, const SolveConfig& cfg, cudaStream_t st, in
   } else if (sd.solver == DV_SOLVER_PGS) {
     launch_pgs_solve(sd, cfg, st, solve_only);
   } else if (sd.precision == DV_PREC_MIXED) {
-    if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st, solve_only);
-    else launch_typed<float, 2>(sd, cfg, st, solve_only);
+    // with refinement the FP32 launch stops before the update, and an FP64
+    // launch refines the solves it marked, then updates
+    const bool refine = sd.refine_any != 0;
+    if (cfg.blocks_per_sm == 3) launch_typed<float, 3>(sd, cfg, st, solve_only || refine);
+    else launch_typed<float, 2>(sd, cfg, st, solve_only || refine);
+    if (refine) {
+      ++*launches;
+      SolveConfig c2 = cfg;
+      c2.blocks_per_sm = 2;
+      c2.grid = std::min(cfg.grid, std::max(1, sd.refine_grid));
+      cudaMemsetAsync(sd.ew->bar, 0, sizeof(sd.ew->bar), st);
+      cudaMemsetAsync(&sd.ew->last_release, 0, sizeof(unsigned long long), st);
+      launch_typed<double, 2>(sd, c2, st, solve_only, true);
+    }
   } else if (sd.anti_relax) {
     launch_typed<double, 2, true>(sd, cfg, st, solve_only);
   } else {

@@ -41,6 +41,7 @@ void fill_step_stats(const StepRecord& r, int s, dv_step_stats* out) {
   out->residual = X.ctl.residual;
   out->objective = X.ctl.objective;
   out->sweeps = X.ctl.sweeps;
+  out->refine_iterations = X.ctl.refine_it;
   out->elapsed_ms = r.ms_total;
   out->collide_ms = r.ms_collide;
   out->solve_ms = r.ms_solve;
@@ -81,6 +82,7 @@ static int check_params(const dv_params& p) {
   if (p.warm_start < 0 || p.warm_start > 2) return DV_ERR_ARG;
   if (p.fp64_narrowphase != 0 && p.fp64_narrowphase != 1) return DV_ERR_ARG;
   if (p.anti_relaxation != 0 && p.anti_relaxation != 1) return DV_ERR_ARG;
+  if (p.refine_iterations < 0) return DV_ERR_ARG;
   // anti-relaxation: an APGD option, FP64 only
   if (p.anti_relaxation && (p.solver != DV_SOLVER_APGD || p.precision != DV_PREC_FP64))
     return DV_ERR_UNSUPPORTED;
@@ -139,6 +141,14 @@ int Engine::alloc_contacts(size_t cap) {
 int Engine::upload_segments() {
   DV_CUDA_TRY(cudaMemcpyAsync(d.seg, hseg_.data(), sizeof(SegParams) * hseg_.size(),
                               cudaMemcpyHostToDevice, st_));
+  // a second (FP64) solve launch per step when a segment asks for refinement
+  int ra = 0;
+  for (const SegParams& G : hseg_) ra |= (G.active && G.refine > 0) ? 1 : 0;
+  if (ra != d.refine_any) {
+    d.refine_any = ra;
+    if (ra && !d.refine_grid) d.refine_grid = apgd_max_ctas(DV_PREC_FP64, 2);
+    drop_graph();
+  }
   return DV_OK;
 }
 
@@ -308,6 +318,7 @@ int Engine::reconfigure(const std::vector<SlotSpec>& slots) {
       G.warm = P.warm_start;
       G.exact = P.fp64_narrowphase;
       G.ar = P.anti_relaxation;
+      G.refine = P.refine_iterations;
       G.active = 1;
       G.b0 = nb2;
       G.b1 = nb2 + n;
@@ -639,6 +650,7 @@ int Engine::set_segment_params(int s, const dv_params& P) {
   G.warm = P.warm_start;
   G.exact = P.fp64_narrowphase;
   G.ar = P.anti_relaxation;
+  G.refine = P.refine_iterations;
   if (P.solver != P_[s].solver) {
     if (d.nseg != 1) return DV_ERR_UNSUPPORTED;
     d.solver = P.solver;

@@ -68,6 +68,7 @@ struct SegParams {
   int wbase, wcap;          // warm-start region [wbase, wbase + wcap) of the gamma arena
   int bil0, nbil;           // bilateral DOF rows [bil0, bil0 + nbil) (System.cu:510-532)
   int ar;                   // APGD anti-relaxation (APGD.cu:335-345)
+  int refine;               // mixed precision: FP64 iterations after a stalled FP32 phase (0: off)
 };
 
 // Scalar state of one APGD solve (APGD.cu:208-223, 266-332).  Iterates live in
@@ -97,6 +98,14 @@ struct ApgdCtl {
   int sweeps;           // iterations executed
   int rsel;             // anti-relaxation: plane of the current r_n and ar (the other: next)
   double objN;          // anti-relaxation: half of gamma_hat . N gamma_hat
+  // mixed precision with FP64 refinement: accepted iterations since the best
+  // residual last improved (FP32 phase); whether the FP64 phase refines this
+  // solve (set at the end of the FP32 phase); the FP64 phase's iterations; the
+  // FP32 phase's counts while the FP64 phase runs
+  int since_best;
+  int refined;
+  int refine_it;
+  int it_lo, bt_lo, sw_lo;
 };
 
 // Per-segment results of the current step (device-written).
@@ -217,6 +226,10 @@ struct SceneDev {
   // and the anti-relaxation vector, current and next (2 planes of ccap each),
   // and v = Minv (k + D^T x) of the iterate x under test (nb)
   int anti_relax = 0;
+  // mixed precision: some segment asks for FP64 refinement (a second,
+  // FP64 solve launch follows the FP32 one in every step)
+  int refine_any = 0;
+  int refine_grid = 0;          // co-resident CTAs of the FP64 solve kernel
   double* ar_r0 = nullptr;
   double* ar_v = nullptr;
   double4* v_ar = nullptr;

@@ -39,6 +39,7 @@ template <class T>
 struct KArgs {
   int nb, nseg;
   int solve_only;     // 1: the solve without the update (v, p, f_contact, clock untouched)
+  int refine;         // 1: FP64 refinement of the solves a mixed-precision launch marked
   int tcap;           // plane stride of the partials
   int chunk, contiguous;
   size_t S;           // plane stride of contact arrays
@@ -175,6 +176,28 @@ __device__ inline Frame<double> stored_frame(const KArgs<T>& a, int c) {
   f.u0 = __ldg(F + 3 * S + c); f.u1 = __ldg(F + 4 * S + c); f.u2 = __ldg(F + 5 * S + c);
   f.v0 = __ldg(F + 6 * S + c); f.v1 = __ldg(F + 7 * S + c); f.v2 = __ldg(F + 8 * S + c);
   return f;
+}
+
+// The frame of contact c in the iterating passes, with its normal already at
+// hand: in FP64 the tangents are read from the stored u, v planes (the bits
+// the narrowphase wrote, which rebuilding them from the normal reproduces),
+// taking the frame's FP64 division and float square roots off the passes'
+// latency chain; in FP32 they are rebuilt from the FP32 normal.
+#ifndef DV_STORED_FRAME
+#define DV_STORED_FRAME 0
+#endif
+template <class T, bool kStored = true>
+__device__ inline Frame<T> iter_frame(const KArgs<T>& a, int c, T n0, T n1, T n2, bool exact) {
+  if (sizeof(T) == sizeof(double) && kStored) {
+    const double* F = a.F;
+    const size_t S = a.S;
+    Frame<T> f;
+    f.n0 = n0; f.n1 = n1; f.n2 = n2;
+    f.u0 = (T)__ldg(F + 3 * S + c); f.u1 = (T)__ldg(F + 4 * S + c); f.u2 = (T)__ldg(F + 5 * S + c);
+    f.v0 = (T)__ldg(F + 6 * S + c); f.v1 = (T)__ldg(F + 7 * S + c); f.v2 = (T)__ldg(F + 8 * S + c);
+    return f;
+  }
+  return make_frame<T>(n0, n1, n2, exact);
 }
 
 // Stores of the vectors a pass writes and the next pass reads at once (q for
@@ -683,6 +706,7 @@ __device__ inline ApgdCtl ctl_read(const ApgdCtl* C) {
   c.first = __ldcg(&C->first); c.backtracks = __ldcg(&C->backtracks); c.err = __ldcg(&C->err);
   c.iterations = __ldcg(&C->iterations); c.sweeps = __ldcg(&C->sweeps);
   c.rsel = __ldcg(&C->rsel);
+  c.since_best = __ldcg(&C->since_best);
   return c;
 }
 
@@ -946,6 +970,7 @@ KArgs<T> make_kargs(SceneDev& sd, const SolveConfig& cfg) {
   a.nb = sd.nb;
   a.nseg = sd.nseg;
   a.solve_only = 0;
+  a.refine = 0;
   a.tcap = sd.tcap;
   a.chunk = cfg.chunk > 0 ? cfg.chunk : 1;
   a.contiguous = cfg.contiguous;

@@ -220,6 +220,20 @@ def ball_on_ground(h=1e-2, tolerance=1e-5, warm_start=0, latforce=0.0) -> Scene:
                  np.full(2, -1, dtype=np.int32), params, "ball_on_ground")
 
 
+def sphere_stack(n=5, radius=0.05, rho=2600.0, mu=0.25, h=1e-3, tolerance=1e-8,
+                 max_iterations=20000, warm_start=1, overlap=0.0) -> Scene:
+    """n equal spheres stacked on one vertical line on a fixed floor, each
+    touching the one below (gap -overlap): n contacts in a chain, every
+    normal exactly vertical.  The contact impulses are unique (the solve is
+    determinate): at rest the k-th contact from the top carries k m g h."""
+    z = radius - overlap + np.arange(n) * (2.0 * radius - overlap)
+    pos = np.stack([np.zeros(n), np.zeros(n), z], axis=1)
+    boxes = [((0.0, 0.0, -0.05), (0.5, 0.5, 0.05), True)]
+    params = default_params(h=h, mu=mu, gravity=(0.0, 0.0, -G), tolerance=tolerance,
+                            max_iterations=max_iterations, warm_start=warm_start)
+    return _assemble(boxes, pos, np.full(n, radius), rho, params, f"stack_{n}")
+
+
 def random_cluster(seed, n=40, box=True, radius=0.05, mu=0.25, h=1e-3, warm_start=1,
                    max_iterations=400, tolerance=1e-6) -> Scene:
     """Small parity-test scene: spheres on a jittered cubic lattice whose

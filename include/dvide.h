@@ -74,6 +74,11 @@ typedef struct dv_params {
   int32_t anti_relaxation;  /* APGD::setAntiRelaxation (APGD.cuh:63, APGD.cu:335-345), default 0;
                                FP64 APGD scenes of their own (not in batches or servers),
                                without bilateral rows and without dv_apgd_solve */
+  int32_t refine_iterations; /* extension, DV_PREC_MIXED APGD only, default 0 (off): at most
+                               this many FP64 APGD iterations after the FP32 ones, started
+                               from the FP32 best iterate, for every solve whose FP32 phase
+                               ended above the tolerance (iteration cap, or no new best
+                               residual for 50 accepted iterations) */
 } dv_params;
 
 /* Per-step report (System.cu:586-599 and APGD.cu:351-357). */
@@ -91,7 +96,7 @@ typedef struct dv_step_stats {
   double collide_ms;         /* device time of collision detection */
   double solve_ms;           /* device time of the persistent solve kernel */
   int32_t sweeps;            /* APGD iterations executed (iterations + 1 when converged) */
-  int32_t pad_;
+  int32_t refine_iterations; /* of `iterations`, those of the FP64 refinement (mixed precision) */
 } dv_step_stats;
 
 typedef struct dv_scene dv_scene;
@@ -203,12 +208,16 @@ DV_API int dv_get_phase_times(dv_scene* s, double* ns, int64_t* counts, int32_t 
  * (normalsAndPenetrations_d: normal B->A, gap), ida/idb per contact, v 3 per
  * body (System::v_d); out4 receives (min gamma_n, min v_n, gamma_n . v_n,
  * ||cone violation||) in device memory, queued on `stream` (a cudaStream_t,
- * NULL = legacy default stream).  Scratch is a fixed 1 MiB array in device
- * memory that each GPU holds until the process exits; nc above
- * DV_NOALLOC_MAX_CONTACTS is rejected with DV_ERR_ARG.  The first call on a
- * device looks the array's device address up (cudaGetSymbolAddress); make it
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU (unordered streams) race. */
+ * NULL = legacy default stream).  Every ida/idb must be below nb: a contact
+ * naming another body is not read, and all four outputs are NaN.  Results equal
+ * dv_ccp_violation's for the same scene bit for bit, NaN inputs included.
+ * Scratch is a fixed 1.75 MiB array in device memory that each CUDA context
+ * (each GPU, for the runtime's own contexts) holds until the process exits; nc
+ * above DV_NOALLOC_MAX_CONTACTS is rejected with DV_ERR_ARG.  The first call in
+ * a context looks the array's device address up (cudaGetSymbolAddress) and
+ * keeps it under the context's unique id; make that call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU
+ * (unordered streams) race. */
 #define DV_NOALLOC_MAX_CONTACTS 16777216
 DV_API int dv_ccp_violation_noalloc(int32_t nc, int32_t nb, const double* gamma, const double* nP,
                                     const uint32_t* ida, const uint32_t* idb, const double* v,
