@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include <cmath>
+#include <cstdlib>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -206,7 +208,65 @@ std::vector<double> System::getPositions() { return p_d; }
 std::vector<double> System::getVelocities() { return v_d; }
 std::vector<double> System::getContactForces() { return f_contact_d; }
 
-// System.cu:1699-1737: one CSV row per rigid body.
+// The rigid-body rows of the System CSV file: System.cu:1699-1737 writes
+// them and :1856-1910 reads them back.  Header: the body count followed by
+// the (here always zero) counts of beams, plates and 2-D bodies.  One row per
+// body: index, fixed flag, position, the unit orientation quaternion
+// (1, 0, 0, 0), velocity, then the shape code with its geometry -- 0 and the
+// radius for a sphere, 2 and the three half-extents for a box.  Every field
+// is followed by ", "; numbers use the stream's default formatting (six
+// significant digits), as the reference's files do.
+namespace {
+
+struct BodyRow {
+  int index = 0, fixed = 0, shape = 0;
+  double p[3] = {0, 0, 0}, v[3] = {0, 0, 0}, geom[3] = {0, 0, 0};
+};
+
+void write_body_row(std::ostream& os, const BodyRow& r) {
+  os << r.index << ", " << r.fixed << ", " << r.p[0] << ", " << r.p[1] << ", " << r.p[2]
+     << ", 1, 0, 0, 0, " << r.v[0] << ", " << r.v[1] << ", " << r.v[2] << ", " << r.shape << ", ";
+  const int ng = r.shape == 0 ? 1 : 3;
+  for (int k = 0; k < ng; ++k) os << r.geom[k] << ", ";
+  os << "\n";
+}
+
+// The comma-separated fields of one line as numbers (empty fields skipped).
+std::vector<double> csv_numbers(const std::string& line) {
+  std::vector<double> out;
+  size_t i = 0;
+  while (i < line.size()) {
+    size_t j = line.find(',', i);
+    if (j == std::string::npos) j = line.size();
+    const std::string f = line.substr(i, j - i);
+    const char* c = f.c_str();
+    char* e = nullptr;
+    const double x = strtod(c, &e);
+    if (e != c) out.push_back(x);
+    i = j + 1;
+  }
+  return out;
+}
+
+bool parse_body_row(const std::string& line, BodyRow* r) {
+  const std::vector<double> f = csv_numbers(line);
+  // index, fixed, p (3), quaternion (4), v (3), shape, geometry (1 or 3)
+  if (f.size() < 14) return false;
+  r->index = (int)f[0];
+  r->fixed = (int)f[1];
+  for (int k = 0; k < 3; ++k) {
+    r->p[k] = f[2 + k];
+    r->v[k] = f[9 + k];
+  }
+  r->shape = (int)f[12];
+  const size_t ng = r->shape == 0 ? 1 : 3;
+  if (f.size() < 13 + ng) return false;
+  for (int k = 0; k < 3; ++k) r->geom[k] = (size_t)k < ng ? f[13 + k] : 0.0;
+  return true;
+}
+
+}  // namespace
+
 int System::exportSystem(std::string filename) {
   std::ofstream fs(filename.c_str());
   if (!fs) return DV_ERR_ARG;
@@ -215,93 +275,103 @@ int System::exportSystem(std::string filename) {
   f_contact_h = f_contact_d;
   fs << bodies.size() << ", " << 0 << ", " << 0 << ", " << 0 << ", " << std::endl;
   for (size_t i = 0; i < bodies.size(); ++i) {
-    double3 g = bodies[i]->contactGeometry;
-    fs << i << ", " << bodies[i]->isFixed() << ", " << p_h[3 * i] << ", " << p_h[3 * i + 1]
-       << ", " << p_h[3 * i + 2] << ", " << "1, " << "0, " << "0, " << "0, " << v_h[3 * i]
-       << ", " << v_h[3 * i + 1] << ", " << v_h[3 * i + 2] << ", ";
-    if (g.y == 0) fs << "0, " << g.x << ", ";
-    else fs << "2, " << g.x << ", " << g.y << ", " << g.z << ", ";
-    fs << "\n";
+    BodyRow r;
+    r.index = (int)i;
+    r.fixed = bodies[i]->isFixed() ? 1 : 0;
+    const double3 g = bodies[i]->contactGeometry;
+    r.shape = g.y == 0 ? 0 : 2;
+    r.geom[0] = g.x;
+    r.geom[1] = g.y;
+    r.geom[2] = g.z;
+    for (int k = 0; k < 3; ++k) {
+      r.p[k] = p_h[3 * i + k];
+      r.v[k] = v_h[3 * i + k];
+    }
+    write_body_row(fs, r);
   }
   return 0;
 }
 
-// System.cu:1856-1910: reads the rows written by exportSystem; spheres get
-// the reference's hard-coded density 2600 (and its value of pi).
+// Adds the file's bodies.  A sphere gets the mass the reference's importer
+// gives every sphere (density 2600 and its value of pi,
+// 2600 * 4 * 3.14159 * r^3 / 3 with r^3 = pow(r, 3)); a box gets mass 1.
 int System::importSystem(std::string filename) {
   std::ifstream in(filename.c_str());
   if (!in) return DV_ERR_ARG;
   std::string line;
   if (!std::getline(in, line)) return DV_ERR_ARG;
-  for (char& c : line)
-    if (c == ',') c = ' ';
-  int numBodies = 0, numBeams = 0, numPlates = 0, numBodies2D = 0;
-  std::stringstream ss1(line);
-  ss1 >> numBodies >> numBeams >> numPlates >> numBodies2D;
-  for (int i = 0; i < numBodies; ++i) {
-    if (!std::getline(in, line)) return DV_ERR_ARG;
-    for (char& c : line)
-      if (c == ',') c = ' ';
-    std::stringstream ss(line);
-    int index = 0, isFixed = 0, shape = 0;
-    double blah;
-    double3 pos, vel, geometry = make_double3(0, 0, 0);
-    ss >> index >> isFixed >> pos.x >> pos.y >> pos.z >> blah >> blah >> blah >> blah >> vel.x >>
-        vel.y >> vel.z >> shape;
-    if (shape == 0) {
-      ss >> geometry.x;
-    } else {
-      ss >> geometry.x >> geometry.y >> geometry.z;
-    }
-    Body* b = new Body(pos);
-    b->setBodyFixed(isFixed != 0);
-    b->setGeometry(geometry);
-    b->setVelocity(vel);
-    if (shape == 0) b->setMass(2600 * 4.0 * 3.14159 * geometry.x * geometry.x * geometry.x / 3.0);
-    else b->setMass(1.0);
+  const std::vector<double> head = csv_numbers(line);
+  if (head.empty()) return DV_ERR_ARG;
+  const int count = (int)head[0];
+  for (int i = 0; i < count; ++i) {
+    BodyRow r;
+    if (!std::getline(in, line) || !parse_body_row(line, &r)) return DV_ERR_ARG;
+    Body* b = new Body(make_double3(r.p[0], r.p[1], r.p[2]));
+    b->setBodyFixed(r.fixed != 0);
+    b->setGeometry(make_double3(r.geom[0], r.geom[1], r.geom[2]));
+    b->setVelocity(make_double3(r.v[0], r.v[1], r.v[2]));
+    b->setMass(r.shape == 0 ? 2600 * 4.0 * 3.14159 * std::pow(r.geom[0], 3.0) / 3.0 : 1.0);
     add(b);
   }
   return 0;
 }
 
-int System::calculateContactForcePerCollision() { return 0; }
+// System.cu:1259-1295: the normal and friction force of every contact of the
+// last step, gamma_n n / h and (gamma_u u + gamma_v v) / h, into
+// normalForcePerCollision_h and frictionForcePerCollision_h.
+int System::calculateContactForcePerCollision() {
+  normalForcePerCollision_h.clear();
+  frictionForcePerCollision_h.clear();
+  if (!scene) return DV_ERR_ARG;
+  int32_t nc = 0, np = 0;
+  int rc = dv_get_num_contacts(scene, &nc, &np);
+  if (rc != DV_OK) return rc;
+  std::vector<double> fn(3 * (size_t)nc), ff(3 * (size_t)nc);
+  if (nc && (rc = dv_contact_forces_per_collision(scene, fn.data(), ff.data())) != DV_OK) return rc;
+  normalForcePerCollision_h.resize(nc);
+  frictionForcePerCollision_h.resize(nc);
+  for (int i = 0; i < nc; ++i) {
+    normalForcePerCollision_h[i] = make_double3(fn[3 * i], fn[3 * i + 1], fn[3 * i + 2]);
+    frictionForcePerCollision_h[i] = make_double3(ff[3 * i], ff[3 * i + 1], ff[3 * i + 2]);
+  }
+  return 0;
+}
 
 // System.cu:1672-1697
 int System::outputContactForcePerCollision(std::string filename) {
   std::ofstream fs(filename.c_str());
   if (!fs || !scene) return DV_ERR_ARG;
-  int32_t nc = 0, np = 0;
-  dv_get_num_contacts(scene, &nc, &np);
+  int rc = calculateContactForcePerCollision();
+  if (rc != 0) return rc;
+  const int nc = (int)normalForcePerCollision_h.size();
   std::vector<uint32_t> a(nc), b(nc);
-  std::vector<double> loc(3 * (size_t)nc), fn(3 * (size_t)nc), ff(3 * (size_t)nc);
-  if (nc) {
-    dv_get_contacts(scene, a.data(), b.data(), nullptr, loc.data());
-    dv_contact_forces_per_collision(scene, fn.data(), ff.data());
-  }
+  std::vector<double> loc(3 * (size_t)nc);
+  if (nc) dv_get_contacts(scene, a.data(), b.data(), nullptr, loc.data());
   fs << nc << ", " << bodies.size() << ", " << 0 << ", " << 0 << ", " << 0 << ", " << std::endl;
-  for (int i = 0; i < nc; ++i)
+  for (int i = 0; i < nc; ++i) {
+    const double3 fn = normalForcePerCollision_h[i], ff = frictionForcePerCollision_h[i];
     fs << i << ", " << a[i] << ", " << b[i] << ", " << loc[3 * i] << ", " << loc[3 * i + 1] << ", "
-       << loc[3 * i + 2] << ", " << fn[3 * i] << ", " << fn[3 * i + 1] << ", " << fn[3 * i + 2]
-       << ", " << ff[3 * i] << ", " << ff[3 * i + 1] << ", " << ff[3 * i + 2] << ", \n";
+       << loc[3 * i + 2] << ", " << fn.x << ", " << fn.y << ", " << fn.z << ", " << ff.x << ", "
+       << ff.y << ", " << ff.z << ", \n";
+  }
   return 0;
 }
 
 // System.cu:1297-1319: the contact forces of the last step on stdout.
 int System::outputContactForcePerCollision() {
   if (!scene) return DV_ERR_ARG;
-  int32_t nc = 0, np = 0;
-  dv_get_num_contacts(scene, &nc, &np);
+  int rc = calculateContactForcePerCollision();
+  if (rc != 0) return rc;
+  const int nc = (int)normalForcePerCollision_h.size();
   std::vector<uint32_t> a(nc), b(nc);
-  std::vector<double> loc(3 * (size_t)nc), fn(3 * (size_t)nc), ff(3 * (size_t)nc);
-  if (nc) {
-    dv_get_contacts(scene, a.data(), b.data(), nullptr, loc.data());
-    dv_contact_forces_per_collision(scene, fn.data(), ff.data());
-  }
+  std::vector<double> loc(3 * (size_t)nc);
+  if (nc) dv_get_contacts(scene, a.data(), b.data(), nullptr, loc.data());
   for (int i = 0; i < nc; ++i) {
+    const double3 fn = normalForcePerCollision_h[i], ff = frictionForcePerCollision_h[i];
     printf("Collision #%d: Body %u to %u\n", i, a[i], b[i]);
     printf("  Collision location: (%f, %f, %f)\n", loc[3 * i], loc[3 * i + 1], loc[3 * i + 2]);
-    printf("  Collision normal:   (%f, %f, %f)\n", fn[3 * i], fn[3 * i + 1], fn[3 * i + 2]);
-    printf("  Collision friction: (%f, %f, %f)\n\n", ff[3 * i], ff[3 * i + 1], ff[3 * i + 2]);
+    printf("  Collision normal:   (%f, %f, %f)\n", fn.x, fn.y, fn.z);
+    printf("  Collision friction: (%f, %f, %f)\n\n", ff.x, ff.y, ff.z);
   }
   return 0;
 }

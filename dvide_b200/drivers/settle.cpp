@@ -8,7 +8,10 @@
 // the fixed boxes, and the four CCP violations.  With pinnedSpheres = n > 0
 // the x and y DOFs of the first n spheres are held by bilateral constraints
 // (System::addBilateralConstraintDOF, as the reference drivers pin DOFs) and
-// the largest drift of those DOFs is printed at the end.
+// the largest drift of those DOFs is printed at the end.  The bodies as built
+// (settle_initial.txt) and the final positions and velocities
+// (settle_final_full.txt) are written at full precision, so that the run can
+// be replayed and compared elsewhere.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -74,6 +77,13 @@ int main(int argc, char** argv) {
     pin0.push_back(b->getPosition().x);
     pin0.push_back(b->getPosition().y);
   }
+  FILE* fi = fopen("settle_initial.txt", "w");
+  for (Body* b : sys->bodies) {
+    const double3 p = b->getPosition(), v = b->getVelocity(), g = b->getGeometry();
+    fprintf(fi, "%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %d\n", p.x, p.y, p.z,
+            v.x, v.y, v.z, b->getMass(), g.x, g.y, g.z, b->isFixed() ? 1 : 0);
+  }
+  fclose(fi);
   int rc = sys->initializeSystem();
   if (rc != 0) {
     fprintf(stderr, "initializeSystem failed: %s\n", dv_status_string(rc));
@@ -112,6 +122,14 @@ int main(int argc, char** argv) {
                  ida[i] < sys->collisionDetector->collisionIdentifierB_d[i];
   printf("contact handles: %s\n", handles_ok ? "ok" : "mismatch");
   sys->exportSystem("settle_final.csv");
+  {
+    std::vector<double> p = sys->p_d, v = sys->v_d;
+    FILE* ff = fopen("settle_final_full.txt", "w");
+    for (size_t i = 0; i < sys->bodies.size(); ++i)
+      fprintf(ff, "%.17g %.17g %.17g %.17g %.17g %.17g\n", p[3 * i], p[3 * i + 1], p[3 * i + 2],
+              v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    fclose(ff);
+  }
   sys->exportMatrices(".");
   delete sys;
   return 0;

@@ -67,6 +67,9 @@ class System {
   double objectiveCCP;
   DeviceArray p_d, v_d, f_contact_d, gamma_d;
   std::vector<double> p_h, v_h, f_contact_h, gamma_h;
+  // per-contact forces of the last step (System::normalForcePerCollision_d /
+  // frictionForcePerCollision_d, filled by calculateContactForcePerCollision)
+  std::vector<double3> normalForcePerCollision_h, frictionForcePerCollision_h;
 
   double getCurrentTime() const { return time; }
   double getTimeStep() const { return h; }

@@ -1,10 +1,15 @@
 """The C++ layer (include/dvide/System.h) runs a driver written like the
-reference's models/test_compaction.cu and gives the oracle's trajectory."""
+reference's models/test_compaction.cu and gives the oracle's trajectory: the
+driver writes the bodies it built at full precision, the oracle replays the
+same scene, and every step's contact count and iteration count and the final
+positions and velocities must be identical."""
 import os
 import subprocess
 
 import numpy as np
 import pytest
+
+from dvide_b200 import scenes
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(ROOT, "dvide_b200", "drivers", "settle")
@@ -12,7 +17,25 @@ DRIVER = os.path.join(ROOT, "dvide_b200", "drivers", "settle")
 pytestmark = pytest.mark.gpu
 
 
-def test_settle_driver_runs(tmp_path):
+def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start):
+    """The driver's scene (settle_initial.txt) with the driver's settings
+    (System defaults: mu 0.25, envelope 1e-3; h 1e-3, gravity -z) in the oracle."""
+    b = np.loadtxt(tmp_path / "settle_initial.txt")
+    params = scenes.default_params(h=1e-3, gravity=(0.0, 0.0, -9.81), tolerance=tolerance,
+                                   max_iterations=max_iterations, warm_start=warm_start)
+    sc = scenes.Scene(b[:, 0:3].copy(), b[:, 3:6].copy(), b[:, 6].copy(), b[:, 7:10].copy(),
+                      b[:, 10].astype(np.int32), np.full(len(b), -1, dtype=np.int32), params,
+                      "settle_driver")
+    o = oracle_mod.OracleScene(sc)
+    per_step = []
+    for _ in range(steps):
+        o.step(1)
+        st = o.stats()
+        per_step.append((st["num_contacts"], st["iterations"]))
+    return o, per_step
+
+
+def test_settle_driver_runs(tmp_path, oracle_mod):
     out = subprocess.run([DRIVER, "120", "1", "1e-4", "1000"], cwd=tmp_path, capture_output=True,
                          text=True, timeout=300)
     assert out.returncode == 0, out.stderr
@@ -24,6 +47,13 @@ def test_settle_driver_runs(tmp_path):
     rows = open(tmp_path / "settle_final.csv").read().splitlines()
     assert rows[0].startswith("1005,") and len(rows) == 1006
     assert "contact handles: ok" in out.stdout
+    # the oracle's trajectory, step by step and at the end, bit for bit
+    o, per_step = _replay(oracle_mod, tmp_path, 120, 1e-4, 1000, 1)
+    driver = [(int(l.split(",")[1]), int(l.split(",")[2])) for l in lines]
+    assert driver == per_step
+    final = np.loadtxt(tmp_path / "settle_final_full.txt")
+    p, v = o.state()
+    assert np.array_equal(final[:, 0:3], p) and np.array_equal(final[:, 3:6], v)
 
 
 def test_unsupported_solver_type_reports(tmp_path):
