@@ -269,3 +269,32 @@ def test_column_sample_free_running(native, oracle_mod):
                                  d["radius"][order].astype(np.float64), float(d["wall_height"]))
     st = _free_running(native, oracle_mod, sc, 6)
     assert st["num_contacts"] > 15000
+
+
+def test_column_full_scale_contacts_and_one_step(native, oracle_mod):
+    """The whole settled 200,000-sphere column that the benchmark times
+    (~741,000 contacts): collision detection's contact list (ids, normal and
+    gap, location) and tangent frames bit-identical to the oracle's
+    (CollisionDetector.cu:547-665), then one full step from the same state and
+    warm start (the 500-iteration APGD solve and the update, System.cu:544-583):
+    gamma, v, p, iterations, backtracks and residual identical."""
+    sc = workloads.column_settled()
+    g, o = _pair(native, oracle_mod, sc)
+    g.collide()
+    o.collide()
+    nc = _compare_contacts(g, o)
+    assert nc > 700000
+    assert np.array_equal(g.frames(), o.frames())
+    assert g.num_contacts()[1] == o.stats()["num_possible"]
+    g.step(1)
+    o.step(1)
+    so, sg = o.stats(), g.stats()
+    assert sg["num_contacts"] == so["num_contacts"]
+    for key in ("iterations", "backtracks", "residual", "objective"):
+        assert sg[key] == so[key], key
+    gg, go = g.gamma(), o.gamma()
+    pg, vg = g.state()
+    po, vo = o.state()
+    assert _rel(gg, go) <= REL_TOL and _rel(vg, vo) <= REL_TOL
+    assert np.array_equal(gg, go)
+    assert np.array_equal(vg, vo) and np.array_equal(pg, po)
