@@ -49,6 +49,18 @@
 #include <omp.h>
 #endif
 
+// The bin sort of the collision pass runs on Thrust's OpenMP backend where
+// the CUDA toolkit's headers are on the include path (the reference sorts
+// with Thrust: CollisionDetector.cu:583-590), else with std::sort; the sorted
+// order is the same either way.
+#if defined(_OPENMP) && defined(__has_include)
+#if __has_include(<thrust/sort.h>)
+#define DV_ORACLE_THRUST_OMP 1
+#include <thrust/sort.h>
+#include <thrust/system/omp/execution_policy.h>
+#endif
+#endif
+
 namespace {
 
 struct V3 {
@@ -404,7 +416,21 @@ void collide(Scene& S) {
     ckey[i] = cx[i] + D0 * (cy[i] + D1 * (int64_t)cz[i]);
     cells.push_back(std::make_pair(ckey[i], i));
   }
+#ifdef DV_ORACLE_THRUST_OMP
+  {
+    // (cell, body) order: a stable sort by cell of bodies in ascending id
+    std::vector<int64_t> keys(cells.size());
+    std::vector<int> ids(cells.size());
+    for (size_t k = 0; k < cells.size(); ++k) {
+      keys[k] = cells[k].first;
+      ids[k] = cells[k].second;
+    }
+    thrust::stable_sort_by_key(thrust::omp::par, keys.data(), keys.data() + keys.size(), ids.data());
+    for (size_t k = 0; k < cells.size(); ++k) cells[k] = std::make_pair(keys[k], ids[k]);
+  }
+#else
   std::sort(cells.begin(), cells.end());
+#endif
 
   std::vector<std::vector<ContactOut>> per(nb);
   std::vector<int> ncand(nb, 0);

@@ -15,8 +15,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "liboracle.so")
 
+CUDA_INCLUDE = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
 CFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
-          "-fPIC", "-shared", "-std=c++17", "-Wall"]
+          "-fPIC", "-shared", "-std=c++17", "-Wall",
+          # Thrust's OpenMP backend for the collision pass's bin sort (header-only)
+          "-DTHRUST_DEVICE_SYSTEM=THRUST_DEVICE_SYSTEM_OMP", "-I", CUDA_INCLUDE]
 
 
 def build(force=False):
