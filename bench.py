@@ -57,6 +57,14 @@ def solve_bytes(nc, nb, sweeps, backtracks):
     return sweeps * (440 * nc + 120 * nb) + backtracks * bN + 2 * bN + (136 * nc + 96 * nb)
 
 
+# The same count for the kernel's own sequence: ONE Schur product per APGD
+# iteration (N y is formed from the stored products of the last two iterates),
+# i.e. 440 nc + 120 nb less one product's 136 nc + 60 nb.
+def solve_bytes_one_product(nc, nb, sweeps, backtracks):
+    bN = 136 * nc + 60 * nb
+    return sweeps * (304 * nc + 60 * nb) + backtracks * bN + 2 * bN + (136 * nc + 96 * nb)
+
+
 # DRAM bytes per algorithmic byte of the solve kernel, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum = 6.350 GB) on a 30-iteration
 # launch on this workload (11.415 GB algorithmic); the full launch is scaled by it.
@@ -130,17 +138,20 @@ def load_workload(name):
     return sc, desc
 
 
+# The reference's APGD as written (src/APGD.cu:164-361): four Schur products
+# per iteration, sequential host sums, COO entries in their literal order.
+LITERAL = dict(reduce_mode=1, spmv_mode=1, apgd_mode=1)
+
+
 def run_reference(args, sc, desc):
-    """The reference's algorithm on the host cores (oracle/), same state and config."""
+    """The reference's algorithm on the host cores (oracle/, its literal APGD
+    sequence), same state and config; the fused evaluation order the GPU uses,
+    timed beside it on one step, as a second number."""
     from oracle import oracle as O
     O.build()
     threads = os.cpu_count() or 1
-    o = O.OracleScene(sc, threads=threads)
+    o = O.OracleScene(sc, threads=threads, **LITERAL)
     budget = args.ref_budget_s
-    warm = 1 if args.warmup > 0 else 0
-    t0 = time.perf_counter()
-    o.step(warm)
-    t_warm = time.perf_counter() - t0
     contacts = 0
     done = 0
     t0 = time.perf_counter()
@@ -152,16 +163,42 @@ def run_reference(args, sc, desc):
             break
     dt = time.perf_counter() - t0
     value = contacts / dt
-    sample = (f"{done} of {args.steps} full time steps after {warm} warm-up step "
-              f"({t_warm:.1f} s), {threads} OpenMP threads, oracle port of APGD/System")
+    f = O.OracleScene(sc, threads=threads)
+    t1 = time.perf_counter()
+    f.step(1)
+    dtf = time.perf_counter() - t1
+    fused = f.stats()["num_contacts"] / dtf
+    at_tol = None
+    if args.workload == "column":
+        # the compacting column (every step at the tolerance), first steps
+        from dvide_b200 import workloads
+        c = O.OracleScene(workloads.column_compacting(), threads=threads, **LITERAL)
+        ct, cc, cn, its = 0.0, 0, 0, []
+        while cn < args.ref_tol_steps:
+            t2 = time.perf_counter()
+            c.step(1)
+            ct += time.perf_counter() - t2
+            cc += c.stats()["num_contacts"]
+            its.append(c.stats()["iterations"])
+            cn += 1
+        at_tol = {"value": cc / ct, "unit": "contact-steps/s", "cores": threads,
+                  "sample": f"first {cn} of the compacting column's steps ({ct:.1f} s), literal "
+                            f"sequence", "iterations": its}
+    sample = (f"first {done} of {args.steps} full time steps from the benchmark's initial state "
+              f"({dt:.1f} s), {threads} OpenMP threads, the reference's literal APGD sequence "
+              f"(four Schur products per iteration, sequential sums)")
     return {"metric": "contact-steps/s", "value": value, "unit": "contact-steps/s",
-            "impl": "reference", "n_gpus": 0, "steps": done, "warmup": warm,
+            "impl": "reference", "n_gpus": 0, "steps": done, "warmup": 0,
             "ms_per_step": 1e3 * dt / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc},
             "cpu_baseline": {"value": value, "unit": "contact-steps/s", "cores": threads,
                              "kind": "port", "sample": sample},
+            "column_at_tolerance": at_tol,
+            "fused_order_port": {"value": fused, "unit": "contact-steps/s", "cores": threads,
+                                 "sample": f"first step, {dtf:.1f} s, one Schur product per "
+                                           f"iteration (the GPU's evaluation order)"},
             "e2e": {"value": value, "unit": "contact-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -170,7 +207,7 @@ def cpu_baseline_sample(sc, budget_s):
     from oracle import oracle as O
     O.build()
     threads = os.cpu_count() or 1
-    o = O.OracleScene(sc, threads=threads)
+    o = O.OracleScene(sc, threads=threads, **LITERAL)
     t0 = time.perf_counter()
     contacts = 0
     n = 0
@@ -183,7 +220,13 @@ def cpu_baseline_sample(sc, budget_s):
     dt = time.perf_counter() - t0
     return {"value": contacts / dt, "unit": "contact-steps/s", "cores": threads, "kind": "port",
             "sample": f"first {n} time step(s) from the same initial state and stored warm "
-                      f"start, {dt:.1f} s"}
+                      f"start, {dt:.1f} s, the reference's literal APGD sequence"}
+
+
+def _rel(a, b):
+    n = float(np.linalg.norm(b))
+    d = float(np.linalg.norm(a - b))
+    return d / n if n > 0 else d
 
 
 def run_mixed_error(N, stream, steps=500, every=10):
@@ -194,21 +237,18 @@ def run_mixed_error(N, stream, steps=500, every=10):
     of gamma and v, the largest velocity difference, and both residuals.  At
     the benchmark tolerance 1e-4 the two solves stop at different iterates, so
     the difference includes the solver tolerance; at 1e-6 it is the precision.
+    The settling box is statically indeterminate once it rests (gamma is not
+    unique there); `determinate` holds the scenes whose FP64 gamma is pinned.
     The FP64 path gives the oracle's results bit for bit
     (tests/test_gpu_parity.py)."""
     from dvide_b200 import scenes
 
-    def rel(a, b):
-        n = float(np.linalg.norm(b))
-        d = float(np.linalg.norm(a - b))
-        return d / n if n > 0 else d
-
     out = {"workload": (f"settling_box 1000 spheres, every {every}th of {steps} steps "
                         f"(teacher-forced from the FP64 run), h 1e-3, maxIter 1000")}
-    for tol in (1e-4, 1e-6):
+    for tol, refine in ((1e-4, 0), (1e-6, 0), (1e-6, 2000)):
         sc = scenes.settling_box(tolerance=tol)
         f = N.NativeScene.from_scene(sc)
-        m = N.NativeScene.from_scene(sc, precision=N.DV_PREC_MIXED)
+        m = N.NativeScene.from_scene(sc, precision=N.DV_PREC_MIXED, refine_iterations=refine)
         f.set_stream(stream.cuda_stream)
         m.set_stream(stream.cuda_stream)
         rows = []
@@ -225,14 +265,16 @@ def run_mixed_error(N, stream, steps=500, every=10):
             if sf["num_contacts"] == 0:
                 continue
             vf, vm = f.state()[1], m.state()[1]
-            rows.append((rel(m.gamma(), f.gamma()), rel(vm, vf), float(np.abs(vm - vf).max()),
-                         sf["residual"], sm["residual"], sf["iterations"], sm["iterations"]))
+            rows.append((_rel(m.gamma(), f.gamma()), _rel(vm, vf), float(np.abs(vm - vf).max()),
+                         sf["residual"], sm["residual"], sf["iterations"], sm["iterations"],
+                         sm["refine_iterations"]))
         f.close()
         m.close()
         if not rows:
             continue
         a = np.array(rows)
-        out[f"tolerance_{tol:g}"] = {
+        key = f"tolerance_{tol:g}" + ("_fp64_refinement" if refine else "")
+        out[key] = {
             "steps_compared": len(rows),
             "gamma_rel_err": {"max": float(a[:, 0].max()), "median": float(np.median(a[:, 0]))},
             "v_rel_err": {"max": float(a[:, 1].max()), "median": float(np.median(a[:, 1]))},
@@ -241,7 +283,118 @@ def run_mixed_error(N, stream, steps=500, every=10):
             "residual_mixed_max": float(a[:, 4].max()),
             "iterations_mean": {"fp64": float(a[:, 5].mean()), "mixed": float(a[:, 6].mean())},
         }
+        if refine:
+            out[key]["fp64_refinement_iterations_mean"] = float(a[:, 7].mean())
+    out["determinate"] = run_mixed_determinate(N, stream)
     return out
+
+
+def run_mixed_determinate(N, stream, tol=1e-8, refine=2000):
+    """Mixed precision on scenes whose FP64 gamma is pinned at tolerance 1e-8
+    (a warm- and a cold-started FP64 solve of the same step agree to < 1e-5;
+    tests/test_oracle_indeterminate.py): a ball sliding on the ground, a
+    5-sphere stack dropping and sliding, the 40-sphere cluster.  Teacher-forced
+    from the FP64 run; the mixed solve with FP64 refinement (up to `refine`
+    FP64 iterations from the FP32 best iterate once the FP32 phase stalls) and
+    without it.  Cost: device time per step of each."""
+    from dvide_b200 import scenes
+
+    def scene(which):
+        if which == "ball_sliding":
+            sc = scenes.ball_on_ground(h=1e-2, tolerance=tol, warm_start=1)
+            sc.vel[1] = (0.2, 0.0, 0.1)
+            return sc, 5
+        if which == "stack5_moving":
+            sc = scenes.sphere_stack(5, tolerance=tol)
+            sc.vel[1:] = (0.1, 0.0, -0.05)
+            return sc, 20
+        return scenes.random_cluster(0, n=40, max_iterations=5000, tolerance=tol), 8
+
+    out = {"tolerance": tol, "bound": "gamma and v within 1e-5 relative of FP64"}
+    for which in ("ball_sliding", "stack5_moving", "cluster40"):
+        sc, steps = scene(which)
+        f = N.NativeScene.from_scene(sc)
+        forms = {"mixed": N.NativeScene.from_scene(sc, precision=N.DV_PREC_MIXED),
+                 "mixed_refined": N.NativeScene.from_scene(sc, precision=N.DV_PREC_MIXED,
+                                                           refine_iterations=refine)}
+        for g in [f, *forms.values()]:
+            g.set_stream(stream.cuda_stream)
+        acc = {k: {"g": 0.0, "v": 0.0, "res": 0.0, "it": [], "rit": [], "ms": []} for k in forms}
+        fms = []
+        for _ in range(steps):
+            p, v = f.state()
+            gam = f.gamma()
+            for g in forms.values():
+                g.set_state(p, v)
+                g.set_gamma(gam)
+            f.step(1)
+            sf = f.stats()
+            if sf["num_contacts"] == 0:
+                continue
+            fms.append(sf["elapsed_ms"])
+            gf, vf = f.gamma(), f.state()[1]
+            for k, g in forms.items():
+                g.step(1)
+                sg = g.stats()
+                a = acc[k]
+                a["g"] = max(a["g"], _rel(g.gamma(), gf))
+                a["v"] = max(a["v"], _rel(g.state()[1], vf))
+                a["res"] = max(a["res"], sg["residual"])
+                a["it"].append(sg["iterations"] - sg["refine_iterations"])
+                a["rit"].append(sg["refine_iterations"])
+                a["ms"].append(sg["elapsed_ms"])
+        row = {"steps": len(fms), "fp64_ms_per_step": float(np.mean(fms)) if fms else None}
+        for k, a in acc.items():
+            row[k] = {"gamma_rel_err_max": a["g"], "v_rel_err_max": a["v"],
+                      "residual_max": a["res"],
+                      "fp32_iterations_mean": float(np.mean(a["it"])) if a["it"] else 0.0,
+                      "fp64_refinement_iterations_mean": float(np.mean(a["rit"])) if a["rit"] else 0.0,
+                      "ms_per_step": float(np.mean(a["ms"])) if a["ms"] else None}
+        out[which] = row
+        for g in [f, *forms.values()]:
+            g.close()
+    return out
+
+
+def run_column_at_tolerance(args, N, torch, stream):
+    """The 200,000-sphere column while it compacts (workloads.column_compacting:
+    the state from which the next 10 steps all reach the APGD tolerance 1e-4
+    within the 500-iteration cap, ~7.29e5 contacts), stepped through those 10
+    steps with the benchmark's own settings: contact-steps/s at residual 1e-4,
+    with the iterations each step needed.  The kernels are warm (the headline
+    ran first)."""
+    from dvide_b200 import workloads
+    sc = workloads.column_compacting()
+    g = N.NativeScene.from_scene(sc)
+    g.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.step(args.tol_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    hist = g.history(clear=True)
+    g.close()
+    contacts = sum(h["num_contacts"] for h in hist)
+    tol = sc.params["tolerance"]
+    conv = [h for h in hist if h["residual"] < tol]
+    conv_ms = sum(h["elapsed_ms"] for h in conv)
+    return {
+        "converged_steps_only": ({"value": sum(h["num_contacts"] for h in conv) / (conv_ms / 1e3),
+                                  "unit": "contact-steps/s", "steps": len(conv)}
+                                 if conv and len(conv) < len(hist) else None),
+        "workload": (f"column_compacting: the 200000-sphere column while it compacts, "
+                     f"{args.tol_steps} steps from the saved state, tol {tol:g} maxIter "
+                     f"{sc.params['max_iterations']} warm start, FP64"),
+        "value": contacts / (ms / 1e3), "unit": "contact-steps/s", "ms_per_step": ms / len(hist),
+        "contacts_per_step": contacts / len(hist),
+        "iterations": [h["iterations"] for h in hist],
+        "backtracks": [h["backtracks"] for h in hist],
+        "residual_max": max(h["residual"] for h in hist),
+        "steps_at_tolerance": f"{sum(1 for h in hist if h['residual'] < tol)}/{len(hist)}",
+    }
 
 
 def run_batched(args, N, torch, stream):
@@ -327,18 +480,35 @@ def run_served(args, N, stream):
     gaps = rng.exponential(1.0 / args.serve_rate, size=n_req)
     arrive = np.cumsum(gaps) - gaps[0]
     sizes = np.exp(rng.uniform(np.log(500), np.log(50000), size=n_req)).astype(np.int64)
-    reqs = [scenes.lattice_container(rng, int(n), name=f"req{i}") for i, n in enumerate(sizes)]
+    # the request scenes are generated in order by a producer thread, a bounded
+    # number ahead of their arrival (a long stream does not fit in host memory
+    # at once, and generating it in the serving loop would delay the rounds)
+    import queue
+    import threading
+    ahead = queue.Queue(maxsize=min(n_req, 512))
+
+    def produce():
+        for j, n in enumerate(sizes):
+            ahead.put(scenes.lattice_container(rng, int(n), name=f"req{j}"))
+
+    threading.Thread(target=produce, daemon=True).start()
+    while ahead.qsize() < min(n_req, 512):
+        time.sleep(0.01)
     srv = N.NativeServer(precision=N.DV_PREC_MIXED, hbm_budget_bytes=150e9,
                          steps_per_round=args.serve_round, keep_states=False)
     srv.set_stream(stream.cuda_stream)
+    sampler = ClockSampler(torch_device_index())
+    sampler.start()
     t0 = time.perf_counter()
     i = 0
     results = []
     busy = False
+    trace = []  # (seconds, requests waiting, requests resident, bytes resident) after each round
+    next_mark = 0.0
     while i < n_req or busy:
         now = time.perf_counter() - t0
         while i < n_req and arrive[i] <= now:
-            srv.submit(reqs[i], args.serve_steps)
+            srv.submit(ahead.get(), args.serve_steps)
             i += 1
         if not busy and i < n_req and arrive[i] > now:
             time.sleep(min(arrive[i] - now, 0.01))
@@ -346,7 +516,13 @@ def run_served(args, N, stream):
             continue
         busy = srv.round()
         results += srv.poll()
+        if now >= next_mark:
+            st = srv.stats()
+            trace.append((round(now, 2), int(st["pending"]), int(st["active"]),
+                          float(st["bytes_in_use"])))
+            next_mark = now + args.serve_trace_s
     wall = time.perf_counter() - t0
+    clocks = sampler.stop()
     results += srv.poll()
     st = srv.stats()
     srv.close()
@@ -354,12 +530,21 @@ def run_served(args, N, stream):
     step_p50 = np.array([r["step_ms_p50"] for r in results])
     step_p99 = np.array([r["step_ms_p99"] for r in results])
     contact_steps = st["contact_steps"]
-    # plain FP64 one request at a time on a stratified sample
+    # plain FP64 one request at a time on a stratified sample (rebuilt from the
+    # same generator: the requests were handed over)
+    rng2 = np.random.default_rng(11)
+    rng2.exponential(1.0 / args.serve_rate, size=n_req)
+    rng2.uniform(np.log(500), np.log(50000), size=n_req)
     order = np.argsort(sizes)
-    pick = order[::max(1, n_req // args.plain_sample)]
+    pick = set(order[::max(1, n_req // args.plain_sample)].tolist())
+    sample_reqs = {}
+    for j, n in enumerate(sizes):
+        sc_j = scenes.lattice_container(rng2, int(n), name=f"req{j}")
+        if j in pick:
+            sample_reqs[j] = sc_j
     p_cs, p_ms = 0.0, 0.0
-    for j in pick:
-        g = N.NativeScene.from_scene(reqs[j])
+    for j in sorted(pick):
+        g = N.NativeScene.from_scene(sample_reqs[j])
         g.set_stream(stream.cuda_stream)
         g.step(args.serve_steps)
         h = g.history(clear=True)
@@ -380,12 +565,138 @@ def run_served(args, N, stream):
                              "p99": float(np.percentile(step_p99, 99))},
         "completion_latency_s": {"p50": float(np.percentile(lat, 50)),
                                  "p99": float(np.percentile(lat, 99))},
+        "backlog": {"max_waiting": max(t[1] for t in trace) if trace else 0,
+                    "max_resident": max(t[2] for t in trace) if trace else 0,
+                    "peak_resident_gb": max(t[3] for t in trace) / 1e9 if trace else 0.0,
+                    "trace_s_waiting_resident_gb": [(t[0], t[1], t[2], round(t[3] / 1e9, 2))
+                                                    for t in trace]},
         "plain_fp64_one_at_a_time": {
             "value": plain, "unit": "contact-steps/s (device time)",
             "sample": f"{len(pick)} of {n_req} requests (every {max(1, n_req // args.plain_sample)}th "
                       f"by size)"},
         "speedup_vs_plain": (served / plain) if plain else None,
+        "clocks": clocks,
     }
+
+
+def torch_device_index():
+    import torch
+    return torch.cuda.current_device()
+
+
+def _oracle_timed_steps(O, threads, sc, states, mode):
+    """Steps the oracle once from each (p, v, gamma) in `states` (one step each,
+    teacher-forced), timing only the step; returns per-step (contacts,
+    seconds, iterations, residual)."""
+    o = O.OracleScene(sc, threads=threads, **mode)
+    rows = []
+    for p, v, gam in states:
+        o.set_state(p, v)
+        o.set_gamma(gam)
+        t = time.perf_counter()
+        o.step(1)
+        dt = time.perf_counter() - t
+        st = o.stats()
+        rows.append((st["num_contacts"], dt, st["iterations"], st["residual"]))
+    return rows
+
+
+def _cpu_row(rows, what):
+    c = np.array([r[0] for r in rows], dtype=np.float64)
+    t = np.array([r[1] for r in rows])
+    return {"sample": what, "contact_steps_per_s": float(c.sum() / t.sum()),
+            "steps": len(rows), "seconds": float(t.sum()),
+            "step_ms": {"mean": float(1e3 * t.mean()), "p50": float(1e3 * np.percentile(t, 50)),
+                        "p99": float(1e3 * np.percentile(t, 99))},
+            "iterations_mean": float(np.mean([r[2] for r in rows]))}
+
+
+def run_cpu_table(args):
+    """The CPU baseline of every configuration: the reference's literal APGD
+    sequence (oracle/, all host cores), with the GPU's evaluation order beside
+    it.  C0 runs all 500 steps from its initial state.  C1 and the samples of
+    C3 and C4 step the oracle once from states of the plain FP64 GPU
+    trajectory (bit-identical to the oracle's own), so that the CPU time goes
+    to the timed steps only."""
+    import torch
+    from oracle import oracle as O
+    from dvide_b200 import _native as N
+    from dvide_b200 import scenes, workloads
+    O.build()
+    threads = os.cpu_count() or 1
+    out = {"cores": threads, "modes": {"literal": "the reference's APGD as written (four Schur "
+                                                  "products per iteration, sequential sums)",
+                                       "fused": "the GPU's evaluation order (one product)"}}
+    try:
+        out["lscpu"] = subprocess.run(["lscpu"], capture_output=True, text=True).stdout.splitlines()[:20]
+    except Exception:
+        pass
+    modes = {"literal": LITERAL, "fused": {}}
+    # C0: every step from the start
+    sc = scenes.settling_box()
+    row = {}
+    for name, m in modes.items():
+        o = O.OracleScene(sc, threads=threads, **m)
+        rows = []
+        for _ in range(500):
+            t = time.perf_counter()
+            o.step(1)
+            dt = time.perf_counter() - t
+            st = o.stats()
+            rows.append((st["num_contacts"], dt, st["iterations"], st["residual"]))
+        row[name] = _cpu_row(rows, "all 500 steps")
+        row[name]["ccp_violation_last"] = o.ccp_violation().tolist()
+    out["C0"] = row
+    # C1: the headline's first step (the column at rest), and the compacting column
+    row = {}
+    for key, scc in (("settled", workloads.column_settled()),
+                     ("compacting", workloads.column_compacting())):
+        states = [(scc.pos, scc.vel, scc.gamma)]
+        row[key] = {name: _cpu_row(_oracle_timed_steps(O, threads, scc, states, m), "first step")
+                    for name, m in modes.items()}
+    out["C1"] = row
+
+    def gpu_states(sc, steps, keep):
+        g = N.NativeScene.from_scene(sc)
+        st = []
+        for k in range(steps):
+            if k in keep:
+                p, v = g.state()
+                st.append((p, v, g.gamma()))
+            g.step(1)
+        g.close()
+        return st
+
+    # C3: every 32nd of the 512 scenes by size, steps 61-100 (every 4th)
+    scs = scenes.batch_scenes(seed=3, count=512)
+    order = np.argsort([x.nb for x in scs])
+    rows = {k: [] for k in modes}
+    keep = set(range(60, 100, 4))
+    for i in order[::32]:
+        st = gpu_states(scs[i], 100, keep)
+        for name, m in modes.items():
+            rows[name] += _oracle_timed_steps(O, threads, scs[i], st, m)
+    out["C3"] = {k: _cpu_row(r, "16 of 512 scenes (every 32nd by size), one at a time, "
+                                "steps 61-100 (every 4th)") for k, r in rows.items()}
+    # C4: 16 requests of the served stream (stratified by size), 200 steps (every 10th)
+    rng = np.random.default_rng(11)
+    n_req = 12000
+    rng.exponential(1.0 / 200.0, size=n_req)
+    sizes = np.exp(rng.uniform(np.log(500), np.log(50000), size=n_req)).astype(np.int64)
+    pick = set(np.argsort(sizes)[::n_req // 16][:16].tolist())
+    rows = {k: [] for k in modes}
+    keep = set(range(0, 200, 10))
+    for j, n in enumerate(sizes):
+        scj = scenes.lattice_container(rng, int(n), name=f"req{j}")
+        if j not in pick:
+            continue
+        st = gpu_states(scj, 200, keep)
+        for name, m in modes.items():
+            rows[name] += _oracle_timed_steps(O, threads, scj, st, m)
+    out["C4"] = {k: _cpu_row(r, "16 of the 12,000 requests (stratified by size), one at a "
+                                "time, 200 steps (every 10th)") for k, r in rows.items()}
+    del torch
+    return out
 
 
 def main():
@@ -394,9 +705,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="print the CPU baseline of every configuration and exit")
     ap.add_argument("--workload", default="column", choices=["column", "settling"])
     ap.add_argument("--cpu-budget-s", type=float, default=30.0)
     ap.add_argument("--ref-budget-s", type=float, default=150.0)
+    ap.add_argument("--ref-tol-steps", type=int, default=2,
+                    help="steps of the compacting column the reference arm times")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-iterations", type=int, default=None,
                     help="override the APGD iteration cap (profiling runs only)")
@@ -406,6 +721,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="precision of the headline workload (fp64 is the plain drop-in)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-scenes line")
+    ap.add_argument("--no-column-at-tolerance", action="store_true",
+                    help="skip the headline state stepped to the APGD tolerance")
+    ap.add_argument("--tol-steps", type=int, default=10)
     ap.add_argument("--no-mixed-error", action="store_true",
                     help="skip the mixed-precision error report")
     ap.add_argument("--batch-scenes", type=int, default=512)
@@ -417,6 +735,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--serve-round", type=int, default=4)
+    ap.add_argument("--serve-trace-s", type=float, default=5.0,
+                    help="interval of the served line's backlog trace")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -424,6 +744,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.cpu_table:
+        print(json.dumps(run_cpu_table(args)), flush=True)
+        return 0
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -519,7 +842,13 @@ def main():
         its = np.array([h["iterations"] for h in hist])
         nposs = np.array([h["num_possible"] for h in hist])
         bytes_per_launch = np.array([solve_bytes(c, nb, s, b) for c, s, b in zip(ncs, sweeps, bts)])
+        own_bytes = np.array([solve_bytes_one_product(c, nb, s, b)
+                              for c, s, b in zip(ncs, sweeps, bts)])
         achieved = float(bytes_per_launch.sum() / (solve_ms.sum() / 1e3) / 1e9)
+        achieved_own = float(own_bytes.sum() / (solve_ms.sum() / 1e3) / 1e9)
+        traffic = float(bytes_per_launch.mean() * TRAFFIC_PER_ALGORITHMIC_BYTE)
+        dram_gbs = traffic / (solve_ms.mean() / 1e3) / 1e9
+        tol = sc.params["tolerance"]
         line = {
             "metric": "contact-steps/s", "value": contacts_all / t_all, "unit": "contact-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
@@ -529,7 +858,16 @@ def main():
             "data": "synthetic (seeded scene, see config)",
             "config": {"workload": desc, "contacts_per_step": float(ncs.mean()),
                        "bodies": nb, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (working set ~0.5 GB)"},
+                       "l2": "inputs larger than L2 (working set ~0.5 GB)",
+                       "apgd_tolerance": tol, "apgd_max_iterations": int(sc.params["max_iterations"])},
+            "convergence": {
+                "iterations_mean": float(its.mean()), "backtracks_mean": float(bts.mean()),
+                "residual_max": float(max(h["residual"] for h in hist)),
+                "residual_last": hist[-1]["residual"],
+                "steps_at_tolerance": f"{sum(1 for h in hist if h['residual'] < tol)}/{len(hist)}",
+                "note": ("at rest every step reaches the iteration cap and reports its best "
+                         "residual; column_at_tolerance is the same column while it compacts, "
+                         "where every timed step reaches the tolerance")},
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                            "p99": float(np.percentile(step_ms, 99))},
             "apgd": {"iterations_mean": float(its.mean()), "sweeps_mean": float(sweeps.mean()),
@@ -540,15 +878,21 @@ def main():
                      "phase_us_mean": {k: round(1e3 * v[0] / v[1], 2) for k, v in phases.items()}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": float(bytes_per_launch.mean() * TRAFFIC_PER_ALGORITHMIC_BYTE),
+                         "traffic": traffic,
                          "kernel": "k_step_solve (persistent APGD + update)",
                          "peak_kind": peak_kind,
-                         "bytes_per_launch": float(bytes_per_launch.mean())},
+                         "bytes_per_launch": float(bytes_per_launch.mean()),
+                         "bytes_model": "compulsory bytes, two Schur products per APGD iteration",
+                         "achieved_one_product_model": achieved_own,
+                         "frac_one_product_model": achieved_own / peak,
+                         "dram_gbs": dram_gbs, "dram_frac": dram_gbs / peak},
             "e2e": {"value": contacts_e2e_all / t_e2e_all, "unit": "contact-steps/s",
                     "h2d_bytes_per_step": 2 * 24 * nb, "d2h_bytes_per_step": 2 * 24 * nb},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
+        if world == 1 and not args.no_column_at_tolerance and args.workload == "column":
+            line["column_at_tolerance"] = run_column_at_tolerance(args, N, torch, stream)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(sc, args.cpu_budget_s)
         if world == 1 and not args.no_mixed_error:
