@@ -408,7 +408,7 @@ def run_batched(args, N, torch, stream):
     total_steps = args.batch_steps
     timed = max(1, min(args.batch_timed, total_steps - 1))
     pre = total_steps - timed
-    b = N.NativeBatch(scs, precision=N.DV_PREC_MIXED)
+    b = N.NativeBatch(scs, precision=N.DV_PREC_MIXED, refine_iterations=args.refine)
     b.set_stream(stream.cuda_stream)
     graph = b.set_graph(True) == 0
     b.step(pre)
@@ -449,7 +449,8 @@ def run_batched(args, N, torch, stream):
     plain = p_contacts / (p_ms / 1e3) if p_ms > 0 else None
     return {
         "workload": (f"{len(scs)} settling scenes, {nb} bodies, steps {pre + 1}-{total_steps} of "
-                     f"{total_steps} timed (h 1e-3), mixed precision, per-scene convergence"),
+                     f"{total_steps} timed (h 1e-3), mixed precision with up to {args.refine} FP64 "
+                     f"refinement iterations, per-scene convergence"),
         "value": batched, "unit": "contact-steps/s", "ms_per_step": ms / timed,
         "contacts_per_step": contacts / timed,
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
@@ -508,7 +509,7 @@ def run_served(args, N, stream):
     while i < n_req or busy:
         now = time.perf_counter() - t0
         while i < n_req and arrive[i] <= now:
-            srv.submit(ahead.get(), args.serve_steps)
+            srv.submit(ahead.get(), args.serve_steps, refine_iterations=args.refine)
             i += 1
         if not busy and i < n_req and arrive[i] > now:
             time.sleep(min(arrive[i] - now, 0.01))
@@ -556,7 +557,8 @@ def run_served(args, N, stream):
     return {
         "workload": (f"{n_req} requests, Poisson {args.serve_rate}/s for {args.serve_seconds} s, "
                      f"{args.serve_steps} steps each (h 1e-3), spheres log-uniform [500, 50000], "
-                     f"mixed precision, 150 GB budget"),
+                     f"mixed precision with up to {args.refine} FP64 refinement iterations, "
+                     f"150 GB budget"),
         "value": served, "unit": "contact-steps/s (wall clock, arrivals included)",
         "device_contact_steps_per_s": contact_steps / (st["device_ms"] / 1e3),
         "wall_s": wall, "completed": int(st["completed"]), "rounds": int(st["rounds"]),
@@ -726,6 +728,9 @@ def main():
     ap.add_argument("--tol-steps", type=int, default=10)
     ap.add_argument("--no-mixed-error", action="store_true",
                     help="skip the mixed-precision error report")
+    ap.add_argument("--refine", type=int, default=500,
+                    help="FP64 refinement iterations of the batched and served mixed-precision "
+                         "solves (0: FP32 iterates alone)")
     ap.add_argument("--batch-scenes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--batch-timed", type=int, default=40)

@@ -154,3 +154,26 @@ def test_refinement_off_is_the_plain_mixed_solve(native):
             assert sc_["refine_iterations"] == 0
             assert np.array_equal(a.gamma(), c.gamma())
             assert np.array_equal(a.state()[1], c.state()[1])
+
+
+def test_refined_batch_equals_refined_alone(native):
+    """FP64 refinement in a batch: each scene's result is the same bits as the
+    scene stepped alone with refinement (the refinement launch, like the FP32
+    one, works per scene), including scenes whose FP32 phase converges and
+    scenes that need FP64 iterations."""
+    rng = np.random.default_rng(4)
+    scs = [scenes.random_cluster(1, n=30, tolerance=1e-8, max_iterations=3000),
+           scenes.lattice_container(rng, 150, tolerance=1e-6),
+           scenes.settling_box(n_side=3)]
+    b = native.NativeBatch(scs, precision=1, refine_iterations=REFINE_ITERATIONS)
+    b.step(10)
+    refined = 0
+    for i, sc in enumerate(scs):
+        g = native.NativeScene.from_scene(sc, precision=1, refine_iterations=REFINE_ITERATIONS)
+        for _ in range(10):
+            g.step(1)
+            refined += g.stats()["refine_iterations"] > 0
+        assert np.array_equal(b.state(i)[0], g.state()[0]), i
+        assert np.array_equal(b.state(i)[1], g.state()[1]), i
+        assert np.array_equal(b.gamma(i), g.gamma()), i
+    assert refined > 0

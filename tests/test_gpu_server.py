@@ -22,15 +22,15 @@ def _requests():
     ]
 
 
-def _alone(native, sc, nsteps, precision):
-    g = native.NativeScene.from_scene(sc, precision=precision)
+def _alone(native, sc, nsteps, precision, **kw):
+    g = native.NativeScene.from_scene(sc, precision=precision, **kw)
     g.step(nsteps)
     p, v = g.state()
     g.close()
     return p, v
 
 
-def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_round=3):
+def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_round=3, **kw):
     srv = native.NativeServer(precision=precision, hbm_budget_bytes=budget, max_active=max_active,
                               steps_per_round=steps_per_round)
     ids = []
@@ -44,7 +44,7 @@ def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_rou
         if r < len(arrivals):
             for i in arrivals[r]:
                 if i < len(reqs):
-                    ids.append((i, srv.submit(reqs[i][0], reqs[i][1])))
+                    ids.append((i, srv.submit(reqs[i][0], reqs[i][1], **kw)))
         busy = srv.round()
         max_resident = max(max_resident, srv.stats()["active"])
         for res in srv.poll():
@@ -57,17 +57,19 @@ def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_rou
     return ids, results, states, st, max_resident
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_served_results_equal_alone(native, precision):
+@pytest.mark.parametrize("precision,refine", [(0, 0), (1, 0), (1, 500)],
+                         ids=["fp64", "mixed", "mixed_refined"])
+def test_served_results_equal_alone(native, precision, refine):
     reqs = _requests()
-    ids, results, states, st, _ = _serve(native, reqs, precision)
+    kw = {"refine_iterations": refine} if refine else {}
+    ids, results, states, st, _ = _serve(native, reqs, precision, **kw)
     assert st["completed"] == len(reqs) and st["pending"] == 0 and st["active"] == 0
     for i, rid in ids:
         res = results[rid]
         assert res["status"] == 0
         assert res["nsteps"] == reqs[i][1]
         assert res["t_admit"] >= res["t_submit"] and res["t_done"] >= res["t_admit"]
-        p, v = _alone(native, reqs[i][0], reqs[i][1], precision)
+        p, v = _alone(native, reqs[i][0], reqs[i][1], precision, **kw)
         ps, vs = states[i]
         assert np.array_equal(ps, p) and np.array_equal(vs, v), i
 
