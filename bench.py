@@ -496,7 +496,8 @@ def run_served(args, N, stream):
     while ahead.qsize() < min(n_req, 512):
         time.sleep(0.01)
     srv = N.NativeServer(precision=N.DV_PREC_MIXED, hbm_budget_bytes=150e9,
-                         steps_per_round=args.serve_round, keep_states=False)
+                         steps_per_round=args.serve_round, keep_states=False,
+                         max_resident_bodies=args.serve_max_bodies)
     srv.set_stream(stream.cuda_stream)
     sampler = ClockSampler(torch_device_index())
     sampler.start()
@@ -558,7 +559,9 @@ def run_served(args, N, stream):
         "workload": (f"{n_req} requests, Poisson {args.serve_rate}/s for {args.serve_seconds} s, "
                      f"{args.serve_steps} steps each (h 1e-3), spheres log-uniform [500, 50000], "
                      f"mixed precision with up to {args.refine} FP64 refinement iterations, "
-                     f"150 GB budget"),
+                     f"150 GB budget"
+                     + (f", at most {args.serve_max_bodies} resident bodies"
+                        if args.serve_max_bodies else "")),
         "value": served, "unit": "contact-steps/s (wall clock, arrivals included)",
         "device_contact_steps_per_s": contact_steps / (st["device_ms"] / 1e3),
         "wall_s": wall, "completed": int(st["completed"]), "rounds": int(st["rounds"]),
@@ -740,6 +743,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--serve-round", type=int, default=4)
+    ap.add_argument("--serve-max-bodies", type=int, default=0,
+                    help="resident-body limit of the server (0: none; the 4,096-scene and "
+                         "150 GB limits still hold)")
     ap.add_argument("--serve-trace-s", type=float, default=5.0,
                     help="interval of the served line's backlog trace")
     args = ap.parse_args()

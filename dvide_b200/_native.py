@@ -113,7 +113,7 @@ class TuneReport(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_double), ("max_active", C.c_int32),
                 ("steps_per_round", C.c_int32), ("precision", C.c_int32), ("use_graph", C.c_int32),
-                ("keep_states", C.c_int32), ("pad_", C.c_int32)]
+                ("keep_states", C.c_int32), ("max_resident_bodies", C.c_int32)]
 
 
 class RequestResult(C.Structure):
@@ -608,7 +608,7 @@ class NativeServer:
     the HBM budget allow, resident scenes step together, finished ones leave."""
 
     def __init__(self, precision=DV_PREC_MIXED, hbm_budget_bytes=150e9, max_active=4096,
-                 steps_per_round=4, use_graph=True, keep_states=True):
+                 steps_per_round=4, use_graph=True, keep_states=True, max_resident_bodies=0):
         L = lib()
         cfg = ServerConfig()
         check(L.dv_server_default_config(C.byref(cfg)))
@@ -618,6 +618,7 @@ class NativeServer:
         cfg.precision = int(precision)
         cfg.use_graph = int(bool(use_graph))
         cfg.keep_states = int(bool(keep_states))
+        cfg.max_resident_bodies = int(max_resident_bodies)
         self.cfg = cfg
         h = C.c_void_p()
         check(L.dv_server_create(C.byref(cfg), C.byref(h)), "dv_server_create")

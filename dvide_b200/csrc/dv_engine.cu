@@ -680,11 +680,13 @@ int Engine::ensure_records(int n) {
   int cap = std::max(n, 2 * ring_cap_);
   if (h_ew_ring_) cudaFreeHost(h_ew_ring_);
   if (h_sst_ring_) cudaFreeHost(h_sst_ring_);
-  if (h_red_) cudaFreeHost(h_red_);
   h_ew_ring_ = nullptr;
   h_sst_ring_ = nullptr;
+  // sized by the segment capacity, not the current count: a later layout with
+  // more segments that still fit the capacity keeps this ring
   if (cudaMallocHost(&h_ew_ring_, sizeof(EngineWords) * cap) != cudaSuccess ||
-      cudaMallocHost(&h_sst_ring_, sizeof(SegState) * (size_t)cap * d.nseg) != cudaSuccess)
+      cudaMallocHost(&h_sst_ring_, sizeof(SegState) * (size_t)cap * std::max(seg_cap_, d.nseg)) !=
+          cudaSuccess)
     return dv_record_cuda_error(cudaErrorMemoryAllocation, "cudaMallocHost", __FILE__, __LINE__);
   while ((int)ev_.size() < 3 * cap) {
     cudaEvent_t e;

@@ -1,8 +1,8 @@
 // dv_server.cu -- serving (continuous batching) over an engine: the serving
 // C ABI of include/dvide.h.  No counterpart in the reference.
 //
-// A round: admit pending requests (FIFO) while a slot and the HBM budget
-// allow; if the resident set changed, reconfigure the engine (resident
+// A round: admit pending requests (FIFO) while a slot, the HBM budget and
+// the resident-body limit allow; if the resident set changed, reconfigure the engine (resident
 // scenes keep their state on the device); run `steps_per_round` steps of
 // every resident scene (fewer when a resident scene needs fewer to finish);
 // retire the scenes whose steps are done, copying their final state out.
@@ -117,8 +117,14 @@ struct dv_server {
     }
     active.clear();
     bool changed = departed;
+    long long bodies = 0;
+    for (auto& r : next) bodies += (long long)r->bodies.size();
+    const long long body_cap = cfg.max_resident_bodies;
     while (!pending.empty() && (int)next.size() < cfg.max_active &&
-           (next.empty() || bytes_in_use + pending.front()->bytes <= cfg.hbm_budget_bytes)) {
+           (next.empty() || bytes_in_use + pending.front()->bytes <= cfg.hbm_budget_bytes) &&
+           (body_cap <= 0 || next.empty() ||
+            bodies + (long long)pending.front()->bodies.size() <= body_cap)) {
+      bodies += (long long)pending.front()->bodies.size();
       std::unique_ptr<Request> r = std::move(pending.front());
       pending.pop_front();
       r->t_admit = now();
@@ -232,7 +238,7 @@ DV_API int dv_server_default_config(dv_server_config* c) {
 
 DV_API int dv_server_create(const dv_server_config* cfg, dv_server** out) {
   if (!cfg || !out || cfg->max_active <= 0 || cfg->steps_per_round <= 0 ||
-      !(cfg->hbm_budget_bytes > 0))
+      !(cfg->hbm_budget_bytes > 0) || cfg->max_resident_bodies < 0)
     return DV_ERR_ARG;
   if (cfg->precision != DV_PREC_FP64 && cfg->precision != DV_PREC_MIXED) return DV_ERR_UNSUPPORTED;
   dv_server* s = new dv_server();

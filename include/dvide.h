@@ -320,7 +320,9 @@ typedef struct dv_server_config {
   int32_t precision;         /* DV_PREC_FP64 or DV_PREC_MIXED for every scene */
   int32_t use_graph;         /* replay steps from a CUDA graph between membership changes */
   int32_t keep_states;       /* keep each finished scene's final p, v for dv_server_result_state */
-  int32_t pad_;
+  int32_t max_resident_bodies; /* resident bodies at most, 0 = no limit: bounds the work (and so
+                                  the time) of each step; a scene larger than the limit is
+                                  admitted alone */
 } dv_server_config;
 
 typedef struct dv_request_result {

@@ -298,3 +298,19 @@ def test_column_full_scale_contacts_and_one_step(native, oracle_mod):
     assert _rel(gg, go) <= REL_TOL and _rel(vg, vo) <= REL_TOL
     assert np.array_equal(gg, go)
     assert np.array_equal(vg, vo) and np.array_equal(pg, po)
+
+
+def test_diagnostics_after_the_step_records_grow(native, oracle_mod):
+    """The CCP violation and energies read back through a pinned buffer that
+    must survive the growth of the per-step record ring (a long dv_step call
+    after a short one)."""
+    sc = scenes.random_cluster(9, n=30)
+    g, o = _pair(native, oracle_mod, sc)
+    g.step(1)
+    o.step(1)
+    assert np.array_equal(g.ccp_violation(), o.ccp_violation())
+    g.step(40)
+    o.step(40)
+    assert np.array_equal(g.ccp_violation(), o.ccp_violation())
+    ke, pe = g.energies()
+    assert ke == o.kinetic_energy() and pe == o.potential_energy()

@@ -30,9 +30,10 @@ def _alone(native, sc, nsteps, precision, **kw):
     return p, v
 
 
-def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_round=3, **kw):
+def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_round=3,
+           max_bodies=0, **kw):
     srv = native.NativeServer(precision=precision, hbm_budget_bytes=budget, max_active=max_active,
-                              steps_per_round=steps_per_round)
+                              steps_per_round=steps_per_round, max_resident_bodies=max_bodies)
     ids = []
     results = {}
     max_resident = 0
@@ -94,3 +95,46 @@ def test_max_active_one_is_sequential(native):
     order = sorted(results.values(), key=lambda r: r["t_admit"])
     for a, b in zip(order, order[1:]):
         assert b["t_admit"] >= a["t_done"]
+
+
+def test_resident_body_limit(native):
+    """max_resident_bodies bounds the bodies stepped together (the work of a
+    step): at every admission the requests admitted and not yet finished hold
+    at most that many bodies, unless one request alone is larger; results stay
+    the same bits as alone."""
+    reqs = _requests()
+    cap = 150
+    ids, results, states, st, _ = _serve(native, reqs, 1, max_bodies=cap)
+    assert st["completed"] == len(reqs)
+    res = list(results.values())
+    for r in res:
+        t = r["t_admit"]
+        resident = [q for q in res if q["t_admit"] <= t < q["t_done"]]
+        if len(resident) > 1:
+            assert sum(q["nb"] for q in resident) <= cap, (t, [(q["id"], q["nb"]) for q in resident])
+    assert max(r["nb"] for r in res) > cap  # one request is admitted alone
+    for i, rid in ids:
+        p, v = _alone(native, reqs[i][0], reqs[i][1], 1)
+        assert np.array_equal(states[i][0], p), i
+
+
+def test_segment_count_growing_within_capacity(native):
+    """Admissions that raise the resident count without outgrowing the segment
+    capacity (100 resident, then 101 -- capacity 125 --, then 121) keep the
+    per-step records in bounds: every result is the same bits as alone."""
+    balls = [scenes.free_balls(n=1 + (i % 3), tolerance=1e-6) for i in range(121)]
+    srv = native.NativeServer(precision=0, max_active=4096, steps_per_round=2)
+    ids = []
+    for stage in (range(0, 100), range(100, 101), range(101, 121)):
+        for i in stage:
+            ids.append((i, srv.submit(balls[i], 6)))
+        srv.round()
+    busy = True
+    while busy:
+        busy = srv.round()
+    srv.poll()
+    for i, rid in ids:
+        p, v = _alone(native, balls[i], 6, 0)
+        ps, vs = srv.result_state(rid)
+        assert np.array_equal(ps, p) and np.array_equal(vs, v), i
+    srv.close()
