@@ -623,7 +623,6 @@ def run_cpu_table(args):
     C3 and C4 step the oracle once from states of the plain FP64 GPU
     trajectory (bit-identical to the oracle's own), so that the CPU time goes
     to the timed steps only."""
-    import torch
     from oracle import oracle as O
     from dvide_b200 import _native as N
     from dvide_b200 import scenes, workloads
@@ -700,7 +699,6 @@ def run_cpu_table(args):
             rows[name] += _oracle_timed_steps(O, threads, scj, st, m)
     out["C4"] = {k: _cpu_row(r, "16 of the 12,000 requests (stratified by size), one at a "
                                 "time, 200 steps (every 10th)") for k, r in rows.items()}
-    del torch
     return out
 
 
