@@ -441,6 +441,9 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       if (t < 0) break;
       locate(a, sc, t);
       const int s = sc.s;
+      // refinement launch: a solve it does not refine needs no r, start or Lipschitz
+      // estimate (its q and warm start from the FP32 launch stand)
+      if (a.refine && !__ldcg(&a.sst[s].ctl.refined)) continue;
       if (s != run.s) {
         if (run.n) {
           fold_parked<1, false>(a, s_def, nslot);
@@ -580,6 +583,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
       if (t < 0) break;
       locate(a, sc, t);
       const int s = sc.s;
+      if (a.refine && !__ldcg(&a.sst[s].ctl.refined)) continue;
       if (s != run.s) {
         if (run.n) {
           fold_parked<1, false>(a, s_def, nslot);
@@ -795,9 +799,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           int k = k0 + m * kThreads + threadIdx.x;
           if (k < nc) {
             const int c = c0 + k;
-            const T* nrm = normal_planes<T>(a);
-            Frame<T> f = iter_frame<T, (DV_STORED_FRAME & 2) != 0>(a, c, nrm[c], nrm[S + c],
-                                                                   nrm[2 * S + c], s_st.exact != 0);
+            Frame<T> f = load_frame<T>(a, c, s_st.exact != 0);
             T c0v = Gc[0 * S + c], c1v = Gc[1 * S + c], c2v = Gc[2 * S + c];
             T y0, y1, y2, N0, N1, N2;
             if (yr) {
@@ -989,8 +991,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
           const uint32_t* su = reinterpret_cast<const uint32_t*>(sd + (size_t)kStagePlanes * 32);
           const int j = lane;
           Frame<T> f =
-              iter_frame<T, (DV_STORED_FRAME & 1) != 0>(a, c, sd[0 * 32 + j], sd[1 * 32 + j],
-                                                         sd[2 * 32 + j], ps.exact != 0);
+              make_frame<T>(sd[0 * 32 + j], sd[1 * 32 + j], sd[2 * 32 + j], ps.exact != 0);
           V wa = wv[su[j]], wb = wv[su[32 + j]];
           T N0, N1, N2;
           ft_times<T, V>(f, wa, wb, &N0, &N1, &N2);
@@ -1196,7 +1197,7 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
   // ---- gamma = gamma_hat (APGD.cu:358) into the warm-start region; q = F gamma (FP64)
   {
     int cs = -1, cbest = -1;
-    bool keep = false;
+    bool keep = false, skip = false;
     const T* src = nullptr;
     for (int i = 0;; ++i) {
       const int t = cta_tile(a, NT, i);
@@ -1207,10 +1208,14 @@ __global__ void __launch_bounds__(kThreads, kMinB) k_step_solve(KArgs<T> a) {
         cs = s;
         cbest = __ldcg(&a.sst[s].ctl.best);
         src = cbest >= 0 ? a.G[cbest] : nullptr;
-        // refinement launch: a solve it did not refine, or whose FP64 phase
-        // accepted no iterate, keeps the FP32 phase's gamma_hat
-        keep = a.refine && (!__ldcg(&a.sst[s].ctl.refined) || cbest < 0);
+        // refinement launch: a solve it did not refine keeps the FP32 launch's
+        // gamma_hat and q = F gamma_hat, written by that launch's final pass; one
+        // whose FP64 phase accepted no iterate keeps that gamma_hat, and q is
+        // formed again (this launch's setup passes wrote over it)
+        skip = a.refine && !__ldcg(&a.sst[s].ctl.refined);
+        keep = a.refine && cbest < 0;
       }
+      if (skip) continue;
       const SegParams& P = a.seg[s];
       const int k0 = (t - sc.t0) * kTileItems, nc = sc.nc, c0 = sc.c0;
       const int kb = a.nbil ? bil_tile_k0(t, sc.t0, nc) : -1;
