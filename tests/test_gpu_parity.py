@@ -3,7 +3,7 @@
 Bar: bit-exact for the contact list (ids, normal, gap, location, frame) and,
 because both sides share one floating-point order, bit-exact for the FP64
 solve too (gamma, v, p, contact forces, iteration count, residual); the
-north-star tolerance (1e-10 relative on gamma and v) is asserted as well so a
+parity tolerance (1e-10 relative on gamma and v) is asserted as well so a
 failure reports its size."""
 import numpy as np
 import pytest
