@@ -570,6 +570,8 @@ def run_served(args, N, stream):
                              "p99": float(np.percentile(step_p99, 99))},
         "completion_latency_s": {"p50": float(np.percentile(lat, 50)),
                                  "p99": float(np.percentile(lat, 99))},
+        "scene_solves_at_tolerance": (f"{sum(r['solves_at_tolerance'] for r in results)}/"
+                                      f"{sum(r['solves'] for r in results)}"),
         "backlog": {"max_waiting": max(t[1] for t in trace) if trace else 0,
                     "max_resident": max(t[2] for t in trace) if trace else 0,
                     "peak_resident_gb": max(t[3] for t in trace) / 1e9 if trace else 0.0,

@@ -118,7 +118,8 @@ class ServerConfig(C.Structure):
 
 class RequestResult(C.Structure):
     _fields_ = [("id", C.c_int64), ("nb", C.c_int32), ("nsteps", C.c_int32),
-                ("status", C.c_int32), ("rounds", C.c_int32), ("t_submit", C.c_double),
+                ("status", C.c_int32), ("rounds", C.c_int32), ("solves", C.c_int32),
+                ("solves_at_tolerance", C.c_int32), ("t_submit", C.c_double),
                 ("t_admit", C.c_double), ("t_done", C.c_double), ("contact_steps", C.c_double),
                 ("step_ms_mean", C.c_double), ("step_ms_p50", C.c_double),
                 ("step_ms_p99", C.c_double), ("bytes", C.c_double)]

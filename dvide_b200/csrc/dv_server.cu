@@ -26,6 +26,7 @@ struct Request {
   std::vector<dv_body_desc> bodies;
   dv_params P{};
   int nsteps = 0, done = 0, status = DV_OK, rounds = 0;
+  int solves = 0, solves_at_tol = 0;
   double t_submit = 0, t_admit = 0, t_done = 0;
   double contact_steps = 0, bytes = 0;
   std::vector<float> step_ms;
@@ -167,6 +168,10 @@ struct dv_server {
         const SegState& X = rec.sst[q.seg];
         q.contact_steps += X.nc;
         st.contact_steps += X.nc;
+        if (X.nc > 0) {
+          q.solves += 1;
+          if (X.ctl.residual < q.P.tolerance) q.solves_at_tol += 1;
+        }
         q.step_ms.push_back(rec.ms_total);
         if (q.status == DV_OK) q.status = status_from_bits(X.err);
       }
@@ -190,6 +195,8 @@ struct dv_server {
       o.nsteps = q.nsteps;
       o.status = q.status;
       o.rounds = q.rounds;
+      o.solves = q.solves;
+      o.solves_at_tolerance = q.solves_at_tol;
       o.t_submit = q.t_submit;
       o.t_admit = q.t_admit;
       o.t_done = q.t_done;

@@ -331,6 +331,8 @@ typedef struct dv_request_result {
   int32_t nsteps;
   int32_t status;            /* first solver error of the scene, DV_OK otherwise */
   int32_t rounds;
+  int32_t solves;            /* its steps that solved (contacts or rows present) */
+  int32_t solves_at_tolerance; /* ... whose solve ended below the solver tolerance */
   double t_submit, t_admit, t_done;
   double contact_steps;      /* contacts summed over its steps */
   double step_ms_mean, step_ms_p50, step_ms_p99;  /* device time of the steps it took part in */

@@ -70,6 +70,7 @@ def test_served_results_equal_alone(native, precision, refine):
         assert res["status"] == 0
         assert res["nsteps"] == reqs[i][1]
         assert res["t_admit"] >= res["t_submit"] and res["t_done"] >= res["t_admit"]
+        assert 0 <= res["solves_at_tolerance"] <= res["solves"] <= res["nsteps"]
         p, v = _alone(native, reqs[i][0], reqs[i][1], precision, **kw)
         ps, vs = states[i]
         assert np.array_equal(ps, p) and np.array_equal(vs, v), i
