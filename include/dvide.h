@@ -74,11 +74,12 @@ typedef struct dv_params {
   int32_t anti_relaxation;  /* APGD::setAntiRelaxation (APGD.cuh:63, APGD.cu:335-345), default 0;
                                FP64 APGD scenes of their own (not in batches or servers),
                                without bilateral rows and without dv_apgd_solve */
-  int32_t refine_iterations; /* extension, DV_PREC_MIXED APGD only, default 0 (off): at most
-                               this many FP64 APGD iterations after the FP32 ones, started
-                               from the FP32 best iterate, for every solve whose FP32 phase
-                               ended above the tolerance (iteration cap, or no new best
-                               residual for 50 accepted iterations) */
+  int32_t refine_iterations; /* extension, default 0 (off); used by DV_PREC_MIXED APGD and
+                               ignored by FP64 scenes, PGJ and PGS: at most this many FP64
+                               APGD iterations after the FP32 ones, started from the FP32
+                               best iterate, for every solve whose FP32 phase ended above
+                               the tolerance (iteration cap, or no new best residual for 50
+                               accepted iterations) */
 } dv_params;
 
 /* Per-step report (System.cu:586-599 and APGD.cu:351-357). */
