@@ -177,3 +177,19 @@ def test_refined_batch_equals_refined_alone(native):
         assert np.array_equal(b.state(i)[1], g.state()[1]), i
         assert np.array_equal(b.gamma(i), g.gamma()), i
     assert refined > 0
+
+
+def test_refinement_with_scenes_without_contacts(native):
+    """A refined batch holding a scene without contacts (free flight) and
+    scenes whose FP32 phase converges: each steps as it does alone."""
+    scs = [scenes.free_balls(n=3, tolerance=1e-6),
+           scenes.random_cluster(2, n=27, tolerance=1e-4),
+           scenes.ball_on_ground(h=1e-3, tolerance=1e-8, warm_start=1)]
+    b = native.NativeBatch(scs, precision=1, refine_iterations=REFINE_ITERATIONS)
+    b.step(6)
+    for i, sc in enumerate(scs):
+        g = native.NativeScene.from_scene(sc, precision=1, refine_iterations=REFINE_ITERATIONS)
+        g.step(6)
+        assert np.array_equal(b.state(i)[0], g.state()[0]), i
+        assert np.array_equal(b.state(i)[1], g.state()[1]), i
+    assert b.scene_stats()[0]["num_contacts"] == 0
