@@ -178,28 +178,6 @@ __device__ inline Frame<double> stored_frame(const KArgs<T>& a, int c) {
   return f;
 }
 
-// The frame of contact c in the iterating passes, with its normal already at
-// hand: in FP64 the tangents are read from the stored u, v planes (the bits
-// the narrowphase wrote, which rebuilding them from the normal reproduces),
-// taking the frame's FP64 division and float square roots off the passes'
-// latency chain; in FP32 they are rebuilt from the FP32 normal.
-#ifndef DV_STORED_FRAME
-#define DV_STORED_FRAME 0
-#endif
-template <class T, bool kStored = true>
-__device__ inline Frame<T> iter_frame(const KArgs<T>& a, int c, T n0, T n1, T n2, bool exact) {
-  if (sizeof(T) == sizeof(double) && kStored) {
-    const double* F = a.F;
-    const size_t S = a.S;
-    Frame<T> f;
-    f.n0 = n0; f.n1 = n1; f.n2 = n2;
-    f.u0 = (T)__ldg(F + 3 * S + c); f.u1 = (T)__ldg(F + 4 * S + c); f.u2 = (T)__ldg(F + 5 * S + c);
-    f.v0 = (T)__ldg(F + 6 * S + c); f.v1 = (T)__ldg(F + 7 * S + c); f.v2 = (T)__ldg(F + 8 * S + c);
-    return f;
-  }
-  return make_frame<T>(n0, n1, n2, exact);
-}
-
 // Stores of the vectors a pass writes and the next pass reads at once (q for
 // the body pass, w for the contact pass's gathers), with an L2 evict-last
 // priority: each contact pass streams more contact data than L2 holds, and
