@@ -595,40 +595,53 @@ __device__ inline int pass_tile(const K& a, int lon, int n, int i) {
   return (t < 0 || !lon) ? t : __ldcg(a.act_tiles + t);
 }
 
-// Sum of -q over B-side contacts, then +q over A-side contacts, ascending
-// contact order (the flat incidence list); loads are issued in groups of
-// eight, the additions stay in order.
-template <class T, class V, class K>
-__device__ inline V gather_q(const K& a, const V* q, int b) {
-  T ax = T(0), ay = T(0), az = T(0);
-  const int s = __ldg(a.inc_start + b), e = __ldg(a.inc_start + b + 1);
-  for (int i = s; i < e; i += 8) {
-    uint32_t c[8];
-    V qq[8];
+// Eight incidence entries c[0, n) of a body's run (n <= 8): their q gathered
+// together, then added to (ax, ay, az) in order, -q for a B side.
+template <class T, class V>
+__device__ inline void add_q8(const V* q, const uint32_t* c, int n, T& ax, T& ay, T& az) {
+  V qq[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) c[j] = (i + j < e) ? __ldg(a.inc + i + j) : 0u;
+  for (int j = 0; j < 8; ++j) {
+    if (j < n) {
+      qq[j] = q[c[j] & 0x7fffffffu];
+    } else {
+      qq[j].x = T(0); qq[j].y = T(0); qq[j].z = T(0); qq[j].w = T(0);
+    }
+  }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (i + j < e) {
-        qq[j] = q[c[j] & 0x7fffffffu];
+  for (int j = 0; j < 8; ++j) {
+    if (j < n) {
+      if (c[j] & 0x80000000u) {
+        ax = ax - qq[j].x; ay = ay - qq[j].y; az = az - qq[j].z;
       } else {
-        qq[j].x = T(0); qq[j].y = T(0); qq[j].z = T(0); qq[j].w = T(0);
+        ax = ax + qq[j].x; ay = ay + qq[j].y; az = az + qq[j].z;
       }
     }
+  }
+}
+
+// Sum of -q over B-side contacts, then +q over A-side contacts, ascending
+// contact order (the flat incidence list).  Sixteen incidence entries are
+// read at once (a settled body has about seven contacts, often more than
+// eight), their q in two groups of eight; the additions stay in order.
+template <class T, class V, class K>
+__device__ inline V gather_q(const K& a, const V* q, int s, int e) {
+  T ax = T(0), ay = T(0), az = T(0);
+  for (int i = s; i < e; i += 16) {
+    uint32_t c[16];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (i + j < e) {
-        if (c[j] & 0x80000000u) {
-          ax = ax - qq[j].x; ay = ay - qq[j].y; az = az - qq[j].z;
-        } else {
-          ax = ax + qq[j].x; ay = ay + qq[j].y; az = az + qq[j].z;
-        }
-      }
-    }
+    for (int j = 0; j < 16; ++j) c[j] = (i + j < e) ? __ldg(a.inc + i + j) : 0u;
+    add_q8<T, V>(q, c, e - i, ax, ay, az);
+    if (i + 8 < e) add_q8<T, V>(q, c + 8, e - i - 8, ax, ay, az);
   }
   V r;
   r.x = ax; r.y = ay; r.z = az; r.w = T(0);
   return r;
+}
+
+template <class T, class V, class K>
+__device__ inline V gather_q(const K& a, const V* q, int b) {
+  return gather_q<T, V>(a, q, __ldg(a.inc_start + b), __ldg(a.inc_start + b + 1));
 }
 
 // Bilateral DOF rows.  Tile t of a segment with contacts [0, nc) and tiles
@@ -729,14 +742,32 @@ __device__ inline void mark_done(const K& a, int s) {
 // w_b of one body of an iterating segment.
 // kAR: also v = Minv (k + D^T x) for the anti-relaxation (APGD.cu:338-340;
 // 0 for fixed bodies, whose v enters only as squares).
+// The words a body's gather starts from: its inverse mass, the bounds of its
+// incidence run and (batches) its segment, loaded together so that they cost
+// one memory round trip, and loaded a round ahead by the body pass.
+struct BodyHead {
+  double mi;
+  int s, e, seg;
+};
+
+template <class K>
+__device__ inline BodyHead body_head(const K& a, int b) {
+  BodyHead h;
+  h.mi = __ldg(a.minv + b);
+  h.s = __ldg(a.inc_start + b);
+  h.e = __ldg(a.inc_start + b + 1);
+  h.seg = a.nseg > 1 ? __ldg(a.bseg + b) : 0;
+  return h;
+}
+
 template <class T, bool kAR = false>
-__device__ inline void body_w(const KArgs<T>& a, int b) {
+__device__ inline void body_w(const KArgs<T>& a, int b, const BodyHead& h) {
   using V = typename Vec4<T>::type;
   V* w = reinterpret_cast<V*>(a.wd);
   const V* q = reinterpret_cast<const V*>(a.qd);
-  double mi = __ldg(a.minv + b);
+  const double mi = h.mi;
   if (mi != 0.0) {
-    V s = gather_q<T, V>(a, q, b);
+    V s = gather_q<T, V>(a, q, h.s, h.e);
     if (a.nbil) add_bilateral<T, V>(a.bil_inc_start, a.bil_inc, a.bq, b, s);
     T m = (T)mi;
     V o;
@@ -769,22 +800,21 @@ __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask
       const int4 r = __ldcg(a.act_bodies + p);
       if (mask_done(a, s_mask, mwords, r.z)) continue;
       const int b = r.x + threadIdx.x;
-      if (b < r.y) body_w<T, kAR>(a, b);
+      if (b < r.y) body_w<T, kAR>(a, b, body_head(a, b));
     }
     return;
   }
-  const int nbt = (a.nb + kThreads - 1) / kThreads;
-  for (int bt = blockIdx.x; bt < nbt; bt += gridDim.x) {
-    int b = bt * kThreads + threadIdx.x;
-    // the next round's per-body words into L2 while this round gathers
-    const int bn = b + gridDim.x * kThreads;
-    if (bn < a.nb) {
-      prefetch_l2(a.inc_start + bn);
-      prefetch_l2(a.minv + bn);
-      if (a.nseg > 1) prefetch_l2(a.bseg + bn);
-    }
-    if (b < a.nb && (a.nseg == 1 || !mask_done(a, s_mask, mwords, __ldg(a.bseg + b))))
-      body_w<T, kAR>(a, b);
+  // the next round's heads load into registers while this round gathers
+  const int stride = gridDim.x * kThreads;
+  int b = blockIdx.x * kThreads + threadIdx.x;
+  BodyHead h{0.0, 0, 0, 0};
+  if (b < a.nb) h = body_head(a, b);
+  for (; b < a.nb; b += stride) {
+    const int bn = b + stride;
+    BodyHead hn{0.0, 0, 0, 0};
+    if (bn < a.nb) hn = body_head(a, bn);
+    if (a.nseg == 1 || !mask_done(a, s_mask, mwords, h.seg)) body_w<T, kAR>(a, b, h);
+    h = hn;
   }
 }
 
