@@ -271,6 +271,21 @@ def free_balls(n=2, spacing=0.5, radius=0.05, h=1e-3, warm_start=1, vel=None,
     return sc
 
 
+def crowd(n_around, seed=5, radius=0.05, max_iterations=50) -> Scene:
+    """Sphere 0 with n_around equal spheres overlapping it, all with larger
+    ids (centres 0.5 to 1.5 radii from its centre, random directions), in
+    free space under gravity -z: one free body in contact with n_around
+    others, and the others with some of each other."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n_around, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    c = np.array([0.0, 0.0, 1.0])
+    pos = np.concatenate([c[None], c + d * radius * rng.uniform(0.5, 1.5, size=(n_around, 1))])
+    params = default_params(gravity=(0.0, 0.0, -G), max_iterations=max_iterations)
+    return _assemble([], pos, np.full(n_around + 1, radius), 2600.0, params,
+                     f"crowd_{n_around}")
+
+
 def bilateral_cluster(seed, n=64, warm_start=1, h=1e-3, max_iterations=400,
                       tolerance=1e-6) -> Scene:
     """random_cluster with bilateral rows (System::addBilateralConstraintDOF,

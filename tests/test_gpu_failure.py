@@ -25,29 +25,14 @@ def test_selftest_rejects_bad_limit(native):
         native.selftest_bounded_waits(0)
 
 
-def _crowd(n_around, seed=5):
-    """Sphere 0 with n_around equal spheres overlapping it, all with larger ids
-    (centres 0.5 to 1.5 radii away from its centre), in free space."""
-    import numpy as np
-
-    rng = np.random.default_rng(seed)
-    r = 0.05
-    d = rng.normal(size=(n_around, 3))
-    d /= np.linalg.norm(d, axis=1)[:, None]
-    c = np.array([0.0, 0.0, 1.0])
-    pos = np.concatenate([c[None], c + d * r * rng.uniform(0.5, 1.5, size=(n_around, 1))])
-    params = scenes.default_params(gravity=(0.0, 0.0, -9.81), max_iterations=50)
-    return scenes._assemble([], pos, np.full(n_around + 1, r), 2600.0, params, "crowd")
-
-
 def test_partner_limit_reports_an_argument_error(native):
     """The warp that lists a sphere's partners keeps at most 128 of them with
     larger ids; a sphere with 129 is reported as DV_ERR_ARG with a message,
     the step does nothing, and the scene stays usable."""
-    ok = native.NativeScene.from_scene(_crowd(128))
+    ok = native.NativeScene.from_scene(scenes.crowd(128))
     ok.step(1)
     assert ok.stats()["num_contacts"] >= 128 and ok.stats()["status"] == 0
-    bad = native.NativeScene.from_scene(_crowd(129))
+    bad = native.NativeScene.from_scene(scenes.crowd(129))
     p0, v0 = bad.state()
     with pytest.raises(native.DvError) as e:
         bad.step(1)

@@ -246,6 +246,26 @@ def _free_running(native, oracle_mod, sc, steps):
     return o.stats()
 
 
+@pytest.mark.parametrize("n_around", [9, 16, 17, 40, 128])
+def test_crowd_many_contacts_per_body_free_running(native, oracle_mod, n_around):
+    """One free sphere overlapped by n_around others, which overlap many of
+    each other too: body gathers walk from a few to over a hundred incidence
+    entries (sixteen per load group, q in two halves of eight, ragged ends).
+    Bit-identical to the oracle over three steps while the crowd flies apart:
+    the first step's solve runs its 50 iterations, and by the third step no
+    pair is in contact."""
+    sc = scenes.crowd(n_around)
+    g, o = _pair(native, oracle_mod, sc)
+    g.collide()
+    o.collide()
+    _compare_contacts(g, o)
+    ga = g.contacts()[0]
+    assert np.count_nonzero(ga == 0) == n_around
+    g.close()
+    st = _free_running(native, oracle_mod, sc, 3)
+    assert st["num_contacts"] == 0
+
+
 def test_c0_compressed_free_running(native, oracle_mod):
     """The 1,000-sphere settling box (C0 settings: mu 0.25, h 1e-3, tolerance 1e-4,
     1,000 iterations, warm start) with the lattice squeezed so that ~1,800 contacts
