@@ -266,6 +266,49 @@ def test_crowd_many_contacts_per_body_free_running(native, oracle_mod, n_around)
     assert st["num_contacts"] == 0
 
 
+def test_driver_moved_wall_free_running(native, oracle_mod):
+    """A fixed wall moved between steps by the driver, as the reference's shear
+    driver moves its boxes (models/test_shear.cu:389-406: the fixed boxes' v
+    overwritten, p advanced by h v before DoTimeStep).  The wall's new position
+    enters the next collision pass.  Its overwritten v enters neither k nor r:
+    k = M v with M = 0 for a fixed body (System.cu:1411-1417, 1505).  The update
+    sets it back to 0 (v = Minv (k + D^T gamma), :572, 577), so the step's
+    p += h v (:581) leaves the wall where the driver put it.  Bit-identical to the oracle over 60 steps:
+    the wall starts 1 mm from the lattice and pushes into it at 0.2 m/s while
+    the lattice lands on the floor."""
+    sc = scenes.settling_box()
+    wall = 1  # open_box order: floor, -x wall, +x wall, -y wall, +y wall
+    assert sc.fixed[wall] == 1
+    sph = sc.fixed == 0
+    p = sc.pos.copy()
+    p[wall, 0] = (p[sph, 0] - sc.geom[sph, 0]).min() - 1e-3 - sc.geom[wall, 0]
+    sc.pos = p
+    g, o = _pair(native, oracle_mod, sc)
+    h = sc.params["h"]
+    on_wall = 0
+    for k in range(60):
+        p, v = o.state()
+        v[wall] = (0.2, 0.0, 0.0)
+        p[wall] = p[wall] + h * v[wall]
+        o.set_state(p, v)
+        g.set_state(p, v)
+        assert o.step(1) == 0, k
+        g.step(1)
+        so, sg = o.stats(), g.stats()
+        assert sg["num_contacts"] == so["num_contacts"], k
+        for key in ("iterations", "backtracks", "residual", "objective"):
+            assert sg[key] == so[key], (k, key)
+        assert np.array_equal(g.gamma(), o.gamma()), k
+        pg, vg = g.state()
+        po, vo = o.state()
+        assert np.array_equal(vg, vo) and np.array_equal(pg, po), k
+        assert np.array_equal(g.fcontact(), o.fcontact()), k
+        assert (vo[wall] == 0.0).all() and np.array_equal(po[wall], p[wall]), k
+        ga, gb = g.contacts()[:2]
+        on_wall = max(on_wall, int(np.count_nonzero((ga == wall) | (gb == wall))))
+    assert on_wall > 20 and so["num_contacts"] > 100
+
+
 def test_c0_compressed_free_running(native, oracle_mod):
     """The 1,000-sphere settling box (C0 settings: mu 0.25, h 1e-3, tolerance 1e-4,
     1,000 iterations, warm start) with the lattice squeezed so that ~1,800 contacts
