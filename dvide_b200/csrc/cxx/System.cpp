@@ -43,6 +43,30 @@ DeviceArray::operator std::vector<double>() const {
   return download3(sys->scene, w, (int)sys->bodies.size());
 }
 
+DeviceArray& DeviceArray::operator=(const std::vector<double>& x) {
+  if (!sys->scene) throw std::logic_error("System device arrays are written after initializeSystem");
+  const size_t nb = sys->bodies.size();
+  int rc = 0;
+  if (which == kPos || which == kVel) {
+    if (x.size() != 3 * nb)
+      throw std::invalid_argument("System::p_d / v_d take 3 values per body (" +
+                                  std::to_string(3 * nb) + "), not " + std::to_string(x.size()));
+    rc = dv_set_state(sys->scene, which == kPos ? x.data() : nullptr,
+                      which == kVel ? x.data() : nullptr);
+  } else if (which == kGamma) {
+    if (!sys->bilaterals.empty())
+      throw std::logic_error("System::gamma_d of a System with bilateral rows is not writable");
+    if (x.size() % 3)
+      throw std::invalid_argument("System::gamma_d takes 3 values per contact, not " +
+                                  std::to_string(x.size()));
+    rc = dv_set_gamma(sys->scene, x.data(), (int32_t)(x.size() / 3));
+  } else {
+    throw std::logic_error("System::f_contact_d is the output of the last step");
+  }
+  if (rc != 0) throw std::runtime_error(std::string("dv_set_state / dv_set_gamma: ") + dv_last_error());
+  return *this;
+}
+
 size_t DeviceArray::size() const {
   if (which == kGamma) {
     int32_t n = 0, nb = 0;

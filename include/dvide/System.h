@@ -5,7 +5,9 @@
 // driver lines such as `sys->f_contact_h = sys->f_contact_d;` keep working.
 #pragma once
 
+#include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../dvide.h"
@@ -24,6 +26,24 @@ class DeviceArray {
   DeviceArray(System* s, Which w) : sys(s), which(w) {}
   operator std::vector<double>() const;
   size_t size() const;
+  // Uploads, as the reference's drivers write System::p_d, v_d and gamma_d
+  // from host vectors between steps (models/test_shear.cu:404-405): p_d and
+  // v_d take 3 values per body; gamma_d takes 3 per contact, the warm start of
+  // the next solve, on a System without bilateral rows.  Throws
+  // std::logic_error before initializeSystem, for f_contact_d (the output of
+  // the last step) and for gamma_d with bilateral rows;
+  // std::invalid_argument on a size that does not fit; std::runtime_error
+  // when the C ABI reports an error.
+  DeviceArray& operator=(const std::vector<double>& x);
+  // another System's array (or this one's): its values, not its handle
+  DeviceArray& operator=(const DeviceArray& o) {
+    return *this = static_cast<std::vector<double>>(o);
+  }
+  // any other container of doubles (a thrust::host_vector, say)
+  template <class C, class = decltype(std::declval<const C&>().begin())>
+  DeviceArray& operator=(const C& c) {
+    return *this = std::vector<double>(c.begin(), c.end());
+  }
 
  private:
   System* sys;
