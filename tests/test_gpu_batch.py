@@ -73,6 +73,44 @@ def test_batch_matches_oracle(native, oracle_mod):
         assert np.array_equal(b.gamma(i), o.gamma()), i
 
 
+def _ragged():
+    """Scenes at the edges of what a batch holds: a single free sphere (one
+    body, never a contact), only fixed boxes (no free body; box-box pairs are
+    never contacts), one sphere overlapped by 40 others (long incidence runs),
+    beside a ball on the ground and a cluster."""
+    grav = scenes.default_params(gravity=(0.0, 0.0, -9.81))
+    one = scenes._assemble([], np.array([[0.0, 0.0, 1.0]]), np.array([0.05]), 2600.0,
+                           dict(grav), "one_sphere")
+    walls = scenes._assemble(scenes.open_box(1.0, 1.0, 1.0), np.zeros((0, 3)), np.zeros(0),
+                             2600.0, dict(grav), "walls_only")
+    return [one, scenes.crowd(40), walls, scenes.ball_on_ground(h=1e-3),
+            scenes.random_cluster(0, n=40)]
+
+
+def test_batch_ragged_scenes_alone_and_oracle(native, oracle_mod):
+    """Each ragged scene is bit-identical in the batch, alone and in the oracle."""
+    scs = _ragged()
+    steps = 10
+    alone = _states_alone(native, scs, steps)
+    b = native.NativeBatch(scs)
+    b.step(steps)
+    st = b.scene_stats()
+    for i, sc in enumerate(scs):
+        p, v, g, _ = alone[i]
+        pb, vb = b.state(i)
+        assert np.array_equal(pb, p) and np.array_equal(vb, v), i
+        assert np.array_equal(b.gamma(i), g), i
+        o = oracle_mod.OracleScene(sc)
+        o.step(steps)
+        po, vo = o.state()
+        assert np.array_equal(pb, po) and np.array_equal(vb, vo), i
+        assert np.array_equal(b.gamma(i), o.gamma()), i
+        assert st[i]["num_contacts"] == o.stats()["num_contacts"], i
+    assert st[0]["num_contacts"] == 0 and st[2]["num_contacts"] == 0
+    # the fixed boxes did not move
+    assert np.array_equal(b.state(2)[0], scs[2].pos)
+
+
 def test_batch_launch_shapes_and_graph_identical(native):
     scs = _mix()
     steps = 12

@@ -76,6 +76,29 @@ def test_served_results_equal_alone(native, precision, refine):
         assert np.array_equal(ps, p) and np.array_equal(vs, v), i
 
 
+def test_served_ragged_requests_equal_alone(native):
+    """A single free sphere, only fixed boxes, one sphere overlapped by 40
+    others, a ball on the ground and a cluster, served together: each result
+    equals the scene stepped alone; the contact-free ones report no solve."""
+    grav = scenes.default_params(gravity=(0.0, 0.0, -9.81))
+    one = scenes._assemble([], np.array([[0.0, 0.0, 1.0]]), np.array([0.05]), 2600.0,
+                           dict(grav), "one_sphere")
+    walls = scenes._assemble(scenes.open_box(1.0, 1.0, 1.0), np.zeros((0, 3)), np.zeros(0),
+                             2600.0, dict(grav), "walls_only")
+    reqs = [(one, 7), (scenes.crowd(40), 5), (walls, 4), (scenes.ball_on_ground(h=1e-3), 9),
+            (scenes.random_cluster(0, n=40), 6)]
+    ids, results, states, st, _ = _serve(native, reqs, 0)
+    assert st["completed"] == len(reqs)
+    for i, rid in ids:
+        res = results[rid]
+        assert res["status"] == 0 and res["nsteps"] == reqs[i][1]
+        p, v = _alone(native, reqs[i][0], reqs[i][1], 0)
+        ps, vs = states[i]
+        assert np.array_equal(ps, p) and np.array_equal(vs, v), i
+        if i in (0, 2):
+            assert res["solves"] == 0, i
+
+
 def test_budget_limits_residency(native):
     reqs = _requests()
     nb_max = max(sc.nb for sc, _ in reqs)
