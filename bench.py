@@ -57,6 +57,23 @@ def solve_bytes(nc, nb, sweeps, backtracks):
     return sweeps * (440 * nc + 120 * nb) + backtracks * bN + 2 * bN + (136 * nc + 96 * nb)
 
 
+# Mixed precision with FP64 refinement (the batched and served forms): FP32
+# iterations at the FP32 variant's compulsory bytes, 248 nc + 72 nb each, and
+# one FP32 product, 76 nc + 36 nb, per backtrack and for each of the two setup
+# products; the FP64 refinement iterations at 440 nc + 120 nb, with the
+# refinement launch's own FP64 setup (two products) when a solve is refined;
+# then the FP64 update.  A scene without contacts only updates (96 nb).
+def solve_bytes_mixed(nc, nb, iterations, refine_iterations, backtracks):
+    if nc == 0:
+        return 96 * nb
+    bN32 = 76 * nc + 36 * nb
+    bN64 = 136 * nc + 60 * nb
+    it32 = iterations - refine_iterations
+    return (it32 * (248 * nc + 72 * nb) + refine_iterations * (440 * nc + 120 * nb)
+            + backtracks * bN32 + 2 * bN32 + (2 * bN64 if refine_iterations > 0 else 0)
+            + (136 * nc + 96 * nb))
+
+
 # The same count for the kernel's own sequence: ONE Schur product per APGD
 # iteration (N y is formed from the stored products of the last two iterates),
 # i.e. 440 nc + 120 nb less one product's 136 nc + 60 nb.
@@ -431,6 +448,15 @@ def run_batched(args, N, torch, stream):
     launches = b.launches() - l0
     nb = b.nb
     b.close()
+    # roofline over the whole step (collision included; the solve launches are
+    # most of it), bytes from every scene's own iteration counts
+    nbs = [sc.nb for sc in scs]
+    moved = sum(solve_bytes_mixed(x["num_contacts"], nbs[i], x["iterations"],
+                                  x["refine_iterations"], x["backtracks"])
+                for st in hist for i, x in enumerate(st))
+    peak, peak_kind = _peaks()
+    achieved = moved / timed / (ms / timed / 1e3) / 1e9
+    refine_its = sum(x["refine_iterations"] for st in hist for x in st)
     # plain FP64 path, one scene at a time, on a size-stratified sample
     order = np.argsort([sc.nb for sc in scs])
     sample = [scs[i] for i in order[::max(1, len(scs) // args.plain_sample)]]
@@ -457,7 +483,15 @@ def run_batched(args, N, torch, stream):
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                        "p99": float(np.percentile(step_ms, 99))},
         "scene_iterations_mean": float(np.mean(iters)) if iters else 0.0,
+        "scene_refine_iterations_total": int(refine_its),
         "scene_solves_converged": f"{conv}/{len(res)}",
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "the whole batched step: FP32 solve launch, FP64 refinement "
+                               "launch and collision detection",
+                     "bytes_per_step": moved / timed,
+                     "bytes_model": "compulsory bytes: FP32 iterations 248 nc + 72 nb, FP64 "
+                                    "refinement iterations 440 nc + 120 nb, per scene"},
         "graph": graph, "autotune": {"best": tune["candidates"][tune["best"]],
                                       "identical": tune["identical"]},
         "gpu_launches": int(launches),

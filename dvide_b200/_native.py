@@ -87,7 +87,8 @@ class StepStats(C.Structure):
 class SceneStats(C.Structure):
     _fields_ = [("num_contacts", C.c_int32), ("num_possible", C.c_int32),
                 ("iterations", C.c_int32), ("backtracks", C.c_int32), ("residual", C.c_double),
-                ("objective", C.c_double), ("status", C.c_int32), ("sweeps", C.c_int32)]
+                ("objective", C.c_double), ("status", C.c_int32), ("sweeps", C.c_int32),
+                ("refine_iterations", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -27,6 +27,7 @@ void to_scene_stats(const SegState& X, unsigned ew_err, dv_scene_stats* o) {
   o->residual = X.ctl.residual;
   o->objective = X.ctl.objective;
   o->sweeps = X.ctl.sweeps;
+  o->refine_iterations = X.ctl.refine_it;
   int st = status_from_bits(ew_err & (kErrBarrierTimeout | kErrCopyTimeout | kErrCapacity | kErrPartners));
   if (st == DV_OK) st = status_from_bits(X.err);
   o->status = st;

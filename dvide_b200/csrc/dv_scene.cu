@@ -170,6 +170,7 @@ DV_API int dv_apgd_solve(dv_scene* s) {
   L.residual = X.ctl.residual;
   L.objective = X.ctl.objective;
   L.sweeps = X.ctl.sweeps;
+  L.refine_iterations = X.ctl.refine_it;
   L.status = status_from_bits(X.err);
   return L.status;
 }

@@ -248,6 +248,7 @@ typedef struct dv_scene_stats {
   double objective;
   int32_t status;            /* DV_OK, DV_ERR_NAN or DV_ERR_NOCONV for this scene */
   int32_t sweeps;
+  int32_t refine_iterations; /* DV_PREC_MIXED: FP64 refinement iterations (part of iterations) */
 } dv_scene_stats;
 
 typedef struct dv_tune_candidate {

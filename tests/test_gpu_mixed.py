@@ -167,12 +167,17 @@ def test_refined_batch_equals_refined_alone(native):
            scenes.settling_box(n_side=3)]
     b = native.NativeBatch(scs, precision=1, refine_iterations=REFINE_ITERATIONS)
     b.step(10)
+    hist, _ = b.history()
     refined = 0
     for i, sc in enumerate(scs):
         g = native.NativeScene.from_scene(sc, precision=1, refine_iterations=REFINE_ITERATIONS)
-        for _ in range(10):
+        for k in range(10):
             g.step(1)
-            refined += g.stats()["refine_iterations"] > 0
+            st = g.stats()
+            refined += st["refine_iterations"] > 0
+            # the batch's per-scene report of the same step (dv_batch_step_history)
+            assert hist[k][i]["refine_iterations"] == st["refine_iterations"], (i, k)
+            assert hist[k][i]["iterations"] == st["iterations"], (i, k)
         assert np.array_equal(b.state(i)[0], g.state()[0]), i
         assert np.array_equal(b.state(i)[1], g.state()[1]), i
         assert np.array_equal(b.gamma(i), g.gamma()), i
