@@ -72,6 +72,10 @@ Engine::~Engine() {
   if (own_stream_ && st_) cudaStreamDestroy(st_);
 }
 
+static const char* const kPartnerLimitText =
+    "a sphere has more than 8192 contact partners with larger ids, or more than 256 spheres "
+    "have over 128 in one step";
+
 static int check_params(const dv_params& p) {
   if (!(p.h > 0) || !(p.envelope >= 0) || !(p.mu >= 0) || !(p.tolerance >= 0)) return DV_ERR_ARG;
   if (p.max_iterations < 0 || p.max_backtracks < 0) return DV_ERR_ARG;
@@ -219,6 +223,7 @@ int Engine::init(const std::vector<SceneInput>& scenes, int precision) {
   own_stream_ = true;
   d.precision = precision;
   TRY(dalloc(&d.ew, 1));
+  TRY(dalloc(&d.wide_ids, kWideSpheres));
   if (cudaMallocHost(&h_ew_, sizeof(EngineWords)) != cudaSuccess)
     return dv_record_cuda_error(cudaErrorMemoryAllocation, "cudaMallocHost", __FILE__, __LINE__);
   memset(h_ew_, 0, sizeof(EngineWords));
@@ -883,7 +888,7 @@ int Engine::step(int n) {
     done += failed;
     const EngineWords& w = *h_ew_;
     if (w.err & kErrPartners) {
-      dv_set_error_text("a sphere has more than 128 contact partners with larger ids");
+      dv_set_error_text(kPartnerLimitText);
       return DV_ERR_ARG;
     }
     if (w.err & (kErrBarrierTimeout | kErrCopyTimeout)) {
@@ -915,7 +920,7 @@ int Engine::collide_only() {
     TRY(sync_words());
     const EngineWords& w = *h_ew_;
     if (w.err & kErrPartners) {
-      dv_set_error_text("a sphere has more than 128 contact partners with larger ids");
+      dv_set_error_text(kPartnerLimitText);
       return DV_ERR_ARG;
     }
     if (!(w.err & kErrCapacity)) return DV_OK;

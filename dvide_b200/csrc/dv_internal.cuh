@@ -149,7 +149,13 @@ struct EngineWords {
   int act_nb;           // entries of act_bodies
   int act_base;         // segments iterating when the lists were last built (nseg before)
   int act_rebuild;      // 1: rebuild the lists before the next pass
+  int n_wide;           // spheres of this step with more partners than the warp pair kernel lists
 };
+
+// Spheres per step whose partners (larger ids) exceed the warp pair kernel's
+// list, handled by a CTA each, and the partners one such sphere may have.
+constexpr int kWideSpheres = 256;
+constexpr int kWidePartners = 8192;
 
 struct SceneDev {
   int nb = 0, nseg = 0;
@@ -185,6 +191,7 @@ struct SceneDev {
   int ncell_cap = 0;
   int* cnt_cont = nullptr;    // contacts with A = body
   int* cnt_cand = nullptr;    // candidate pairs with A = body
+  int* wide_ids = nullptr;    // kWideSpheres: the spheres of EngineWords::n_wide
   int* cbase = nullptr;       // exclusive scan of cnt_cont (nb + 1), unpadded
   int* scan_tmp = nullptr;
   size_t scan_tmp_cap = 0;

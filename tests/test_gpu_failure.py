@@ -2,6 +2,7 @@
 waits (grid barrier, bulk-copy mbarrier) are run against conditions that never
 come true and must end at their time limit with an error status the host
 reads; the device stays usable."""
+import numpy as np
 import pytest
 
 from dvide_b200 import scenes
@@ -26,18 +27,26 @@ def test_selftest_rejects_bad_limit(native):
 
 
 def test_partner_limit_reports_an_argument_error(native):
-    """The warp that lists a sphere's partners keeps at most 128 of them with
-    larger ids; a sphere with 129 is reported as DV_ERR_ARG with a message,
-    the step does nothing, and the scene stays usable."""
-    ok = native.NativeScene.from_scene(scenes.crowd(128))
+    """A sphere with more than 128 partners with larger ids is written by a CTA
+    of its own (at most 256 such spheres per step, 8,192 partners each).  A
+    crowd of 400 around one sphere has 248 such spheres and steps; one of 500
+    has 359, which is reported as DV_ERR_ARG with a message, the step does
+    nothing, and the scene stays usable."""
+    ok = native.NativeScene.from_scene(scenes.crowd(400))
     ok.step(1)
-    assert ok.stats()["num_contacts"] >= 128 and ok.stats()["status"] == 0
-    bad = native.NativeScene.from_scene(scenes.crowd(129))
+    assert ok.stats()["num_contacts"] > 60000 and ok.stats()["status"] == 0
+    bad = native.NativeScene.from_scene(scenes.crowd(500))
     p0, v0 = bad.state()
     with pytest.raises(native.DvError) as e:
         bad.step(1)
-    assert e.value.status == 1 and "128 contact partners" in str(e.value)
+    assert e.value.status == 1 and "more than 256 spheres" in str(e.value)
     p1, v1 = bad.state()
     assert (p0 == p1).all() and (v0 == v1).all()
+    # usable: moved apart, it steps
+    p2 = p0.copy()
+    p2[:, 0] += 0.2 * np.arange(len(p2))
+    bad.set_state(p2, v0)
+    bad.step(1)
+    assert bad.stats()["status"] == 0 and bad.stats()["num_contacts"] == 0
     ok.close()
     bad.close()
