@@ -74,6 +74,18 @@ def solve_bytes_mixed(nc, nb, iterations, refine_iterations, backtracks):
             + (136 * nc + 96 * nb))
 
 
+# solve_bytes_mixed summed over a served request's steps, from the sums the
+# server reports (dv_request_result).
+def request_bytes_mixed(r):
+    nb, c = r["nb"], r["contact_steps"]
+    return (248 * r["iteration_contacts"] + 72 * nb * r["iterations"]
+            + 440 * r["refine_iteration_contacts"] + 120 * nb * r["refine_iterations"]
+            + 76 * r["backtrack_contacts"] + 36 * nb * r["backtracks"]
+            + 2 * (76 * c + 36 * nb * r["solves"])
+            + 2 * (136 * r["refined_contacts"] + 60 * nb * r["refined_solves"])
+            + 136 * c + 96 * nb * r["nsteps"])
+
+
 # The same count for the kernel's own sequence: ONE Schur product per APGD
 # iteration (N y is formed from the stored products of the last two iterates),
 # i.e. 440 nc + 120 nb less one product's 136 nc + 60 nb.
@@ -590,6 +602,9 @@ def run_served(args, N, stream):
         g.close()
     plain = p_cs / (p_ms / 1e3) if p_ms > 0 else None
     served = contact_steps / wall
+    peak, peak_kind = _peaks()
+    moved = sum(request_bytes_mixed(r) for r in results)
+    achieved = moved / (st["device_ms"] / 1e3) / 1e9 if st["device_ms"] > 0 else 0.0
     return {
         "workload": (f"{n_req} requests, Poisson {args.serve_rate}/s for {args.serve_seconds} s, "
                      f"{args.serve_steps} steps each (h 1e-3), spheres log-uniform [500, 50000], "
@@ -617,6 +632,12 @@ def run_served(args, N, stream):
             "sample": f"{len(pick)} of {n_req} requests (every {max(1, n_req // args.plain_sample)}th "
                       f"by size)"},
         "speedup_vs_plain": (served / plain) if plain else None,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "every served step's device time: FP32 solve launch, FP64 "
+                               "refinement launch and collision detection",
+                     "bytes_model": "compulsory bytes of the batched line, summed per request "
+                                    "from the server's per-request solver counts"},
         "clocks": clocks,
     }
 

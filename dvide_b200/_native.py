@@ -123,7 +123,11 @@ class RequestResult(C.Structure):
                 ("solves_at_tolerance", C.c_int32), ("t_submit", C.c_double),
                 ("t_admit", C.c_double), ("t_done", C.c_double), ("contact_steps", C.c_double),
                 ("step_ms_mean", C.c_double), ("step_ms_p50", C.c_double),
-                ("step_ms_p99", C.c_double), ("bytes", C.c_double)]
+                ("step_ms_p99", C.c_double), ("bytes", C.c_double),
+                ("iterations", C.c_double), ("iteration_contacts", C.c_double),
+                ("refine_iterations", C.c_double), ("refine_iteration_contacts", C.c_double),
+                ("backtracks", C.c_double), ("backtrack_contacts", C.c_double),
+                ("refined_solves", C.c_double), ("refined_contacts", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

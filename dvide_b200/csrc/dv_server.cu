@@ -29,6 +29,7 @@ struct Request {
   int solves = 0, solves_at_tol = 0;
   double t_submit = 0, t_admit = 0, t_done = 0;
   double contact_steps = 0, bytes = 0;
+  double it = 0, it_c = 0, rit = 0, rit_c = 0, bt = 0, bt_c = 0, refined = 0, refined_c = 0;
   std::vector<float> step_ms;
   int seg = -1;  // segment index in the current engine layout
 };
@@ -171,6 +172,17 @@ struct dv_server {
         if (X.nc > 0) {
           q.solves += 1;
           if (X.ctl.residual < q.P.tolerance) q.solves_at_tol += 1;
+          const double nc = X.nc, ri = X.ctl.refine_it, i0 = X.ctl.iterations - ri;
+          q.it += i0;
+          q.it_c += i0 * nc;
+          q.rit += ri;
+          q.rit_c += ri * nc;
+          q.bt += X.ctl.backtracks;
+          q.bt_c += X.ctl.backtracks * nc;
+          if (ri > 0) {
+            q.refined += 1;
+            q.refined_c += nc;
+          }
         }
         q.step_ms.push_back(rec.ms_total);
         if (q.status == DV_OK) q.status = status_from_bits(X.err);
@@ -201,6 +213,14 @@ struct dv_server {
       o.t_admit = q.t_admit;
       o.t_done = q.t_done;
       o.contact_steps = q.contact_steps;
+      o.iterations = q.it;
+      o.iteration_contacts = q.it_c;
+      o.refine_iterations = q.rit;
+      o.refine_iteration_contacts = q.rit_c;
+      o.backtracks = q.bt;
+      o.backtrack_contacts = q.bt_c;
+      o.refined_solves = q.refined;
+      o.refined_contacts = q.refined_c;
       double sum = 0;
       for (float m : q.step_ms) sum += m;
       o.step_ms_mean = q.step_ms.empty() ? 0.0 : sum / q.step_ms.size();

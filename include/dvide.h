@@ -342,6 +342,15 @@ typedef struct dv_request_result {
   double contact_steps;      /* contacts summed over its steps */
   double step_ms_mean, step_ms_p50, step_ms_p99;  /* device time of the steps it took part in */
   double bytes;              /* admission estimate */
+  /* Solver work summed over its steps (for byte models): iterations in the
+   * solve's working precision (FP32 under DV_PREC_MIXED, FP64 refinement
+   * iterations counted apart), refinement iterations, backtracks, each also
+   * weighted by the step's contacts; the contacts and count of its refined
+   * solves. */
+  double iterations, iteration_contacts;
+  double refine_iterations, refine_iteration_contacts;
+  double backtracks, backtrack_contacts;
+  double refined_solves, refined_contacts;
 } dv_request_result;
 
 typedef struct dv_server_stats {

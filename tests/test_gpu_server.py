@@ -30,6 +30,33 @@ def _alone(native, sc, nsteps, precision, **kw):
     return p, v
 
 
+def _work_alone(native, sc, nsteps, precision, **kw):
+    """The solver-work sums a served request reports, from the scene stepped
+    alone (per-step history)."""
+    g = native.NativeScene.from_scene(sc, precision=precision, **kw)
+    g.step(nsteps)
+    h = g.history(clear=True)
+    g.close()
+    w = dict.fromkeys(("iterations", "iteration_contacts", "refine_iterations",
+                       "refine_iteration_contacts", "backtracks", "backtrack_contacts",
+                       "refined_solves", "refined_contacts"), 0.0)
+    for x in h:
+        nc = x["num_contacts"]
+        if nc == 0:
+            continue
+        ri, it = x["refine_iterations"], x["iterations"] - x["refine_iterations"]
+        w["iterations"] += it
+        w["iteration_contacts"] += it * nc
+        w["refine_iterations"] += ri
+        w["refine_iteration_contacts"] += ri * nc
+        w["backtracks"] += x["backtracks"]
+        w["backtrack_contacts"] += x["backtracks"] * nc
+        if ri > 0:
+            w["refined_solves"] += 1
+            w["refined_contacts"] += nc
+    return w
+
+
 def _serve(native, reqs, precision, budget=150e9, max_active=4096, steps_per_round=3,
            max_bodies=0, **kw):
     srv = native.NativeServer(precision=precision, hbm_budget_bytes=budget, max_active=max_active,
@@ -74,6 +101,11 @@ def test_served_results_equal_alone(native, precision, refine):
         p, v = _alone(native, reqs[i][0], reqs[i][1], precision, **kw)
         ps, vs = states[i]
         assert np.array_equal(ps, p) and np.array_equal(vs, v), i
+        w = _work_alone(native, reqs[i][0], reqs[i][1], precision, **kw)
+        for key, val in w.items():
+            assert res[key] == val, (i, key)
+    if refine:
+        assert sum(results[rid]["refined_solves"] for _, rid in ids) > 0
 
 
 def test_served_ragged_requests_equal_alone(native):
