@@ -17,12 +17,13 @@ DRIVER = os.path.join(ROOT, "dvide_b200", "drivers", "settle")
 pytestmark = pytest.mark.gpu
 
 
-def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start):
+def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start, solver=1):
     """The driver's scene (settle_initial.txt) with the driver's settings
     (System defaults: mu 0.25, envelope 1e-3; h 1e-3, gravity -z) in the oracle."""
     b = np.loadtxt(tmp_path / "settle_initial.txt")
     params = scenes.default_params(h=1e-3, gravity=(0.0, 0.0, -9.81), tolerance=tolerance,
-                                   max_iterations=max_iterations, warm_start=warm_start)
+                                   max_iterations=max_iterations, warm_start=warm_start,
+                                   solver=solver)
     sc = scenes.Scene(b[:, 0:3].copy(), b[:, 3:6].copy(), b[:, 6].copy(), b[:, 7:10].copy(),
                       b[:, 10].astype(np.int32), np.full(len(b), -1, dtype=np.int32), params,
                       "settle_driver")
@@ -66,7 +67,10 @@ def test_unsupported_solver_type_reports(tmp_path):
 @pytest.mark.parametrize("args", [["5", "1e-3", "2000"], ["6", "1e-4", "3000"],
                                   ["1", "1e-4", "1000", "2"]],
                          ids=["pgj", "pgs", "apgd_matched_warm_start"])
-def test_settle_driver_other_solver_forms(tmp_path, args):
+def test_settle_driver_other_solver_forms(tmp_path, oracle_mod, args):
+    """System(5) (PGJ), System(6) (PGS) and APGD with the warm start matched by
+    contact pair, through the C++ layer: the oracle's trajectory, bit for bit.
+    The System passes warm_start 0 to PGJ and PGS, which start from (1, 0, 0)."""
     out = subprocess.run([DRIVER, "120", *args], cwd=tmp_path, capture_output=True, text=True,
                          timeout=300)
     assert out.returncode == 0, out.stderr
@@ -75,6 +79,15 @@ def test_settle_driver_other_solver_forms(tmp_path, args):
     last = [float(x) for x in lines[-1].split(",")]
     assert last[1] > 100
     assert all(np.isfinite(float(x)) for x in lines[-1].split(","))
+    solver = int(args[0])
+    warm = int(args[3]) if len(args) > 3 else (1 if solver == 1 else 0)
+    o, per_step = _replay(oracle_mod, tmp_path, 120, float(args[1]), int(args[2]), warm,
+                          solver=solver)
+    driver = [(int(l.split(",")[1]), int(l.split(",")[2])) for l in lines]
+    assert driver == per_step
+    final = np.loadtxt(tmp_path / "settle_final_full.txt")
+    p, v = o.state()
+    assert np.array_equal(final[:, 0:3], p) and np.array_equal(final[:, 3:6], v)
 
 
 
