@@ -17,7 +17,8 @@ DRIVER = os.path.join(ROOT, "dvide_b200", "drivers", "settle")
 pytestmark = pytest.mark.gpu
 
 
-def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start, solver=1):
+def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start, solver=1,
+            rows=()):
     """The driver's scene (settle_initial.txt) with the driver's settings
     (System defaults: mu 0.25, envelope 1e-3; h 1e-3, gravity -z) in the oracle."""
     b = np.loadtxt(tmp_path / "settle_initial.txt")
@@ -28,6 +29,8 @@ def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start, 
                       b[:, 10].astype(np.int32), np.full(len(b), -1, dtype=np.int32), params,
                       "settle_driver")
     o = oracle_mod.OracleScene(sc)
+    for row in rows:
+        o.add_bilateral(*row)
     per_step = []
     for _ in range(steps):
         o.step(1)
@@ -91,10 +94,10 @@ def test_settle_driver_other_solver_forms(tmp_path, oracle_mod, args):
 
 
 
-def test_settle_driver_with_pinned_spheres(tmp_path):
+def test_settle_driver_with_pinned_spheres(tmp_path, oracle_mod):
     """System::addBilateralConstraintDOF through the C++ layer: the x and y
     DOFs of a column of 10 spheres stay where they started while the pile
-    settles around them."""
+    settles around them, and the run is the oracle's with the same rows."""
     out = subprocess.run([DRIVER, "120", "1", "1e-4", "1000", "1", "10"], cwd=tmp_path,
                          capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
@@ -103,6 +106,14 @@ def test_settle_driver_with_pinned_spheres(tmp_path):
     drift = [l for l in out.stdout.splitlines() if l.startswith("pinned drift:")]
     assert len(drift) == 1
     assert float(drift[0].split(":")[1]) < 1e-5
+    # the oracle with the same rows (x, then y, of spheres 5..14), bit for bit
+    rows = [(3 * (5 + i) + k, -1) for i in range(10) for k in range(2)]
+    o, per_step = _replay(oracle_mod, tmp_path, 120, 1e-4, 1000, 1, rows=rows)
+    driver = [(int(l.split(",")[1]), int(l.split(",")[2])) for l in lines]
+    assert driver == per_step
+    final = np.loadtxt(tmp_path / "settle_final_full.txt")
+    p, v = o.state()
+    assert np.array_equal(final[:, 0:3], p) and np.array_equal(final[:, 3:6], v)
 
 
 def _mm(path):
