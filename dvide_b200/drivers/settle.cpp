@@ -3,7 +3,7 @@
 // spheres (r = 0.05 m, rho = 2600) on a 10x10x10 lattice in an open box of
 // five fixed boxes, mu = 0.25, h = 1e-3, APGD with warm start.
 // Usage: settle <steps> <solverType> <tolerance> [maxIterations] [warmStartMode]
-//               [pinnedSpheres]
+//               [pinnedSpheres] [antiRelaxation]
 // Prints one line per step: time, contacts, iterations, weight carried by
 // the fixed boxes, and the four CCP violations.  With pinnedSpheres = n > 0
 // the x and y DOFs of the first n spheres are held by bilateral constraints
@@ -11,7 +11,8 @@
 // the largest drift of those DOFs is printed at the end.  The bodies as built
 // (settle_initial.txt) and the final positions and velocities
 // (settle_final_full.txt) are written at full precision, so that the run can
-// be replayed and compared elsewhere.
+// be replayed and compared elsewhere.  antiRelaxation = 1 turns on APGD's
+// anti-relaxation (APGD::setAntiRelaxation).
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -35,6 +36,7 @@ int main(int argc, char** argv) {
   int maxIterations = argc > 4 ? atoi(argv[4]) : 1000;
   int warmStartMode = argc > 5 ? atoi(argv[5]) : 1;
   int pinned = argc > 6 ? atoi(argv[6]) : 0;
+  int antiRelaxation = argc > 7 ? atoi(argv[7]) : 0;
 
   System* sys = new System(solverType);
   sys->setTimeStep(1e-3);
@@ -42,7 +44,10 @@ int main(int argc, char** argv) {
   sys->solver->tolerance = tolerance;
   sys->solver->maxIterations = maxIterations;
   sys->collisionDetector->setBinsPerAxis(make_uint3(10, 10, 10));
-  if (solverType == 1) dynamic_cast<APGD*>(sys->solver)->setWarmStarting(warmStartMode);
+  if (solverType == 1) {
+    dynamic_cast<APGD*>(sys->solver)->setWarmStarting(warmStartMode);
+    if (antiRelaxation) dynamic_cast<APGD*>(sys->solver)->setAntiRelaxation(true);
+  }
 
   const double t = 0.05, inner = 0.6, H = 0.75;
   double3 c[5] = {make_double3(0, 0, -t), make_double3(-inner - t, 0, H), make_double3(inner + t, 0, H),

@@ -18,13 +18,13 @@ pytestmark = pytest.mark.gpu
 
 
 def _replay(oracle_mod, tmp_path, steps, tolerance, max_iterations, warm_start, solver=1,
-            rows=()):
+            rows=(), anti_relaxation=0):
     """The driver's scene (settle_initial.txt) with the driver's settings
     (System defaults: mu 0.25, envelope 1e-3; h 1e-3, gravity -z) in the oracle."""
     b = np.loadtxt(tmp_path / "settle_initial.txt")
     params = scenes.default_params(h=1e-3, gravity=(0.0, 0.0, -9.81), tolerance=tolerance,
                                    max_iterations=max_iterations, warm_start=warm_start,
-                                   solver=solver)
+                                   solver=solver, anti_relaxation=anti_relaxation)
     sc = scenes.Scene(b[:, 0:3].copy(), b[:, 3:6].copy(), b[:, 6].copy(), b[:, 7:10].copy(),
                       b[:, 10].astype(np.int32), np.full(len(b), -1, dtype=np.int32), params,
                       "settle_driver")
@@ -111,6 +111,23 @@ def test_settle_driver_with_pinned_spheres(tmp_path, oracle_mod):
     o, per_step = _replay(oracle_mod, tmp_path, 120, 1e-4, 1000, 1, rows=rows)
     driver = [(int(l.split(",")[1]), int(l.split(",")[2])) for l in lines]
     assert driver == per_step
+    final = np.loadtxt(tmp_path / "settle_final_full.txt")
+    p, v = o.state()
+    assert np.array_equal(final[:, 0:3], p) and np.array_equal(final[:, 3:6], v)
+
+
+def test_settle_driver_anti_relaxation(tmp_path, oracle_mod):
+    """APGD::setAntiRelaxation through the C++ layer: the oracle's trajectory
+    with anti-relaxation, bit for bit."""
+    out = subprocess.run([DRIVER, "80", "1", "1e-4", "1000", "1", "0", "1"], cwd=tmp_path,
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [l for l in out.stdout.splitlines() if l and l[0].isdigit()]
+    assert len(lines) == 80
+    o, per_step = _replay(oracle_mod, tmp_path, 80, 1e-4, 1000, 1, anti_relaxation=1)
+    driver = [(int(l.split(",")[1]), int(l.split(",")[2])) for l in lines]
+    assert driver == per_step
+    assert max(c for c, _ in per_step) > 100
     final = np.loadtxt(tmp_path / "settle_final_full.txt")
     p, v = o.state()
     assert np.array_equal(final[:, 0:3], p) and np.array_equal(final[:, 3:6], v)
