@@ -464,98 +464,101 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
 }
 
 // The write pass for the spheres the count pass listed in wide_ids (more than
-// kMaxPerBody partners with larger ids): one CTA per sphere scans the same 27
-// cells and box list, keeps the partners in shared memory (at most
-// kWidePartners), sorts them by id (bitonic) and writes the contacts at the
-// sphere's slot in (A, B) order -- the same contacts, in the same order, as
-// the warp kernel writes for a sphere with fewer partners.
+// kMaxPerBody partners with larger ids): each CTA takes listed spheres in turn;
+// for each it scans the same 27 cells and box list, keeps the partners in
+// shared memory (at most kWidePartners), sorts them by id (bitonic) and writes
+// the contacts at the sphere's slot in (A, B) order -- the same contacts, in
+// the same order, as the warp kernel writes for a sphere with fewer partners.
 __global__ void __launch_bounds__(kThreads) k_sphere_pairs_wide(CollideArgs a) {
   __shared__ int s_ids[kWidePartners];
   __shared__ int s_beg[28], s_off[29];
   __shared__ int s_n;
   if (a.ew->err) return;
-  if ((int)blockIdx.x >= min(a.ew->n_wide, kWideSpheres)) return;
-  const int A = a.wide_ids[blockIdx.x];
-  const int sg = a.bseg[A];
-  const SegParams& P = a.seg[sg];
-  const double env = P.env;
-  const bool exact = P.exact != 0;
-  // ranges 0..26: the neighbour cells (as the warp kernel's lanes); 27: boxes
-  if (threadIdx.x < 28) {
-    const int r = threadIdx.x;
-    int beg = 0, len = 0;
-    if (r < 27) {
-      const int4 cA = a.cell[A];
-      const int x = cA.x + (r % 3) - 1, y = cA.y + ((r / 3) % 3) - 1, z = cA.z + (r / 9) - 1;
-      const GridInfo* g = a.grid + sg;
-      if (x >= 0 && y >= 0 && z >= 0 && x < g->dx && y < g->dy && z < g->dz) {
-        const int id = P.cell_base + x + g->dx * (y + g->dy * z);
-        const int cs = a.cstart[id];
-        if (cs >= 0) {
-          beg = cs;
-          len = a.cend[id] - cs;
-        }
-      }
-    } else {
-      beg = P.l0;
-      len = P.l1 - P.l0;
-    }
-    s_beg[r] = beg;
-    s_off[r + 1] = len;
-  }
-  if (threadIdx.x == 0) s_n = 0;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_off[0] = 0;
-    for (int r = 0; r < 28; ++r) s_off[r + 1] += s_off[r];
-  }
-  __syncthreads();
-  const int total = s_off[28];
-  for (int f = threadIdx.x; f < total; f += kThreads) {
-    int r = 0;
-    while (r < 27 && s_off[r + 1] <= f) ++r;
-    const int at = s_beg[r] + (f - s_off[r]);
-    const int B = r < 27 ? (int)a.sorted_bodies[at] : a.large_ids[at];
-    if (B <= A) continue;
-    if (!is_candidate(a.amin, a.amax, a.fam, A, B)) continue;
-    NpOut o;
-    if (narrowphase(a.p4, a.g4, A, B, env, exact, &o)) {
-      const int slot = atomicAdd(&s_n, 1);
-      if (slot < kWidePartners) s_ids[slot] = B;
-    }
-  }
-  __syncthreads();
-  const int n = s_n;
-  if (n != a.cnt_cont[A] || n > kWidePartners) {
-    // not the count pass's partners (cannot happen: same tests, same order)
-    if (threadIdx.x == 0) atomicOr(&a.ew->err, kErrPartners);
-    return;
-  }
-  int m = 1;
-  while (m < n) m <<= 1;
-  for (int i = n + threadIdx.x; i < m; i += kThreads) s_ids[i] = 0x7fffffff;
-  __syncthreads();
-  for (int k = 2; k <= m; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < m; i += kThreads) {
-        const int l = i ^ j;
-        if (l > i) {
-          const int x = s_ids[i], y = s_ids[l];
-          if ((x > y) == ((i & k) == 0)) {
-            s_ids[i] = y;
-            s_ids[l] = x;
+  const int nw = min(a.ew->n_wide, kWideSpheres);
+  for (int w = blockIdx.x; w < nw; w += gridDim.x) {
+    __syncthreads();  // the previous sphere's reads of the shared arrays are done
+    const int A = a.wide_ids[w];
+    const int sg = a.bseg[A];
+    const SegParams& P = a.seg[sg];
+    const double env = P.env;
+    const bool exact = P.exact != 0;
+    // ranges 0..26: the neighbour cells (as the warp kernel's lanes); 27: boxes
+    if (threadIdx.x < 28) {
+      const int r = threadIdx.x;
+      int beg = 0, len = 0;
+      if (r < 27) {
+        const int4 cA = a.cell[A];
+        const int x = cA.x + (r % 3) - 1, y = cA.y + ((r / 3) % 3) - 1, z = cA.z + (r / 9) - 1;
+        const GridInfo* g = a.grid + sg;
+        if (x >= 0 && y >= 0 && z >= 0 && x < g->dx && y < g->dy && z < g->dz) {
+          const int id = P.cell_base + x + g->dx * (y + g->dy * z);
+          const int cs = a.cstart[id];
+          if (cs >= 0) {
+            beg = cs;
+            len = a.cend[id] - cs;
           }
         }
+      } else {
+        beg = P.l0;
+        len = P.l1 - P.l0;
       }
-      __syncthreads();
+      s_beg[r] = beg;
+      s_off[r + 1] = len;
     }
-  }
-  const size_t base = (size_t)(a.cbase[A] + a.sst[sg].delta);
-  for (int e = threadIdx.x; e < n; e += kThreads) {
-    const int B = s_ids[e];
-    NpOut o;
-    narrowphase(a.p4, a.g4, A, B, env, exact, &o);
-    write_contact(a, base + e, A, B, o, exact);
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_off[0] = 0;
+      for (int r = 0; r < 28; ++r) s_off[r + 1] += s_off[r];
+    }
+    __syncthreads();
+    const int total = s_off[28];
+    for (int f = threadIdx.x; f < total; f += kThreads) {
+      int r = 0;
+      while (r < 27 && s_off[r + 1] <= f) ++r;
+      const int at = s_beg[r] + (f - s_off[r]);
+      const int B = r < 27 ? (int)a.sorted_bodies[at] : a.large_ids[at];
+      if (B <= A) continue;
+      if (!is_candidate(a.amin, a.amax, a.fam, A, B)) continue;
+      NpOut o;
+      if (narrowphase(a.p4, a.g4, A, B, env, exact, &o)) {
+        const int slot = atomicAdd(&s_n, 1);
+        if (slot < kWidePartners) s_ids[slot] = B;
+      }
+    }
+    __syncthreads();
+    const int n = s_n;
+    if (n != a.cnt_cont[A] || n > kWidePartners) {
+      // not the count pass's partners (cannot happen: same tests, same order)
+      if (threadIdx.x == 0) atomicOr(&a.ew->err, kErrPartners);
+      return;
+    }
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = n + threadIdx.x; i < m; i += kThreads) s_ids[i] = 0x7fffffff;
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < m; i += kThreads) {
+          const int l = i ^ j;
+          if (l > i) {
+            const int x = s_ids[i], y = s_ids[l];
+            if ((x > y) == ((i & k) == 0)) {
+              s_ids[i] = y;
+              s_ids[l] = x;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    const size_t base = (size_t)(a.cbase[A] + a.sst[sg].delta);
+    for (int e = threadIdx.x; e < n; e += kThreads) {
+      const int B = s_ids[e];
+      NpOut o;
+      narrowphase(a.p4, a.g4, A, B, env, exact, &o);
+      write_contact(a, base + e, A, B, o, exact);
+    }
   }
 }
 
@@ -850,7 +853,7 @@ void collide(SceneDev& sd, cudaStream_t st, int64_t* launches) {
   *launches += 2;
   if (sd.n_small > 0) {
     k_sphere_pairs<true><<<pair_blocks, kThreads, 0, st>>>(a);
-    k_sphere_pairs_wide<<<kWideSpheres, kThreads, 0, st>>>(a);
+    k_sphere_pairs_wide<<<kWideGrid, kThreads, 0, st>>>(a);
     *launches += 2;
   }
   if (sd.n_large > 0) {

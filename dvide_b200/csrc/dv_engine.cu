@@ -73,7 +73,7 @@ Engine::~Engine() {
 }
 
 static const char* const kPartnerLimitText =
-    "a sphere has more than 8192 contact partners with larger ids, or more than 256 spheres "
+    "a sphere has more than 8192 contact partners with larger ids, or more than 65536 spheres "
     "have over 128 in one step";
 
 static int check_params(const dv_params& p) {

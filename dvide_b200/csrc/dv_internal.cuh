@@ -153,8 +153,10 @@ struct EngineWords {
 };
 
 // Spheres per step whose partners (larger ids) exceed the warp pair kernel's
-// list, handled by a CTA each, and the partners one such sphere may have.
-constexpr int kWideSpheres = 256;
+// list, the CTAs that take them in turn, and the partners one such sphere may
+// have.
+constexpr int kWideSpheres = 65536;
+constexpr int kWideGrid = 256;
 constexpr int kWidePartners = 8192;
 
 struct SceneDev {

@@ -286,6 +286,35 @@ def crowd(n_around, seed=5, radius=0.05, max_iterations=50) -> Scene:
                      f"crowd_{n_around}")
 
 
+def raspberry(n, big=1.0, small=0.015, overlap=5e-4, ballast=0, max_iterations=50) -> Scene:
+    """One sphere of radius `big` (body 0) with n spheres of radius `small` on
+    its surface (a Fibonacci lattice, each overlapping it by `overlap`), in
+    free space without gravity: body 0 has n contact partners, all with
+    larger ids; the small spheres are too far apart to touch one another.
+    With ballast = m > 0, m spheres of radius big / 3 on a lattice 1 m apart,
+    20 m away and touching nothing, raise the median radius so that the big
+    sphere goes through the uniform grid and the sphere pair kernels (a
+    sphere above four times the median radius is paired against every body
+    of its scene instead)."""
+    i = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * i / n
+    rho = np.sqrt(1.0 - z * z)
+    phi = i * math.pi * (3.0 - math.sqrt(5.0))
+    d = big + small - overlap
+    pos = [np.zeros((1, 3)), d * np.stack([rho * np.cos(phi), rho * np.sin(phi), z], axis=1)]
+    r = [np.array([big]), np.full(n, small)]
+    if ballast:
+        k = int(math.ceil(ballast ** (1.0 / 3.0)))
+        g = np.stack(np.meshgrid(np.arange(k), np.arange(k), np.arange(k), indexing="ij"),
+                     axis=-1).reshape(-1, 3)[:ballast]
+        pos.append(20.0 + g.astype(np.float64))
+        r.append(np.full(ballast, big / 3.0))
+    pos = np.concatenate(pos)
+    r = np.concatenate(r)
+    params = default_params(gravity=(0.0, 0.0, 0.0), max_iterations=max_iterations)
+    return _assemble([], pos, r, 2600.0, params, f"raspberry_{n}")
+
+
 def bilateral_cluster(seed, n=64, warm_start=1, h=1e-3, max_iterations=400,
                       tolerance=1e-6) -> Scene:
     """random_cluster with bilateral rows (System::addBilateralConstraintDOF,

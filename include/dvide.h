@@ -117,8 +117,8 @@ DV_API int dv_scene_set_stream(dv_scene* s, void* cuda_stream);
 DV_API int dv_set_params(dv_scene* s, const dv_params* params);
 
 /* System::DoTimeStep (System.cu:544-602), nsteps times.  DV_ERR_ARG (with
- * dv_last_error's text) when a step has more than 256 spheres with over 128
- * contact partners of larger id, or a sphere with more than 8192; that step
+ * dv_last_error's text) when a sphere has more than 8192 contact partners of
+ * larger id, or more than 65536 spheres have over 128 in one step; that step
  * leaves the state as it was. */
 DV_API int dv_step(dv_scene* s, int32_t nsteps);
 

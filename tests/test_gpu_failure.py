@@ -27,24 +27,25 @@ def test_selftest_rejects_bad_limit(native):
 
 
 def test_partner_limit_reports_an_argument_error(native):
-    """A sphere with more than 128 partners with larger ids is written by a CTA
-    of its own (at most 256 such spheres per step, 8,192 partners each).  A
-    crowd of 400 around one sphere has 248 such spheres and steps; one of 500
-    has 359, which is reported as DV_ERR_ARG with a message, the step does
-    nothing, and the scene stays usable."""
-    ok = native.NativeScene.from_scene(scenes.crowd(400))
+    """A gridded sphere with more than 128 partners with larger ids is
+    written by the wide pair kernel, which keeps at most 8,192 partners of one
+    sphere.  A sphere with 8,192 small ones on its surface steps; with 8,193
+    the step is reported as DV_ERR_ARG with a message, does nothing, and the
+    scene stays usable.  (The ballast makes the big sphere a gridded one; see
+    scenes.raspberry.)"""
+    ok = native.NativeScene.from_scene(scenes.raspberry(8192, ballast=8200))
     ok.step(1)
-    assert ok.stats()["num_contacts"] > 60000 and ok.stats()["status"] == 0
-    bad = native.NativeScene.from_scene(scenes.crowd(500))
+    assert ok.stats()["num_contacts"] == 8192 and ok.stats()["status"] == 0
+    bad = native.NativeScene.from_scene(scenes.raspberry(8193, ballast=8200))
     p0, v0 = bad.state()
     with pytest.raises(native.DvError) as e:
         bad.step(1)
-    assert e.value.status == 1 and "more than 256 spheres" in str(e.value)
+    assert e.value.status == 1 and "8192 contact partners" in str(e.value)
     p1, v1 = bad.state()
     assert (p0 == p1).all() and (v0 == v1).all()
-    # usable: moved apart, it steps
+    # usable: the small spheres moved away, it steps
     p2 = p0.copy()
-    p2[:, 0] += 0.2 * np.arange(len(p2))
+    p2[1:] *= 1.5
     bad.set_state(p2, v0)
     bad.step(1)
     assert bad.stats()["status"] == 0 and bad.stats()["num_contacts"] == 0

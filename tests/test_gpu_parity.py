@@ -246,14 +246,14 @@ def _free_running(native, oracle_mod, sc, steps):
     return o.stats()
 
 
-@pytest.mark.parametrize("n_around", [9, 16, 17, 40, 128, 129, 200, 400])
+@pytest.mark.parametrize("n_around", [9, 16, 17, 40, 128, 129, 200, 400, 500])
 def test_crowd_many_contacts_per_body_free_running(native, oracle_mod, n_around):
     """One free sphere overlapped by n_around others, which overlap many of
     each other too: body gathers walk from a few to hundreds of incidence
     entries (sixteen per load group, q in two halves of eight, ragged ends),
     and from 129 on, spheres with more than 128 partners with larger ids
-    have their contacts written by k_sphere_pairs_wide (1, 59 and 248 such
-    spheres for 129, 200 and 400).
+    have their contacts written by k_sphere_pairs_wide (1, 59, 248 and 359
+    such spheres for 129, 200, 400 and 500; its 256 CTAs take them in turn).
     Bit-identical to the oracle over three steps while the crowd flies apart:
     the first step's solve runs its 50 iterations, and by the third step few
     pairs are still in contact."""
@@ -267,6 +267,27 @@ def test_crowd_many_contacts_per_body_free_running(native, oracle_mod, n_around)
     g.close()
     st = _free_running(native, oracle_mod, sc, 3)
     assert st["num_contacts"] < ga.size // 100 + 1
+
+
+@pytest.mark.parametrize("n,ballast", [(8192, 8200), (8193, 0)], ids=["gridded", "large"])
+def test_raspberry_many_partners_free_running(native, oracle_mod, n, ballast):
+    """One sphere with n small ones on its surface.  Gridded (the ballast
+    raises the median radius), its 8,192 partners are the most the wide pair
+    kernel keeps for one sphere: a full 8,192-entry bitonic sort.  Without
+    ballast it is above four times the median radius and is paired against
+    every body of the scene, with no partner limit.  Either way the contact
+    list and the first step (a 5-iteration solve) are bit-identical to the
+    oracle.  (On the next step every contact separates; with 8,193 spheres on
+    the every-body path the reference's APGD then ends that solve on a
+    non-finite objective, in the oracle as on the GPU.)"""
+    sc = scenes.raspberry(n, ballast=ballast)
+    g, o = _pair(native, oracle_mod, sc)
+    g.collide()
+    o.collide()
+    assert _compare_contacts(g, o) == n
+    g.close()
+    st = _free_running(native, oracle_mod, sc, 1)
+    assert st["num_contacts"] == n and st["iterations"] > 0
 
 
 def test_driver_moved_wall_free_running(native, oracle_mod):
