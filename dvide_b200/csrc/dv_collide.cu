@@ -423,8 +423,12 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs(CollideArgs a) {
       // more partners than this kernel lists: k_sphere_pairs_wide writes them
       if (ncont > kMaxPerBody) {
         const int k = atomicAdd(&a.ew->n_wide, 1);
-        if (k < kWideSpheres && ncont <= kWidePartners) a.wide_ids[k] = A;
-        else atomicOr(&a.ew->err, kErrPartners);
+        if (k < kWideSpheres && ncont <= kWidePartners) {
+          a.wide_ids[k] = A;
+        } else {
+          atomicOr(&a.ew->err, kErrPartners);
+          atomicOr(&a.sst[sg].err, kErrPartners);  // whose scene (a server retires it)
+        }
       }
       if (ncand) {
         atomicAdd(&a.sst[sg].npossible, ncand);
@@ -530,7 +534,10 @@ __global__ void __launch_bounds__(kThreads) k_sphere_pairs_wide(CollideArgs a) {
     const int n = s_n;
     if (n != a.cnt_cont[A] || n > kWidePartners) {
       // not the count pass's partners (cannot happen: same tests, same order)
-      if (threadIdx.x == 0) atomicOr(&a.ew->err, kErrPartners);
+      if (threadIdx.x == 0) {
+        atomicOr(&a.ew->err, kErrPartners);
+        atomicOr(&a.sst[sg].err, kErrPartners);
+      }
       return;
     }
     int m = 1;

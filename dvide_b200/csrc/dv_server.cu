@@ -27,6 +27,7 @@ struct Request {
   dv_params P{};
   int nsteps = 0, done = 0, status = DV_OK, rounds = 0;
   int solves = 0, solves_at_tol = 0;
+  bool failed = false;  // its scene made a step fail for every scene: retired early
   double t_submit = 0, t_admit = 0, t_done = 0;
   double contact_steps = 0, bytes = 0;
   double it = 0, it_c = 0, rit = 0, rit_c = 0, bt = 0, bt_c = 0, refined = 0, refined_c = 0;
@@ -159,7 +160,21 @@ struct dv_server {
     for (auto& r : active) k = std::min(k, r->nsteps - r->done);
     k = std::max(k, 1);
     int rc = E->step(k);
-    if (rc != DV_OK) return rc;
+    if (rc == DV_ERR_ARG) {
+      // a scene over the pair kernels' partner limits fails the step for every
+      // scene: retire the requests whose scenes did it (with DV_ERR_ARG and
+      // the steps done before), and serve the others from the next round
+      bool any = false;
+      for (auto& r : active)
+        if (E->seg_state(r->seg).err & kErrPartners) {
+          r->failed = true;
+          r->status = DV_ERR_ARG;
+          any = true;
+        }
+      if (!any) return rc;
+    } else if (rc != DV_OK) {
+      return rc;
+    }
     const std::vector<StepRecord>& R = E->records();
     for (const StepRecord& rec : R) {
       st.steps += 1;
@@ -195,7 +210,7 @@ struct dv_server {
       Request& q = *r;
       q.done += (int)R.size();
       q.rounds += 1;
-      if (q.done < q.nsteps) {
+      if (q.done < q.nsteps && !q.failed) {
         stay.push_back(std::move(r));
         continue;
       }
@@ -204,7 +219,7 @@ struct dv_server {
       memset(&o, 0, sizeof(o));
       o.id = q.id;
       o.nb = (int)q.bodies.size();
-      o.nsteps = q.nsteps;
+      o.nsteps = q.done;
       o.status = q.status;
       o.rounds = q.rounds;
       o.solves = q.solves;

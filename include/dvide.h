@@ -333,8 +333,10 @@ typedef struct dv_server_config {
 typedef struct dv_request_result {
   int64_t id;
   int32_t nb;
-  int32_t nsteps;
-  int32_t status;            /* first solver error of the scene, DV_OK otherwise */
+  int32_t nsteps;            /* steps done: the steps asked for, unless retired early */
+  int32_t status;            /* first solver error of the scene, DV_OK otherwise; DV_ERR_ARG
+                                when its scene went over the pair kernels' partner limits
+                                (dv_step): retired at once, the others served on */
   int32_t rounds;
   int32_t solves;            /* its steps that solved (contacts or rows present) */
   int32_t solves_at_tolerance; /* ... whose solve ended below the solver tolerance */

@@ -131,6 +131,27 @@ def test_served_ragged_requests_equal_alone(native):
             assert res["solves"] == 0, i
 
 
+def test_request_over_the_partner_limit_is_retired_alone(native):
+    """A request whose scene goes over the pair kernels' partner limit (a
+    gridded sphere with 8,193 partners, scenes.raspberry) fails the step for
+    every resident scene; the server retires that request with DV_ERR_ARG and
+    no steps done, and the others are served to the end, each equal to the
+    scene stepped alone."""
+    reqs = [(scenes.random_cluster(0, n=40), 6), (scenes.raspberry(8193, ballast=8200), 4),
+            (scenes.ball_on_ground(h=1e-3), 9)]
+    ids, results, states, st, _ = _serve(native, reqs, 0)
+    assert st["completed"] == len(reqs)
+    for i, rid in ids:
+        res = results[rid]
+        if i == 1:
+            assert res["status"] == 1 and res["nsteps"] == 0
+            continue
+        assert res["status"] == 0 and res["nsteps"] == reqs[i][1]
+        p, v = _alone(native, reqs[i][0], reqs[i][1], 0)
+        ps, vs = states[i]
+        assert np.array_equal(ps, p) and np.array_equal(vs, v), i
+
+
 def test_budget_limits_residency(native):
     reqs = _requests()
     nb_max = max(sc.nb for sc, _ in reqs)
