@@ -639,6 +639,29 @@ __device__ inline V gather_q(const K& a, const V* q, int s, int e) {
   return r;
 }
 
+// gather_q with the run's first eight entries already loaded (c0; zero past
+// the run): entries 8..15 load alongside the first group's q.  The same sums
+// in the same order.
+template <class T, class V, class K>
+__device__ inline V gather_q_pre(const K& a, const V* q, int s, int e, const uint32_t* c0) {
+  T ax = T(0), ay = T(0), az = T(0);
+  uint32_t c1[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c1[j] = (s + 8 + j < e) ? __ldg(a.inc + s + 8 + j) : 0u;
+  add_q8<T, V>(q, c0, e - s, ax, ay, az);
+  if (s + 8 < e) add_q8<T, V>(q, c1, e - s - 8, ax, ay, az);
+  for (int i = s + 16; i < e; i += 16) {
+    uint32_t c[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) c[j] = (i + j < e) ? __ldg(a.inc + i + j) : 0u;
+    add_q8<T, V>(q, c, e - i, ax, ay, az);
+    if (i + 8 < e) add_q8<T, V>(q, c + 8, e - i - 8, ax, ay, az);
+  }
+  V r;
+  r.x = ax; r.y = ay; r.z = az; r.w = T(0);
+  return r;
+}
+
 template <class T, class V, class K>
 __device__ inline V gather_q(const K& a, const V* q, int b) {
   return gather_q<T, V>(a, q, __ldg(a.inc_start + b), __ldg(a.inc_start + b + 1));
@@ -760,14 +783,17 @@ __device__ inline BodyHead body_head(const K& a, int b) {
   return h;
 }
 
-template <class T, bool kAR = false>
-__device__ inline void body_w(const KArgs<T>& a, int b, const BodyHead& h) {
+// kPre: c0 holds the body's first eight incidence entries, loaded a round
+// ahead by the body pass (zero past its run).
+template <class T, bool kAR = false, bool kPre = false>
+__device__ inline void body_w(const KArgs<T>& a, int b, const BodyHead& h,
+                              const uint32_t* c0 = nullptr) {
   using V = typename Vec4<T>::type;
   V* w = reinterpret_cast<V*>(a.wd);
   const V* q = reinterpret_cast<const V*>(a.qd);
   const double mi = h.mi;
   if (mi != 0.0) {
-    V s = gather_q<T, V>(a, q, h.s, h.e);
+    V s = kPre ? gather_q_pre<T, V>(a, q, h.s, h.e, c0) : gather_q<T, V>(a, q, h.s, h.e);
     if (a.nbil) add_bilateral<T, V>(a.bil_inc_start, a.bil_inc, a.bq, b, s);
     T m = (T)mi;
     V o;
@@ -804,17 +830,28 @@ __device__ inline void body_pass_schur(const KArgs<T>& a, const unsigned* s_mask
     }
     return;
   }
-  // the next round's heads load into registers while this round gathers
+  // heads load into registers two rounds ahead, and each body's first eight
+  // incidence entries one round ahead, while the current round gathers
   const int stride = gridDim.x * kThreads;
   int b = blockIdx.x * kThreads + threadIdx.x;
-  BodyHead h{0.0, 0, 0, 0};
+  BodyHead h{0.0, 0, 0, 0}, hn{0.0, 0, 0, 0};
   if (b < a.nb) h = body_head(a, b);
+  if (b + stride < a.nb) hn = body_head(a, b + stride);
+  uint32_t c[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c[j] = (h.s + j < h.e) ? __ldg(a.inc + h.s + j) : 0u;
   for (; b < a.nb; b += stride) {
-    const int bn = b + stride;
-    BodyHead hn{0.0, 0, 0, 0};
-    if (bn < a.nb) hn = body_head(a, bn);
-    if (a.nseg == 1 || !mask_done(a, s_mask, mwords, h.seg)) body_w<T, kAR>(a, b, h);
+    const int bnn = b + 2 * stride;
+    BodyHead hnn{0.0, 0, 0, 0};
+    if (bnn < a.nb) hnn = body_head(a, bnn);
+    uint32_t cn[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) cn[j] = (hn.s + j < hn.e) ? __ldg(a.inc + hn.s + j) : 0u;
+    if (a.nseg == 1 || !mask_done(a, s_mask, mwords, h.seg)) body_w<T, kAR, true>(a, b, h, c);
     h = hn;
+    hn = hnn;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) c[j] = cn[j];
   }
 }
 
