@@ -95,10 +95,10 @@ def solve_bytes_one_product(nc, nb, sweeps, backtracks):
 
 
 # DRAM bytes per algorithmic byte of the solve kernel, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 4.367 + 1.987 GB) on a
+# (dram__bytes_read.sum + dram__bytes_write.sum = 4.371 + 1.994 GB) on a
 # 30-iteration launch on this workload (11.415 GB algorithmic); the full launch
 # is scaled by it.
-TRAFFIC_PER_ALGORITHMIC_BYTE = 6.353819 / 11.415179
+TRAFFIC_PER_ALGORITHMIC_BYTE = 6.365664 / 11.415179
 
 
 def collide_bytes(nc, nb, npossible):
