@@ -2,7 +2,8 @@
 line's per-request sum (request_bytes_mixed, from the server's solver-work
 sums) equals the batched line's per-step model (solve_bytes_mixed) summed
 over the same steps, and the mixed model with no FP32 work left is the FP64
-model's iteration term."""
+model's iteration term; the served line's recorded 60-s run matches its
+profile summary."""
 import importlib.util
 import os
 
@@ -64,3 +65,18 @@ def test_mixed_model_limits():
     assert fp64 == 500 * (440 * nc + 120 * nb) + setup64
     # an FP32 iteration moves less than an FP64 one
     assert b.solve_bytes_mixed(nc, nb, 2, 0, 0) < b.solve_bytes_mixed(nc, nb, 2, 2, 0)
+
+
+def test_served_specification_record_matches_its_profile():
+    """bench.py's SERVED_SPEC_RECORD repeats the recorded 60-s run; its
+    figures are the ones profiles/served_poisson_200ps_60s.md gives."""
+    b = _bench()
+    r = b.SERVED_SPEC_RECORD
+    text = open(os.path.join(ROOT, "profiles", "served_poisson_200ps_60s.md")).read()
+    assert f"{r['value'] / 1e6:.2f} M" in text
+    assert f"{r['device_contact_steps_per_s'] / 1e6:.2f} M" in text
+    assert f"({r['speedup_vs_plain']}x)" in text
+    assert f"{r['time_per_step_ms']['p50']} / {r['time_per_step_ms']['p99']} ms" in text
+    assert f"{r['completion_latency_s']['p50']} / {r['completion_latency_s']['p99']} s" in text
+    assert f"{r['peak_resident_gb']} GB" in text
+    assert r["source"].split(": ")[1].startswith("profiles/served_poisson_200ps_60s.md")
